@@ -1,0 +1,937 @@
+// C ABI of n4b200: context, workspace planning, launches.
+//
+// The reference drives every step from the host with per-iteration
+// cudaMalloc/cudaFree, device-wide synchronisations and host FFTs
+// (cudaN4.cu:1418-1747).  Here a run is four stream-ordered launches with no
+// host round trip: prologue (threshold/shrink/log), the N4 kernel (all levels
+// and iterations on the device), per-axis tables, and the fused full-
+// resolution correction.  Workspaces are owned by the context and only grow.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "n4_kernels.cuh"
+
+using namespace n4;
+
+namespace {
+
+thread_local std::string g_err;
+
+n4_status_t fail(n4_status_t s, const std::string &msg) {
+  g_err = msg;
+  return s;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      cudaGetLastError();                                                                \
+      return fail(e_ == cudaErrorMemoryAllocation ? N4_ERR_OOM : N4_ERR_CUDA,            \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+    }                                                                                    \
+  } while (0)
+
+#define TRY(expr)                                \
+  do {                                           \
+    n4_status_t s_ = (expr);                     \
+    if (s_ != N4_OK) return s_;                  \
+  } while (0)
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  n4_status_t ensure(size_t bytes, const char *what) {
+    if (bytes <= cap) return N4_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    bytes = align_up(std::max<size_t>(bytes, 256), 256);
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(N4_ERR_OOM, std::string("cudaMalloc failed for ") + what);
+    }
+    cap = bytes;
+    return N4_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T> T *as() const { return (T *)p; }
+};
+
+// One slot of the descriptor upload ring: pinned host staging + device copy
+// + an event recorded after the last kernel that reads the slot.
+struct Slot {
+  char *h = nullptr;
+  DevBuf d;
+  size_t cap = 0;
+  cudaEvent_t ev = nullptr;
+  bool pending = false;
+  // report bookkeeping of the run that used the slot
+  int nrep = 0;
+  size_t off_rep = 0, off_flags = 0;
+  std::vector<int> path, csize;
+};
+
+struct TuneKey {
+  int X, Y, Z, nx, ny, nz, levels, bins, batch;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(X, Y, Z, nx, ny, nz, levels, bins, batch) <
+           std::tie(o.X, o.Y, o.Z, o.nx, o.ny, o.nz, o.levels, o.bins, o.batch);
+  }
+};
+struct TuneVal {
+  int grid;   // 1 = whole-GPU path
+  int K;      // CTAs per cluster
+  int nt;     // threads per CTA
+};
+
+constexpr int kStaticSmemReserve = 1024;
+constexpr int kSlots = 4;
+
+}  // namespace
+
+struct n4_context {
+  int device = 0;
+  int nsm = 0;
+  int max_smem = 0;
+  DevBuf imlog, tables, logu, big, red, bar;
+  DevBuf s1, s2, s3, s4, s5;   // component scratch
+  DevBuf h_im, h_mask, h_out, h_lat, h_bias, h_warm;   // host-run staging
+  Slot slots[kSlots];
+  int next_slot = 0;
+  int last_slot = -1;
+  cudaStream_t last_stream = nullptr;
+  cudaEvent_t last_done = nullptr;
+  std::map<TuneKey, TuneVal> tune;
+};
+
+namespace {
+
+// ------------------------------------------------------------------ params
+struct Dims {
+  int FX, FY, FZ;   // full resolution
+  int X, Y, Z;      // fitting grid
+};
+
+int npad_of(int bins) {
+  double e = std::ceil(std::log((double)bins) / std::log(2.0)) + 1.0;
+  return (int)(std::pow(2.0, e) + 0.5);
+}
+
+// float4 I/O is used only when rows are whole float4s and every pointer is 16-byte aligned.
+int vec4_ok(int fz, const void *a, const void *b, const void *c) {
+  auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
+  return (fz % 4 == 0) && al(a) && al(b) && al(c) ? 1 : 0;
+}
+
+int final_nc(unsigned nc0, unsigned levels) { return (int)(((nc0 - 3) << (levels - 1)) + 3); }
+
+n4_status_t check_params(const n4_params_t *p) {
+  if (!p) return fail(N4_ERR_INVALID_ARG, "params is NULL");
+  if (p->SplineOrder != 3) return fail(N4_ERR_UNSUPPORTED_SPLINE_ORDER, "only cubic B-splines (SplineOrder 3) are supported");
+  if (p->NumberOfHistogramBins < 2 || p->NumberOfHistogramBins > 2048)
+    return fail(N4_ERR_INVALID_ARG, "NumberOfHistogramBins must be in [2, 2048]");
+  if (p->NumberOfFittingLevels < 1 || p->NumberOfFittingLevels > N4_MAX_LEVELS)
+    return fail(N4_ERR_INVALID_ARG, "NumberOfFittingLevels must be in [1, 8]");
+  if (p->NumberOfControlPoints_x < 4 || p->NumberOfControlPoints_y < 4 || p->NumberOfControlPoints_z < 4)
+    return fail(N4_ERR_INVALID_ARG, "at least 4 control points per axis are required");
+  const int ncx = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
+  const int ncy = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);
+  const int ncz = final_nc(p->NumberOfControlPoints_z, p->NumberOfFittingLevels);
+  if (ncx > 1024 || ncy > 1024 || ncz > kMaxNcz || (long long)ncx * ncy * ncz > (1 << 20))
+    return fail(N4_ERR_TOO_LARGE, "final lattice too large (z control points <= 64, total <= 2^20)");
+  if (p->ShrinkFactor < 1 || p->ShrinkFactor > 16) return fail(N4_ERR_INVALID_ARG, "ShrinkFactor must be in [1, 16]");
+  if (!(p->WienerFilterNoise >= 0.0f) || !(p->BiasFieldFullWidthAtHalfMaximum > 0.0f))
+    return fail(N4_ERR_INVALID_ARG, "WienerFilterNoise must be >= 0 and the FWHM > 0");
+  if (!(p->FitEpsilon >= 0.0f)) return fail(N4_ERR_INVALID_ARG, "FitEpsilon must be >= 0");
+  for (unsigned l = 0; l < p->NumberOfFittingLevels; ++l)
+    if (p->MaximumNumberOfIterations[l] > 1000000u) return fail(N4_ERR_INVALID_ARG, "too many iterations");
+  return N4_OK;
+}
+
+n4_status_t make_dims(const n4_params_t *p, unsigned fx, unsigned fy, unsigned fz, Dims &d) {
+  const unsigned s = p->ShrinkFactor;
+  if (fx == 0 || fy == 0 || fz == 0) return fail(N4_ERR_INVALID_ARG, "empty volume");
+  if (fx % s || fy % s || fz % s) return fail(N4_ERR_INVALID_ARG, "dimensions must be multiples of ShrinkFactor");
+  if ((unsigned long long)fx * fy * fz >= (1ull << 40)) return fail(N4_ERR_TOO_LARGE, "volume too large");
+  d.FX = (int)fx; d.FY = (int)fy; d.FZ = (int)fz;
+  d.X = (int)(fx / s); d.Y = (int)(fy / s); d.Z = (int)(fz / s);
+  if (d.Z > 1024) return fail(N4_ERR_TOO_LARGE, "fitting grid rows longer than 1024 voxels (raise ShrinkFactor)");
+  if ((long long)d.X * d.Y * d.Z >= (1ll << 22) * 1024) return fail(N4_ERR_TOO_LARGE, "fitting grid too large");
+  return N4_OK;
+}
+
+Params make_dev_params(const n4_params_t *p) {
+  Params r{};
+  r.bins = (int)p->NumberOfHistogramBins;
+  r.wiener = p->WienerFilterNoise;
+  r.fwhm = p->BiasFieldFullWidthAtHalfMaximum;
+  r.thr = p->ConvergenceThreshold;
+  r.eps = p->FitEpsilon;
+  r.zero_den = (p->flags & N4_FLAG_FIT_ZERO_DEN) ? 1 : 0;
+  r.ddof1 = (p->flags & N4_FLAG_CV_DDOF1) ? 1 : 0;
+  for (unsigned l = 0; l < N4_MAX_LEVELS; ++l)
+    r.iters[l] = l < p->NumberOfFittingLevels ? (int)p->MaximumNumberOfIterations[l] : 0;
+  return r;
+}
+
+// Workspace layout for a group of K CTAs over the given fitting grids.
+Plan make_plan(const n4_params_t *p, int K, const std::vector<Dims> &vols, bool grid) {
+  Plan pl{};
+  pl.levels = (int)p->NumberOfFittingLevels;
+  pl.nc0x = (int)p->NumberOfControlPoints_x;
+  pl.nc0y = (int)p->NumberOfControlPoints_y;
+  pl.nc0z = (int)p->NumberOfControlPoints_z;
+  pl.NCX = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
+  pl.NCY = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);
+  pl.NCZ = final_nc(p->NumberOfControlPoints_z, p->NumberOfFittingLevels);
+  pl.NLAT = pl.NCX * pl.NCY * pl.NCZ;
+  pl.bins = (int)p->NumberOfHistogramBins;
+  pl.npad = npad_of(pl.bins);
+  pl.hoff = (int)(0.5 * (pl.npad - pl.bins));
+  long long slab = 0, rows_max = 0, nvxl = 0;
+  for (const Dims &d : vols) {
+    pl.Xmax = std::max(pl.Xmax, d.X);
+    pl.Ymax = std::max(pl.Ymax, d.Y);
+    pl.Zmax = std::max(pl.Zmax, d.Z);
+    const long long rows = (long long)d.X * d.Y;
+    const long long rpc = (rows + K - 1) / K;
+    rows_max = std::max(rows_max, rpc);
+    slab = std::max(slab, rpc * d.Z);
+    nvxl = std::max(nvxl, (rpc - 1) / d.Y + 2);
+  }
+  pl.slab_floats = (int)slab;
+  pl.rows_max = (int)rows_max;
+  pl.nvxl = (int)nvxl;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t r = o; o = align_up(o + bytes, 16); return (int)r; };
+  pl.o_ax = take(axis_bytes(pl.Xmax, pl.NCX - 3));
+  pl.o_ay = take(axis_bytes(pl.Ymax, pl.NCY - 3));
+  pl.o_az = take(axis_bytes(pl.Zmax, pl.NCZ - 3));
+  pl.o_L = take((size_t)pl.NLAT * 4);
+  pl.o_D = take((size_t)pl.NLAT * 4);
+  pl.o_den = take((size_t)pl.NLAT * 4);
+  pl.o_tmp = take((size_t)pl.NLAT * 4);
+  pl.o_aux = take((size_t)pl.NLAT * 4);
+  pl.o_hist = take((size_t)kHistCopies * pl.bins * 8);
+  pl.o_H = take((size_t)pl.bins * 4);
+  pl.o_E = take((size_t)pl.bins * 4);
+  pl.o_fa = take((size_t)pl.npad * 8);
+  pl.o_fb = take((size_t)pl.npad * 8);
+  pl.o_tw = take((size_t)pl.npad * 8);
+  pl.o_ff = take((size_t)pl.npad * 4);
+  pl.o_red = take(160 * 8);
+  pl.o_misc = take(64);
+  pl.sm_bytes = (int)align_up(o, 128);
+  o = 0;
+  if (!grid) {
+    pl.b_imlog = take(((size_t)pl.slab_floats + 8) * 4);
+    pl.b_logu = take((size_t)pl.slab_floats * 4);
+  }
+  pl.b_G = take((size_t)pl.rows_max * pl.NCZ * 4);
+  pl.b_Gd = take((size_t)pl.rows_max * pl.NCZ * 4);
+  pl.b_T2 = take((size_t)pl.nvxl * pl.NCY * pl.NCZ * 4);
+  pl.b_slotA = take(sizeof(Stats));
+  pl.b_slotB = take((size_t)pl.bins * 8);
+  pl.b_slotC = take((size_t)pl.NLAT * 4);
+  pl.big_bytes = (int)align_up(o, 128);
+  return pl;
+}
+
+bool cluster_fits(const n4_context *ctx, const Plan &pl) {
+  return (long long)pl.sm_bytes + pl.big_bytes + kStaticSmemReserve <= ctx->max_smem;
+}
+
+template <int NT>
+n4_status_t cluster_capacity(n4_context *ctx, int K, int smem, int *nclusters) {
+  auto kern = k_n4_cluster<NT>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(K);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = K;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  CK(cudaOccupancyMaxActiveClusters(&n, kern, &cfg));
+  *nclusters = n;
+  return N4_OK;
+}
+
+n4_status_t capacity(n4_context *ctx, int nt, int K, int smem, int *n) {
+  return nt == 1024 ? cluster_capacity<1024>(ctx, K, smem, n) : cluster_capacity<512>(ctx, K, smem, n);
+}
+
+// Largest cluster (<= 16 CTAs) whose per-CTA share of every volume fits.
+n4_status_t choose_cluster(n4_context *ctx, const n4_params_t *p, const std::vector<Dims> &vols, int nt,
+                           int *K_out) {
+  *K_out = 0;
+  for (int K : {16, 12, 8, 6, 4, 2, 1}) {
+    Plan pl = make_plan(p, K, vols, false);
+    if (!cluster_fits(ctx, pl)) continue;
+    int n = 0;
+    TRY(capacity(ctx, nt, K, pl.sm_bytes + pl.big_bytes, &n));
+    if (n > 0) { *K_out = K; return N4_OK; }
+  }
+  return N4_OK;
+}
+
+// ------------------------------------------------------------------ upload ring
+struct Upload {
+  Slot *slot;
+  int index;
+  size_t off;
+  char *h() const { return slot->h; }
+  template <class T> T *hp(size_t o) const { return (T *)(slot->h + o); }
+  template <class T> T *dp(size_t o) const { return (T *)((char *)slot->d.p + o); }
+};
+
+n4_status_t acquire_slot(n4_context *ctx, size_t bytes, Upload &u) {
+  const int i = ctx->next_slot;
+  ctx->next_slot = (ctx->next_slot + 1) % kSlots;
+  Slot &s = ctx->slots[i];
+  if (!s.ev) CK(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
+  if (s.pending) { CK(cudaEventSynchronize(s.ev)); s.pending = false; }
+  if (bytes > s.cap) {
+    if (s.h) cudaFreeHost(s.h);
+    s.h = nullptr;
+    s.cap = 0;
+    const size_t cap = align_up(std::max<size_t>(bytes, 1 << 16), 4096);
+    CK(cudaMallocHost((void **)&s.h, cap));
+    TRY(s.d.ensure(cap, "descriptor slot"));
+    s.cap = cap;
+  }
+  std::memset(s.h, 0, bytes);
+  u.slot = &s;
+  u.index = i;
+  u.off = 0;
+  return N4_OK;
+}
+
+// Order this run after the context's previous run (which may be on another stream).
+n4_status_t begin_run(n4_context *ctx, cudaStream_t st) {
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->last_done) CK(cudaEventCreateWithFlags(&ctx->last_done, cudaEventDisableTiming));
+  if (ctx->last_slot >= 0 && st != ctx->last_stream) CK(cudaStreamWaitEvent(st, ctx->last_done, 0));
+  return N4_OK;
+}
+
+n4_status_t end_run(n4_context *ctx, cudaStream_t st, Upload &u) {
+  CK(cudaEventRecord(u.slot->ev, st));
+  CK(cudaEventRecord(ctx->last_done, st));
+  u.slot->pending = true;
+  ctx->last_slot = u.index;
+  ctx->last_stream = st;
+  return N4_OK;
+}
+
+// ------------------------------------------------------------------ the run
+struct RunVol {
+  const float *im, *mask;
+  float *out, *lat, *bias;
+  const float *warm;
+  float *im_w, *mask_w;
+  Dims d;
+};
+
+n4_status_t launch_grid_path(n4_context *ctx, const n4_params_t *p, const Params &pr, const RunVol &rv,
+                             const VolJob &job0, int nt, cudaStream_t st) {
+  std::vector<Dims> one{rv.d};
+  int nblk = ctx->nsm;
+  Plan pl = make_plan(p, nblk, one, true);
+  if (pl.sm_bytes + kStaticSmemReserve > ctx->max_smem)
+    return fail(N4_ERR_TOO_LARGE, "histogram/lattice workspace exceeds shared memory");
+  const size_t nfit = (size_t)rv.d.X * rv.d.Y * rv.d.Z;
+  if ((long long)pl.rows_max * rv.d.Z >= (1ll << 22))
+    return fail(N4_ERR_TOO_LARGE, "fitting grid too large for one GPU (raise ShrinkFactor)");
+  TRY(ctx->logu.ensure(nfit * 4 + 64, "logU"));
+  TRY(ctx->big.ensure((size_t)pl.big_bytes * nblk, "grid workspace"));
+  TRY(ctx->red.ensure(std::max((size_t)pl.bins * 8, (size_t)pl.NLAT * 4) + 64, "grid reduction"));
+  TRY(ctx->bar.ensure(64, "grid barrier"));
+  CK(cudaMemsetAsync(ctx->bar.p, 0, 64, st));
+  GridArgs a{};
+  a.pl = pl;
+  a.pr = pr;
+  a.job = job0;
+  a.job.logu = ctx->logu.as<float>();
+  a.big_base = ctx->big.as<char>();
+  a.big_stride = pl.big_bytes;
+  a.bar.count = ctx->bar.as<unsigned>();
+  a.bar.gen = ctx->bar.as<unsigned>() + 1;
+  a.bar.err = (int *)ctx->bar.as<unsigned>() + 2;
+  a.bar.nblocks = nblk;
+  a.red_global = ctx->red.as<float>();
+  const int smem = pl.sm_bytes;
+  void *args[] = {&a};
+  if (nt == 1024) {
+    CK(cudaFuncSetAttribute(k_n4_grid<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_n4_grid<1024>, 1024, smem));
+    if (occ < 1) return fail(N4_ERR_TOO_LARGE, "grid kernel does not fit on an SM");
+    CK(cudaLaunchCooperativeKernel((void *)k_n4_grid<1024>, dim3(nblk), dim3(1024), args, smem, st));
+  } else {
+    CK(cudaFuncSetAttribute(k_n4_grid<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_n4_grid<512>, 512, smem));
+    if (occ < 1) return fail(N4_ERR_TOO_LARGE, "grid kernel does not fit on an SM");
+    CK(cudaLaunchCooperativeKernel((void *)k_n4_grid<512>, dim3(nblk), dim3(512), args, smem, st));
+  }
+  return N4_OK;
+}
+
+template <int NT>
+n4_status_t launch_cluster_kernel(const ClusterArgs &a, int K, int nclusters, int smem, cudaStream_t st) {
+  auto kern = k_n4_cluster<NT>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(K * nclusters);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = K;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, kern, a));
+  return N4_OK;
+}
+
+struct Choice {
+  bool grid;
+  int K, nt;
+};
+
+n4_status_t choose_path(n4_context *ctx, const n4_params_t *p, const std::vector<Dims> &vols, bool batch,
+                        Choice &c) {
+  const Dims &d0 = vols[0];
+  c.nt = 1024;
+  c.grid = false;
+  c.K = 0;
+  if (!batch && vols.size() == 1) {
+    TuneKey key{d0.X, d0.Y, d0.Z, (int)p->NumberOfControlPoints_x, (int)p->NumberOfControlPoints_y,
+                (int)p->NumberOfControlPoints_z, (int)p->NumberOfFittingLevels, (int)p->NumberOfHistogramBins, 0};
+    auto it = ctx->tune.find(key);
+    if (it != ctx->tune.end() && !(p->flags & (N4_FLAG_FORCE_GRID | N4_FLAG_FORCE_CLUSTER))) {
+      c.grid = it->second.grid != 0;
+      c.K = it->second.K;
+      c.nt = it->second.nt;
+      return N4_OK;
+    }
+  }
+  if (!(p->flags & N4_FLAG_FORCE_GRID)) TRY(choose_cluster(ctx, p, vols, c.nt, &c.K));
+  if (c.K == 0) {
+    if (p->flags & N4_FLAG_FORCE_CLUSTER) return fail(N4_ERR_TOO_LARGE, "volume does not fit a thread-block cluster");
+    c.grid = true;
+  }
+  return N4_OK;
+}
+
+// Core of n4_run / n4_run_batched: every pointer is a device pointer.
+n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector<RunVol> &rvs, cudaStream_t st,
+                        const Choice *forced) {
+  const int n = (int)rvs.size();
+  const Params pr = make_dev_params(p);
+  std::vector<Dims> dims;
+  for (const RunVol &r : rvs) dims.push_back(r.d);
+  // volumes that fit a cluster run together; the others use the whole GPU
+  Choice ch{};
+  if (forced) ch = *forced;
+  else TRY(choose_path(ctx, p, dims, n > 1, ch));
+  std::vector<int> in_cluster, in_grid;
+  if (!ch.grid) {
+    for (int i = 0; i < n; ++i) in_cluster.push_back(i);
+  } else if (n == 1) {
+    in_grid.push_back(0);
+  } else {
+    // batch with volumes too large for a cluster: split by fit
+    for (int i = 0; i < n; ++i) {
+      std::vector<Dims> one{dims[i]};
+      int K = 0;
+      TRY(choose_cluster(ctx, p, one, 1024, &K));
+      (K ? in_cluster : in_grid).push_back(i);
+    }
+    if (!in_cluster.empty()) {
+      std::vector<Dims> sub;
+      for (int i : in_cluster) sub.push_back(dims[i]);
+      ch.grid = false;
+      ch.nt = 1024;
+      TRY(choose_cluster(ctx, p, sub, 1024, &ch.K));
+    }
+  }
+  // ---- workspaces
+  const int NCX = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
+  const int NCY = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);
+  const int NCZ = final_nc(p->NumberOfControlPoints_z, p->NumberOfFittingLevels);
+  std::vector<size_t> imlog_off(n), tab_off(n);
+  size_t imlog_bytes = 0, tab_bytes = 0;
+  for (int i = 0; i < n; ++i) {
+    imlog_off[i] = imlog_bytes;
+    imlog_bytes = align_up(imlog_bytes + (size_t)dims[i].X * dims[i].Y * dims[i].Z * 4 + 64, 256);
+    tab_off[i] = tab_bytes;
+    tab_bytes += align_up(axis_bytes(dims[i].FX, NCX - 3), 256) + align_up(axis_bytes(dims[i].FY, NCY - 3), 256) +
+                 align_up(axis_bytes(dims[i].FZ, NCZ - 3), 256);
+  }
+  TRY(ctx->imlog.ensure(imlog_bytes, "fitting grid"));
+  TRY(ctx->tables.ensure(tab_bytes, "axis tables"));
+  // ---- descriptors
+  Upload u;
+  size_t o = 0;
+  auto take = [&](size_t b) { size_t r = o; o = align_up(o + b, 16); return r; };
+  const size_t o_pro = take(sizeof(PrologueVol) * n), o_pst = take(8 * n), o_job = take(sizeof(VolJob) * n),
+               o_ord = take(4 * n), o_tab = take(sizeof(TableJob) * 3 * n), o_cor = take(sizeof(CorrectVol) * n),
+               o_tst = take(8 * n), o_rep = take(sizeof(n4_report_t) * n), o_flg = take(4 * n),
+               o_q = take(16);
+  TRY(acquire_slot(ctx, o, u));
+  PrologueVol *pv = u.hp<PrologueVol>(o_pro);
+  long long *pst = u.hp<long long>(o_pst);
+  VolJob *jb = u.hp<VolJob>(o_job);
+  int *ord = u.hp<int>(o_ord);
+  TableJob *tj = u.hp<TableJob>(o_tab);
+  CorrectVol *cv = u.hp<CorrectVol>(o_cor);
+  long long *tst = u.hp<long long>(o_tst);
+  n4_report_t *rep = u.hp<n4_report_t>(o_rep);
+  long long fit_total = 0, tiles = 0;
+  char *tabs = ctx->tables.as<char>();
+  for (int i = 0; i < n; ++i) {
+    const RunVol &r = rvs[i];
+    const Dims &d = dims[i];
+    float *il = (float *)(ctx->imlog.as<char>() + imlog_off[i]);
+    pv[i] = PrologueVol{r.im, r.mask, r.im_w, r.mask_w, d.FX, d.FY, d.FZ, (int)p->ShrinkFactor,
+                        d.X, d.Y, d.Z, il, fit_total};
+    pst[i] = fit_total;
+    fit_total += (long long)d.X * d.Y * d.Z;
+    jb[i] = VolJob{d.X, d.Y, d.Z, il, nullptr, r.warm, r.lat, u.dp<n4_report_t>(o_rep) + i};
+    char *tx = tabs + tab_off[i];
+    char *ty = tx + align_up(axis_bytes(d.FX, NCX - 3), 256);
+    char *tz = ty + align_up(axis_bytes(d.FY, NCY - 3), 256);
+    tj[3 * i] = TableJob{tx, d.FX, NCX};
+    tj[3 * i + 1] = TableJob{ty, d.FY, NCY};
+    tj[3 * i + 2] = TableJob{tz, d.FZ, NCZ};
+    cv[i] = CorrectVol{r.im, r.out, r.bias, r.lat, tx, ty, tz, d.FX, d.FY, d.FZ, NCX, NCY, NCZ, tiles,
+                       vec4_ok(d.FZ, r.im, r.out, r.bias)};
+    tst[i] = tiles;
+    tiles += ((long long)d.FX * d.FY + kRowsPerTile - 1) / kRowsPerTile;
+    std::memset(&rep[i], 0, sizeof(n4_report_t));
+    rep[i].status = -1;
+  }
+  // longest-first order of the cluster queue
+  std::vector<int> order = in_cluster;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (long long)dims[a].X * dims[a].Y * dims[a].Z > (long long)dims[b].X * dims[b].Y * dims[b].Z;
+  });
+  for (size_t k = 0; k < order.size(); ++k) ord[k] = order[k];
+  TRY(begin_run(ctx, st));
+  CK(cudaMemcpyAsync(u.slot->d.p, u.slot->h, o, cudaMemcpyHostToDevice, st));
+  int *flags = u.dp<int>(o_flg);
+  // ---- prologue
+  {
+    const int blocks = (int)std::min<long long>((fit_total + 255) / 256, (long long)ctx->nsm * 16);
+    k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(u.dp<PrologueVol>(o_pro), u.dp<long long>(o_pst), n, fit_total,
+                                                     p->low_value, flags);
+    CK(cudaGetLastError());
+    if (p->ShrinkFactor > 1 && (p->flags & N4_FLAG_INPLACE_THRESH)) {
+      for (int i = 0; i < n; ++i) {
+        const long long nf = (long long)dims[i].FX * dims[i].FY * dims[i].FZ;
+        if (rvs[i].im_w) {
+          k_threshold_inplace<<<(int)std::min<long long>((nf + 255) / 256, ctx->nsm * 16LL), 256, 0, st>>>(
+              rvs[i].im_w, rvs[i].mask_w, nf, p->low_value);
+          CK(cudaGetLastError());
+        }
+      }
+    }
+  }
+  // ---- N4
+  Slot &slot = *u.slot;
+  slot.nrep = n;
+  slot.off_rep = o_rep;
+  slot.off_flags = o_flg;
+  slot.path.assign(n, 0);
+  slot.csize.assign(n, 0);
+  if (!in_cluster.empty()) {
+    std::vector<Dims> sub;
+    for (int i : in_cluster) sub.push_back(dims[i]);
+    Plan pl = make_plan(p, ch.K, sub, false);
+    const int smem = pl.sm_bytes + pl.big_bytes;
+    int cap = 0;
+    TRY(capacity(ctx, ch.nt, ch.K, smem, &cap));
+    if (cap < 1) return fail(N4_ERR_TOO_LARGE, "no cluster of this size fits on the device");
+    ClusterArgs a{};
+    a.pl = pl;
+    a.pr = pr;
+    a.jobs = u.dp<VolJob>(o_job);
+    a.order = u.dp<int>(o_ord);
+    a.njobs = (int)in_cluster.size();
+    a.queue = u.dp<int>(o_q);
+    a.use_tma = 1;
+    const int ncl = std::min<int>(cap, (int)in_cluster.size());
+    if (ch.nt == 1024) TRY(launch_cluster_kernel<1024>(a, ch.K, ncl, smem, st));
+    else TRY(launch_cluster_kernel<512>(a, ch.K, ncl, smem, st));
+    for (int i : in_cluster) { slot.path[i] = 1; slot.csize[i] = ch.K; }
+  }
+  for (int i : in_grid) {
+    VolJob j = jb[i];
+    j.report = u.dp<n4_report_t>(o_rep) + i;
+    TRY(launch_grid_path(ctx, p, pr, rvs[i], j, ch.nt ? ch.nt : 1024, st));
+    slot.path[i] = 2;
+    slot.csize[i] = ctx->nsm;
+  }
+  // ---- final correction at full resolution
+  k_axis_tables<<<3 * n, 256, 0, st>>>(u.dp<TableJob>(o_tab));
+  CK(cudaGetLastError());
+  k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(o_cor), u.dp<long long>(o_tst), n, p->low_value);
+  CK(cudaGetLastError());
+  // reports back to the slot's pinned buffer
+  CK(cudaMemcpyAsync(u.slot->h + o_rep, u.dp<char>(o_rep), sizeof(n4_report_t) * n + 0, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(u.slot->h + o_flg, u.dp<char>(o_flg), 4 * n, cudaMemcpyDeviceToHost, st));
+  return end_run(ctx, st, u);
+}
+
+n4_status_t collect(n4_context *ctx, n4_report_t *out, int n) {
+  if (ctx->last_slot < 0) return fail(N4_ERR_INVALID_ARG, "no run to synchronise with");
+  Slot &s = ctx->slots[ctx->last_slot];
+  CK(cudaEventSynchronize(s.ev));
+  s.pending = false;
+  const n4_report_t *rep = (const n4_report_t *)(s.h + s.off_rep);
+  const int *flg = (const int *)(s.h + s.off_flags);
+  n4_status_t worst = N4_OK;
+  for (int i = 0; i < s.nrep; ++i) {
+    n4_report_t r = rep[i];
+    if (r.status == -1) r.status = N4_ERR_CUDA;
+    if (r.status == N4_OK && flg[i]) r.status = N4_ERR_NONFINITE;
+    r.path = s.path[i];
+    r.cluster_size = s.csize[i];
+    if (out && i < n) out[i] = r;
+    if (r.status != N4_OK && worst == N4_OK) worst = (n4_status_t)r.status;
+  }
+  if (worst != N4_OK) return fail(worst, std::string("volume failed: ") + n4_status_string(worst));
+  return N4_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+void n4_params_default(n4_params_t *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->NumberOfHistogramBins = 200;
+  p->WienerFilterNoise = 0.01f;
+  p->BiasFieldFullWidthAtHalfMaximum = 0.15f;
+  p->NumberOfControlPoints_x = p->NumberOfControlPoints_y = p->NumberOfControlPoints_z = 4;
+  p->NumberOfFittingLevels = 4;
+  for (int l = 0; l < N4_MAX_LEVELS; ++l) p->MaximumNumberOfIterations[l] = 50;
+  p->ConvergenceThreshold = 0.001f;
+  p->low_value = 10.0f;
+  p->ShrinkFactor = 1;
+  p->SplineOrder = 3;
+  p->FitEpsilon = 1e-3f;
+  p->flags = 0;
+}
+
+n4_status_t n4_lattice_dims(const n4_params_t *p, unsigned int dims[3], size_t *count) {
+  TRY(check_params(p));
+  const int x = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
+  const int y = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);
+  const int z = final_nc(p->NumberOfControlPoints_z, p->NumberOfFittingLevels);
+  if (dims) { dims[0] = x; dims[1] = y; dims[2] = z; }
+  if (count) *count = (size_t)x * y * z;
+  return N4_OK;
+}
+
+const char *n4_status_string(int s) {
+  switch (s) {
+    case N4_OK: return "ok";
+    case N4_ERR_INVALID_ARG: return "invalid argument";
+    case N4_ERR_UNSUPPORTED_SPLINE_ORDER: return "unsupported spline order";
+    case N4_ERR_EMPTY_MASK: return "empty mask";
+    case N4_ERR_OOM: return "out of device memory";
+    case N4_ERR_CUDA: return "CUDA error";
+    case N4_ERR_TIMEOUT: return "device wait timed out";
+    case N4_ERR_NONFINITE: return "non-finite intensity in the mask";
+    case N4_ERR_TOO_LARGE: return "request exceeds a supported limit";
+    case N4_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char *n4_last_error_string(void) { return g_err.c_str(); }
+const char *n4_version(void) { return "n4b200 1.0 (sm_100a)"; }
+
+n4_status_t n4_create(n4_context_t **out, int device) {
+  if (!out) return fail(N4_ERR_INVALID_ARG, "ctx is NULL");
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(N4_ERR_NO_DEVICE, "no CUDA device available");
+  }
+  if (device < 0 || device >= count) return fail(N4_ERR_INVALID_ARG, "bad device index");
+  CK(cudaSetDevice(device));
+  int major = 0;
+  CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  if (major != 10) return fail(N4_ERR_NO_DEVICE, "n4b200 is built for sm_100a (B200) only");
+  n4_context *c = new n4_context();
+  c->device = device;
+  CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+  CK(cudaDeviceGetAttribute(&c->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  *out = c;
+  return N4_OK;
+}
+
+n4_status_t n4_destroy(n4_context_t *c) {
+  if (!c) return N4_OK;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  for (DevBuf *b : {&c->imlog, &c->tables, &c->logu, &c->big, &c->red, &c->bar, &c->s1, &c->s2, &c->s3, &c->s4,
+                    &c->s5, &c->h_im, &c->h_mask, &c->h_out, &c->h_lat, &c->h_bias, &c->h_warm})
+    b->release();
+  for (Slot &s : c->slots) {
+    if (s.h) cudaFreeHost(s.h);
+    s.d.release();
+    if (s.ev) cudaEventDestroy(s.ev);
+  }
+  if (c->last_done) cudaEventDestroy(c->last_done);
+  delete c;
+  return N4_OK;
+}
+
+n4_status_t n4_run(n4_context_t *ctx, const n4_params_t *p, const float *d_im, const float *d_mask,
+                   unsigned int fx, unsigned int fy, unsigned int fz, float *d_im_normalized, float *d_lattice,
+                   float *d_bias_field, const float *d_warm_lattice, void *stream, n4_report_t *report) {
+  if (!ctx) return fail(N4_ERR_INVALID_ARG, "ctx is NULL");
+  TRY(check_params(p));
+  if (!d_im || !d_im_normalized || !d_lattice) return fail(N4_ERR_INVALID_ARG, "NULL input/output pointer");
+  RunVol r{};
+  TRY(make_dims(p, fx, fy, fz, r.d));
+  r.im = d_im;
+  r.mask = d_mask;
+  r.out = d_im_normalized;
+  r.lat = d_lattice;
+  r.bias = d_bias_field;
+  r.warm = d_warm_lattice;
+  if (p->flags & N4_FLAG_INPLACE_THRESH) { r.im_w = const_cast<float *>(d_im); r.mask_w = const_cast<float *>(d_mask); }
+  std::vector<RunVol> v{r};
+  TRY(run_volumes(ctx, p, v, (cudaStream_t)stream, nullptr));
+  if (report) return collect(ctx, report, 1);
+  return N4_OK;
+}
+
+n4_status_t n4_run_batched(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols, void *stream,
+                           n4_report_t *reports) {
+  if (!ctx || !vols || n < 1) return fail(N4_ERR_INVALID_ARG, "bad batch");
+  TRY(check_params(p));
+  std::vector<RunVol> v(n);
+  for (int i = 0; i < n; ++i) {
+    const n4_volume_t &q = vols[i];
+    if (!q.im || !q.im_normalized || !q.lattice) return fail(N4_ERR_INVALID_ARG, "NULL pointer in batch");
+    TRY(make_dims(p, q.fx, q.fy, q.fz, v[i].d));
+    v[i].im = q.im;
+    v[i].mask = q.mask;
+    v[i].out = q.im_normalized;
+    v[i].lat = q.lattice;
+    v[i].bias = q.bias_field;
+    v[i].warm = q.warm_lattice;
+  }
+  TRY(run_volumes(ctx, p, v, (cudaStream_t)stream, nullptr));
+  if (reports) return collect(ctx, reports, n);
+  return N4_OK;
+}
+
+n4_status_t n4_sync(n4_context_t *ctx, n4_report_t *reports, int n) {
+  if (!ctx) return fail(N4_ERR_INVALID_ARG, "ctx is NULL");
+  return collect(ctx, reports, n);
+}
+
+n4_status_t n4_run_host(n4_context_t *ctx, const n4_params_t *p, const float *h_im, const float *h_mask,
+                        unsigned int fx, unsigned int fy, unsigned int fz, float *h_im_normalized, float *h_lattice,
+                        float *h_bias_field, const float *h_warm_lattice, n4_report_t *report) {
+  if (!ctx) return fail(N4_ERR_INVALID_ARG, "ctx is NULL");
+  TRY(check_params(p));
+  if (!h_im || !h_im_normalized || !h_lattice) return fail(N4_ERR_INVALID_ARG, "NULL input/output pointer");
+  Dims d;
+  TRY(make_dims(p, fx, fy, fz, d));
+  CK(cudaSetDevice(ctx->device));
+  size_t nlat = 0;
+  TRY(n4_lattice_dims(p, nullptr, &nlat));
+  const size_t nv = (size_t)fx * fy * fz;
+  const size_t nwarm = (size_t)p->NumberOfControlPoints_x * p->NumberOfControlPoints_y * p->NumberOfControlPoints_z;
+  TRY(ctx->h_im.ensure(nv * 4, "input"));
+  TRY(ctx->h_out.ensure(nv * 4, "output"));
+  TRY(ctx->h_lat.ensure(nlat * 4, "lattice"));
+  if (h_mask) TRY(ctx->h_mask.ensure(nv * 4, "mask"));
+  if (h_bias_field) TRY(ctx->h_bias.ensure(nv * 4, "bias"));
+  if (h_warm_lattice) TRY(ctx->h_warm.ensure(nwarm * 4, "warm lattice"));
+  cudaStream_t st = nullptr;
+  CK(cudaMemcpyAsync(ctx->h_im.p, h_im, nv * 4, cudaMemcpyHostToDevice, st));
+  if (h_mask) CK(cudaMemcpyAsync(ctx->h_mask.p, h_mask, nv * 4, cudaMemcpyHostToDevice, st));
+  if (h_warm_lattice) CK(cudaMemcpyAsync(ctx->h_warm.p, h_warm_lattice, nwarm * 4, cudaMemcpyHostToDevice, st));
+  n4_report_t rep;
+  n4_status_t s = n4_run(ctx, p, ctx->h_im.as<float>(), h_mask ? ctx->h_mask.as<float>() : nullptr, fx, fy, fz,
+                         ctx->h_out.as<float>(), ctx->h_lat.as<float>(), h_bias_field ? ctx->h_bias.as<float>() : nullptr,
+                         h_warm_lattice ? ctx->h_warm.as<float>() : nullptr, st, &rep);
+  if (report) *report = rep;
+  if (s != N4_OK && s != N4_ERR_EMPTY_MASK && s != N4_ERR_NONFINITE) return s;
+  CK(cudaMemcpyAsync(h_im_normalized, ctx->h_out.p, nv * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(h_lattice, ctx->h_lat.p, nlat * 4, cudaMemcpyDeviceToHost, st));
+  if (h_bias_field) CK(cudaMemcpyAsync(h_bias_field, ctx->h_bias.p, nv * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return s;
+}
+
+// ---------------------------------------------------------------- components
+static n4_status_t component_tables(n4_context_t *ctx, unsigned fx, unsigned fy, unsigned fz, unsigned nx, unsigned ny,
+                                    unsigned nz, cudaStream_t st, Axis &ax, Axis &ay, Axis &az) {
+  const size_t bx = align_up(axis_bytes(fx, nx - 3), 256), by = align_up(axis_bytes(fy, ny - 3), 256),
+               bz = align_up(axis_bytes(fz, nz - 3), 256);
+  TRY(ctx->s5.ensure(bx + by + bz + sizeof(TableJob) * 3 + 256, "tables"));
+  char *base = ctx->s5.as<char>();
+  TableJob tj[3] = {{base, (int)fx, (int)nx}, {base + bx, (int)fy, (int)ny}, {base + bx + by, (int)fz, (int)nz}};
+  Upload u;
+  TRY(acquire_slot(ctx, sizeof(tj), u));
+  std::memcpy(u.h(), tj, sizeof(tj));
+  TRY(begin_run(ctx, st));
+  CK(cudaMemcpyAsync(u.slot->d.p, u.slot->h, sizeof(tj), cudaMemcpyHostToDevice, st));
+  k_axis_tables<<<3, 256, 0, st>>>(u.dp<TableJob>(0));
+  CK(cudaGetLastError());
+  u.slot->nrep = 0;
+  TRY(end_run(ctx, st, u));
+  ax = axis_at(base, fx, nx);
+  ay = axis_at(base + bx, fy, ny);
+  az = axis_at(base + bx + by, fz, nz);
+  return N4_OK;
+}
+
+n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const float *d_mask, unsigned int ncpt_x,
+                             unsigned int ncpt_y, unsigned int ncpt_z, unsigned int fx, unsigned int fy,
+                             unsigned int fz, float eps, int zero_den, float *d_lattice, void *stream) {
+  if (!ctx || !d_field || !d_lattice) return fail(N4_ERR_INVALID_ARG, "NULL pointer");
+  if (ncpt_x < 4 || ncpt_y < 4 || ncpt_z < 4 || !fx || !fy || !fz) return fail(N4_ERR_INVALID_ARG, "bad sizes");
+  if ((unsigned long long)fx * fy * fz >= (1ull << 36)) return fail(N4_ERR_TOO_LARGE, "field too large");
+  cudaStream_t st = (cudaStream_t)stream;
+  Axis ax, ay, az;
+  TRY(component_tables(ctx, fx, fy, fz, ncpt_x, ncpt_y, ncpt_z, st, ax, ay, az));
+  const size_t t1 = (size_t)fx * fy * ncpt_z, t2 = (size_t)fx * ncpt_y * ncpt_z;
+  TRY(ctx->s1.ensure(t1 * 8, "fit rows"));
+  TRY(ctx->s2.ensure(t2 * 8, "fit planes"));
+  float *t1n = ctx->s1.as<float>(), *t1d = t1n + t1, *t2n = ctx->s2.as<float>(), *t2d = t2n + t2;
+  const int gb = ctx->nsm * 8;
+  k_fit_rows<<<(int)std::min<size_t>((t1 + 255) / 256, gb), 256, 0, st>>>(d_field, d_mask, fx, fy, fz, az, t1n, t1d);
+  k_fit_planes<<<(int)std::min<size_t>((t2 + 255) / 256, gb), 256, 0, st>>>(t1n, t1d, fx, fy, ay, ncpt_z, t2n, t2d);
+  const int nlat = ncpt_x * ncpt_y * ncpt_z;
+  k_fit_final<<<(nlat + 255) / 256, 256, 0, st>>>(t2n, t2d, fx, ax, ncpt_y, ncpt_z, eps, zero_den, d_lattice);
+  CK(cudaGetLastError());
+  return N4_OK;
+}
+
+n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice, unsigned int ncpt_x, unsigned int ncpt_y,
+                                  unsigned int ncpt_z, unsigned int fx, unsigned int fy, unsigned int fz,
+                                  float *d_fitted, void *stream) {
+  if (!ctx || !d_lattice || !d_fitted) return fail(N4_ERR_INVALID_ARG, "NULL pointer");
+  if (ncpt_x < 4 || ncpt_y < 4 || ncpt_z < 4 || !fx || !fy || !fz) return fail(N4_ERR_INVALID_ARG, "bad sizes");
+  if (ncpt_z > (unsigned)kMaxNcz) return fail(N4_ERR_TOO_LARGE, "at most 64 control points along z");
+  cudaStream_t st = (cudaStream_t)stream;
+  Axis ax, ay, az;
+  TRY(component_tables(ctx, fx, fy, fz, ncpt_x, ncpt_y, ncpt_z, st, ax, ay, az));
+  CorrectVol cv{nullptr, d_fitted, nullptr, d_lattice, (char *)ax.s, (char *)ay.s, (char *)az.s,
+                (int)fx, (int)fy, (int)fz, (int)ncpt_x, (int)ncpt_y, (int)ncpt_z, 0,
+                vec4_ok((int)fz, nullptr, d_fitted, nullptr)};
+  const long long tiles = ((long long)fx * fy + kRowsPerTile - 1) / kRowsPerTile;
+  Upload u;
+  TRY(acquire_slot(ctx, sizeof(cv) + 16, u));
+  std::memcpy(u.h(), &cv, sizeof(cv));
+  TRY(begin_run(ctx, st));
+  CK(cudaMemcpyAsync(u.slot->d.p, u.slot->h, sizeof(cv) + 16, cudaMemcpyHostToDevice, st));
+  const size_t so = align_up(sizeof(cv), 16);
+  k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0.0f);
+  CK(cudaGetLastError());
+  u.slot->nrep = 0;
+  return end_run(ctx, st, u);
+}
+
+n4_status_t n4_upsample_lattice3d(n4_context_t *ctx, const float *d_lattice, unsigned int ncpt_x, unsigned int ncpt_y,
+                                  unsigned int ncpt_z, float *d_lattice_upsample, void *stream) {
+  if (!ctx || !d_lattice || !d_lattice_upsample) return fail(N4_ERR_INVALID_ARG, "NULL pointer");
+  if (ncpt_x < 4 || ncpt_y < 4 || ncpt_z < 4) return fail(N4_ERR_INVALID_ARG, "at least 4 control points per axis");
+  CK(cudaSetDevice(ctx->device));
+  k_refine<<<1, 256, 0, (cudaStream_t)stream>>>(d_lattice, ncpt_x, ncpt_y, ncpt_z, d_lattice_upsample);
+  CK(cudaGetLastError());
+  return N4_OK;
+}
+
+n4_status_t n4_sharpen_image(n4_context_t *ctx, const float *d_before, const float *d_mask, unsigned int n,
+                             unsigned int bins, float wiener, float fwhm, float *d_after, float *bin_min,
+                             float *bin_max, float *h_E) {
+  if (!ctx || !d_before || !d_after || n == 0) return fail(N4_ERR_INVALID_ARG, "bad arguments");
+  if (bins < 2 || bins > 2048) return fail(N4_ERR_INVALID_ARG, "bins must be in [2, 2048]");
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = nullptr;
+  const int nb = std::min<int>((int)((n + 255) / 256), ctx->nsm * 8);
+  TRY(ctx->s1.ensure((size_t)nb * 8 + 64, "partials"));
+  TRY(ctx->s2.ensure((size_t)bins * 8 + (size_t)bins * 4 + 64, "histogram"));
+  float *part = ctx->s1.as<float>();
+  float *stats = part + 2 * nb;
+  unsigned long long *hist = ctx->s2.as<unsigned long long>();
+  float *E = (float *)(hist + bins);
+  k_minmax<<<nb, 256, 0, st>>>(d_before, d_mask, n, part);
+  k_minmax_final<<<1, 256, 0, st>>>(part, nb, bins, stats);
+  CK(cudaMemsetAsync(hist, 0, (size_t)bins * 8, st));
+  k_hist<<<nb, 256, bins * 8, st>>>(d_before, d_mask, n, stats, bins, hist);
+  const int npad = npad_of(bins), hoff = (int)(0.5 * (npad - bins));
+  const int smem = npad * (8 * 3 + 4) + bins * 8;
+  CK(cudaFuncSetAttribute(k_sharpen, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_sharpen<<<1, 512, smem, st>>>(hist, stats, bins, npad, hoff, wiener, fwhm, E);
+  k_remap<<<nb, 256, 0, st>>>(d_before, d_mask, n, stats, E, bins, d_after);
+  CK(cudaGetLastError());
+  float hs[3];
+  CK(cudaMemcpyAsync(hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  if (h_E) CK(cudaMemcpyAsync(h_E, E, (size_t)bins * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (bin_min) *bin_min = hs[0];
+  if (bin_max) *bin_max = hs[1];
+  if (!(hs[0] <= hs[1])) return fail(N4_ERR_EMPTY_MASK, "no voxel in the mask");
+  return N4_OK;
+}
+
+n4_status_t n4_convergence(n4_context_t *ctx, const float *d_field1, const float *d_field2, const float *d_mask,
+                           unsigned int n, int ddof, double *cv) {
+  if (!ctx || !d_field1 || !d_field2 || !cv || n == 0) return fail(N4_ERR_INVALID_ARG, "bad arguments");
+  CK(cudaSetDevice(ctx->device));
+  const int nb = std::min<int>((int)((n + 255) / 256), ctx->nsm * 4);
+  TRY(ctx->s1.ensure((size_t)nb * 24, "partials"));
+  k_cv<<<nb, 256>>>(d_field1, d_field2, d_mask, n, ctx->s1.as<double>());
+  CK(cudaGetLastError());
+  std::vector<double> part((size_t)nb * 3);
+  CK(cudaMemcpy(part.data(), ctx->s1.p, part.size() * 8, cudaMemcpyDeviceToHost));
+  double s0 = 0, s1 = 0, c = 0;
+  for (int b = 0; b < nb; ++b) { s0 += part[3 * b]; s1 += part[3 * b + 1]; c += part[3 * b + 2]; }
+  if (c < 1.0) return fail(N4_ERR_EMPTY_MASK, "no voxel in the mask");
+  const double m = s0 / c;
+  double var = s1 / c - m * m;
+  if (ddof) var = c > 1.0 ? var * c / (c - 1.0) : 0.0;
+  *cv = std::sqrt(var > 0 ? var : 0.0) / (1.0 + m);
+  return N4_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,428 @@
+// Device helpers shared by every n4b200 kernel (sm_100a).
+//
+// * per-axis cubic B-spline tables (span index, weights, fit weights),
+//   computed in FP64 with the reference's formulas (N4.py:174-181,
+//   N4.py:210-222) and stored in FP32;
+// * a CTA-level Stockham radix-8/4/2 FFT in shared memory and the Gaussian
+//   Wiener-deconvolution sharpening map built on it (N4.py:32-101,
+//   cudaN4.cu:733-817);
+// * fractional-histogram binning and the piecewise-linear remap
+//   (N4.py:14-29, N4.py:103-113);
+// * warp/CTA reductions and a bounded software grid barrier.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/n4b200.h"
+
+namespace n4 {
+
+constexpr int kMaxThreads = 1024;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr float kHistScale = 16777216.0f;        // 2^24 fixed-point histogram weight
+constexpr double kHistInvScale = 1.0 / 16777216.0;
+constexpr int kHistCopies = 4;                   // shared histogram copies per CTA
+constexpr unsigned long long kSpinLimit = 1ull << 25;   // bounded waits (~2-4 s)
+
+// ---------------------------------------------------------------- tables
+// One axis of the fitting grid at one level.  Arrays live in shared or
+// global memory; all pointers are generic.
+struct Axis {
+  int n;        // voxels along the axis
+  int nc;       // control points (= spans + 3)
+  int nsp;      // spans
+  int *s;       // [n]   span index of each voxel
+  float4 *w;    // [n]   cubic weights B0..B3
+  float *p;     // [4][n] fit numerator weights  w_j^3 / sum_k w_k^2
+  float *q;     // [4][n] fit denominator weights w_j^2
+  int *lo, *hi; // [nsp] voxel range of each span
+};
+
+// Byte size of an axis table with `n` voxels and `nsp` spans (16-B multiple).
+__host__ __device__ inline size_t axis_bytes(int n, int nsp) {
+  size_t b = 0;
+  b += ((size_t)n * 4 + 15) / 16 * 16;          // s
+  b += (size_t)n * 16;                           // w
+  b += (size_t)n * 16 * 2;                       // p, q
+  b += ((size_t)nsp * 8 + 15) / 16 * 16;         // lo, hi
+  return b;
+}
+
+__host__ __device__ inline Axis axis_at(char *base, int n, int nc) {
+  Axis a;
+  a.n = n; a.nc = nc; a.nsp = nc - 3;
+  char *p = base;
+  a.s = (int *)p;    p += ((size_t)n * 4 + 15) / 16 * 16;
+  a.w = (float4 *)p; p += (size_t)n * 16;
+  a.p = (float *)p;  p += (size_t)n * 16;
+  a.q = (float *)p;  p += (size_t)n * 16;
+  a.lo = (int *)p;   a.hi = a.lo + a.nsp;
+  return a;
+}
+
+// Span index of voxel i, as N4.py:210 computes it: floor((i + 0.5) / span)
+// with span = n / nspans, all in IEEE FP64 (no contraction).
+__device__ __forceinline__ int span_of(int i, double span, int nsp) {
+  double u = __dadd_rn((double)i, 0.5);
+  int s = (int)floor(__ddiv_rn(u, span));
+  return s < 0 ? 0 : (s >= nsp ? nsp - 1 : s);
+}
+
+// Fill one axis table with the CTA's threads (caller synchronises).
+__device__ void build_axis(const Axis &a) {
+  const double span = __ddiv_rn((double)a.n, (double)a.nsp);
+  for (int i = threadIdx.x; i < a.n; i += blockDim.x) {
+    int s = span_of(i, span, a.nsp);
+    double u = __dadd_rn((double)i, 0.5);
+    double t = __ddiv_rn(__dsub_rn(u, __dmul_rn((double)s, span)), span);
+    double t2 = t * t, t3 = t * t * t, tm = 1.0 - t;
+    double w0 = tm * tm * tm / 6.0;
+    double w1 = (3.0 * t3 - 6.0 * t2 + 4.0) / 6.0;
+    double w2 = (-3.0 * t3 + 3.0 * t2 + 3.0 * t + 1.0) / 6.0;
+    double w3 = t3 / 6.0;
+    double S = w0 * w0 + w1 * w1 + w2 * w2 + w3 * w3;
+    a.s[i] = s;
+    a.w[i] = make_float4((float)w0, (float)w1, (float)w2, (float)w3);
+    a.p[0 * a.n + i] = (float)(w0 * w0 * w0 / S);
+    a.p[1 * a.n + i] = (float)(w1 * w1 * w1 / S);
+    a.p[2 * a.n + i] = (float)(w2 * w2 * w2 / S);
+    a.p[3 * a.n + i] = (float)(w3 * w3 * w3 / S);
+    a.q[0 * a.n + i] = (float)(w0 * w0);
+    a.q[1 * a.n + i] = (float)(w1 * w1);
+    a.q[2 * a.n + i] = (float)(w2 * w2);
+    a.q[3 * a.n + i] = (float)(w3 * w3);
+  }
+  // voxel range of every span by binary search on the monotone span index
+  for (int sp = threadIdx.x; sp < a.nsp; sp += blockDim.x) {
+    int lo = 0, hi = a.n;              // first voxel with span >= sp
+    while (lo < hi) { int m = (lo + hi) >> 1; if (span_of(m, span, a.nsp) >= sp) hi = m; else lo = m + 1; }
+    int l2 = lo, h2 = a.n;             // first voxel with span >= sp + 1
+    while (l2 < h2) { int m = (l2 + h2) >> 1; if (span_of(m, span, a.nsp) >= sp + 1) h2 = m; else l2 = m + 1; }
+    a.lo[sp] = lo;
+    a.hi[sp] = l2;
+  }
+}
+
+// b = sum_j w_j g[j] with a fixed association (identical in every pass).
+__device__ __forceinline__ float dot4(float4 w, const float *g) {
+  float b = __fmul_rn(w.x, g[0]);
+  b = __fmaf_rn(w.y, g[1], b);
+  b = __fmaf_rn(w.z, g[2], b);
+  b = __fmaf_rn(w.w, g[3], b);
+  return b;
+}
+
+// Exact floor(i / d) for 0 <= i < 2^22 and 1 <= d <= 2^10 via a 32-bit magic.
+struct FastDiv {
+  unsigned d, m;
+  __host__ __device__ FastDiv() : d(1), m(0) {}
+  __host__ __device__ explicit FastDiv(unsigned dd) : d(dd), m((unsigned)((0x100000000ull + dd - 1) / dd)) {}
+  __device__ __forceinline__ unsigned div(unsigned i) const { return d == 1 ? i : __umulhi(i, m); }
+};
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ float warp_min(float v) {
+  for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+  for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// CTA-wide reduction of four values (min, max, sum, sum) into out[0..3] of
+// thread 0; `scratch` holds 4 * 32 doubles.  Deterministic order.
+__device__ void block_reduce4(float vmin, float vmax, double s0, double s1,
+                              double *scratch, double out[4]) {
+  vmin = warp_min(vmin); vmax = warp_max(vmax); s0 = warp_sum(s0); s1 = warp_sum(s1);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) {
+    scratch[wid] = vmin; scratch[32 + wid] = vmax; scratch[64 + wid] = s0; scratch[96 + wid] = s1;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    float a = lane < nw ? (float)scratch[lane] : INFINITY;
+    float b = lane < nw ? (float)scratch[32 + lane] : -INFINITY;
+    double c = lane < nw ? scratch[64 + lane] : 0.0;
+    double d = lane < nw ? scratch[96 + lane] : 0.0;
+    a = warp_min(a); b = warp_max(b); c = warp_sum(c); d = warp_sum(d);
+    if (lane == 0) { out[0] = a; out[1] = b; out[2] = c; out[3] = d; }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------- FFT
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }  // a * (-i)
+
+__device__ __forceinline__ void dft2(float2 *v) {
+  float2 a = v[0], b = v[1];
+  v[0] = cadd(a, b); v[1] = csub(a, b);
+}
+__device__ __forceinline__ void dft4(float2 &v0, float2 &v1, float2 &v2, float2 &v3) {
+  float2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = mul_mi(csub(v1, v3));
+  v0 = cadd(t0, t2); v2 = csub(t0, t2); v1 = cadd(t1, t3); v3 = csub(t1, t3);
+}
+__device__ __forceinline__ void dft8(float2 *v) {
+  const float c = 0.70710678118654752f;
+  float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4(e0, e1, e2, e3);
+  dft4(o0, o1, o2, o3);
+  o1 = make_float2(c * (o1.x + o1.y), c * (o1.y - o1.x));   // * e^{-i pi/4}
+  o2 = mul_mi(o2);                                           // * e^{-i pi/2}
+  o3 = make_float2(c * (o3.y - o3.x), -c * (o3.x + o3.y));  // * e^{-3i pi/4}
+  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+// tw[m] = exp(-2 pi i m / N), m in [0, N).
+__device__ void fft_twiddles(float2 *tw, int N) {
+  for (int m = threadIdx.x; m < N; m += blockDim.x) {
+    float s, c;
+    sincospif(-2.0f * (float)m / (float)N, &s, &c);
+    tw[m] = make_float2(c, s);
+  }
+}
+
+// One Stockham pass of radix R (Govindaraju et al., SC'08, "High performance
+// discrete Fourier transforms on graphics processors"): x -> y.
+template <int R>
+__device__ void stockham_pass(const float2 *x, float2 *y, int N, int Ns, const float2 *tw) {
+  const int T = N / R;
+  const int tstep = N / (Ns * R);
+  for (int j = threadIdx.x; j < T; j += blockDim.x) {
+    const int k = j & (Ns - 1);
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      v[r] = x[j + r * T];
+      if (r) v[r] = cmul(v[r], tw[(r * k * tstep) & (N - 1)]);
+    }
+    if (R == 8) dft8(v);
+    else if (R == 4) dft4(v[0], v[1], v[2], v[3]);
+    else dft2(v);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) y[base + r * Ns] = v[r];
+  }
+}
+
+// Forward FFT of a (length N = 2^m, 4 <= N <= 4096).  Ping-pongs between a
+// and b; returns the buffer that holds the result.  Caller synchronised.
+__device__ float2 *fft_forward(float2 *a, float2 *b, int N, const float2 *tw) {
+  int Ns = 1;
+  int rem = N;
+  while (rem > 1) {
+    if (rem % 8 == 0 && rem != 16 && rem != 32) { stockham_pass<8>(a, b, N, Ns, tw); Ns *= 8; rem /= 8; }
+    else if (rem % 4 == 0) { stockham_pass<4>(a, b, N, Ns, tw); Ns *= 4; rem /= 4; }
+    else { stockham_pass<2>(a, b, N, Ns, tw); Ns *= 2; rem /= 2; }
+    __syncthreads();
+    float2 *t = a; a = b; b = t;
+  }
+  return a;
+}
+
+// ---------------------------------------------------------------- sharpening
+struct SharpenBufs {
+  float2 *a, *b;     // [N] work buffers
+  float2 *tw;        // [N] twiddles (filled by the caller once)
+  float *Ff;         // [N] real Fourier transform of the Gaussian
+};
+
+// E[0..bins) from the fractional histogram H (N4.py:32-101, cudaN4.cu:733-817).
+// H, E in shared memory; all threads of the CTA call it.
+__device__ void sharpen_map(const float *H, int bins, int N, int off, float binMin, float slope,
+                            float wiener, float fwhm, const SharpenBufs &sb, float *E) {
+  const float ln2 = 0.69314718055994531f;
+  const float scaledFWHM = fwhm / slope;
+  const float expFactor = 4.0f * ln2 / (scaledFWHM * scaledFWHM);
+  const float scaleFactor = 2.0f * sqrtf(ln2 / 3.14159265358979324f) / scaledFWHM;
+  // z = V + i F : the padded histogram and the periodic Gaussian in one FFT
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    int d = i <= N / 2 ? i : N - i;
+    float F = scaleFactor * expf(-(float)(d * d) * expFactor);
+    float V = (i >= off && i < off + bins) ? H[i - off] : 0.0f;
+    sb.a[i] = make_float2(V, F);
+  }
+  __syncthreads();
+  float2 *Z = fft_forward(sb.a, sb.b, N, sb.tw);
+  float2 *W = (Z == sb.a) ? sb.b : sb.a;
+  // split the packed transform; Wiener filter Re(conj(Ff)/(|Ff|^2 + w)) with Ff real
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+    float2 zk = Z[k], zn = Z[(N - k) & (N - 1)];
+    float2 Vf = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+    float Ff = 0.5f * (zk.y + zn.y);
+    float g = Ff / (Ff * Ff + wiener);
+    sb.Ff[k] = Ff;
+    // inverse transform by conjugation: store conj(Uf)
+    W[k] = make_float2(Vf.x * g, -Vf.y * g);
+  }
+  __syncthreads();
+  float2 *Y = fft_forward(W, Z, N, sb.tw);
+  float2 *Y2 = (Y == W) ? Z : W;
+  // U = max(Re(ifft(Uf)), 0); pack numerator (real) and U (imaginary)
+  const float invN = 1.0f / (float)N;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    float U = fmaxf(Y[i].x * invN, 0.0f);
+    float c = binMin + (float)(i - off) * slope;
+    Y2[i] = make_float2(c * U, U);
+  }
+  __syncthreads();
+  float2 *P = fft_forward(Y2, Y, N, sb.tw);
+  float2 *P2 = (P == Y2) ? Y : Y2;
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+    float2 v = P[k];
+    float f = sb.Ff[k];
+    P2[k] = make_float2(v.x * f, -v.y * f);   // conj for the inverse transform
+  }
+  __syncthreads();
+  float2 *S = fft_forward(P2, P, N, sb.tw);
+  // smoothed numerator = Re, smoothed denominator = Im (after conj and 1/N)
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+    float2 v = S[off + b];
+    float nu = v.x * invN, de = -v.y * invN;
+    E[b] = (de != 0.0f) ? nu / de : 0.0f;
+  }
+  __syncthreads();
+}
+
+// Fractional histogram contribution of one value (N4.py:21-29), as 2^24
+// fixed-point weights.  Returns the bin or -1 when the value adds nothing.
+__device__ __forceinline__ int hist_bin(float x, float binMin, float slope, int bins,
+                                        unsigned &qlo, unsigned &qhi) {
+  float c = __fdiv_rn(__fsub_rn(x, binMin), slope);
+  float fc = floorf(c);
+  float off = __fsub_rn(c, fc);
+  int idx = (int)fc;
+  if (!(c >= 0.0f) || idx >= bins) return -1;   // NaN / out of range (defensive)
+  if (off == 0.0f) { qlo = 16777216u; qhi = 0u; return idx; }
+  if (idx < bins - 1) {
+    qhi = (unsigned)__float2uint_rn(off * kHistScale);
+    qlo = 16777216u - qhi;
+    return idx;
+  }
+  return -1;                                      // the reference drops it
+}
+
+// Warp-aggregated add of one value into a shared u64 histogram.  All 32
+// lanes must call it (lanes without a value pass key < 0).
+__device__ __forceinline__ void hist_add_warp(unsigned long long *h, int bins, int key,
+                                              unsigned qlo, unsigned qhi) {
+  unsigned grp = __match_any_sync(kFull, key);
+  if (key >= 0) {
+    unsigned slo = __reduce_add_sync(grp, qlo);
+    unsigned shi = __reduce_add_sync(grp, qhi);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(grp) - 1)) {
+      atomicAdd(&h[key], (unsigned long long)slo);
+      if (shi && key + 1 < bins) atomicAdd(&h[key + 1], (unsigned long long)shi);
+    }
+  }
+}
+
+// Piecewise-linear remap through E (N4.py:107-113).
+__device__ __forceinline__ float remap_value(float x, float binMin, float slope, const float *E, int bins) {
+  float c = __fdiv_rn(__fsub_rn(x, binMin), slope);
+  float fc = floorf(c);
+  int idx = (int)fc;
+  if (idx < 0) idx = 0;   // unreachable for x >= binMin; keeps the access in range
+  if (idx < bins - 1) {
+    float e0 = E[idx], e1 = E[idx + 1];
+    return __fadd_rn(e0, __fmul_rn(__fsub_rn(e1, e0), __fsub_rn(c, fc)));
+  }
+  return E[bins - 1];
+}
+
+// Refined lattice value at output index (ox, oy, oz) (array indices), from
+// the (n+3)-point lattice `L` (Lee, Wolberg, Shin 1997 section 4.2;
+// cudaN4.cu:257-339 with its clamped boundary).
+__device__ __forceinline__ void refine_taps(int o, int n, int idx[3], float w[3]) {
+  const int oi = o - 1;                      // lattice coordinate, from -1
+  const int i = (oi >= 0) ? (oi >> 1) : -1;  // floor(oi / 2) for oi >= -1
+  const int par = oi - 2 * i;
+  for (int k = 0; k < 3; ++k) {
+    int c = i - 1 + k;
+    c = c < -1 ? -1 : (c > n + 1 ? n + 1 : c);
+    idx[k] = c + 1;
+  }
+  if (par == 0) { w[0] = 0.125f; w[1] = 0.75f; w[2] = 0.125f; }
+  else          { w[0] = 0.0f;   w[1] = 0.5f;  w[2] = 0.5f; }
+}
+
+__device__ void refine_lattice(const float *L, int ncx, int ncy, int ncz, float *out) {
+  const int nx = ncx - 3, ny = ncy - 3, nz = ncz - 3;
+  const int mx = 2 * nx + 3, my = 2 * ny + 3, mz = 2 * nz + 3;
+  for (int t = threadIdx.x; t < mx * my * mz; t += blockDim.x) {
+    int oz = t % mz, oy = (t / mz) % my, ox = t / (mz * my);
+    int ix[3], iy[3], iz[3];
+    float wx[3], wy[3], wz[3];
+    refine_taps(ox, nx, ix, wx);
+    refine_taps(oy, ny, iy, wy);
+    refine_taps(oz, nz, iz, wz);
+    float acc = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          acc += wx[a] * wy[b] * wz[c] * L[(ix[a] * ncy + iy[b]) * ncz + iz[c]];
+    out[t] = acc;
+  }
+}
+
+// ---------------------------------------------------------------- grid barrier
+// Sense-counting barrier over all CTAs of a cooperative launch.  Every wait
+// is bounded: on timeout (or when another CTA already failed) it records
+// N4_ERR_TIMEOUT in *err and returns false.
+struct GridBarrier {
+  unsigned *count;
+  unsigned *gen;
+  int *err;
+  unsigned nblocks;
+
+  __device__ bool sync() const {
+    __syncthreads();
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+      volatile unsigned *vgen = gen;
+      volatile int *verr = err;
+      int ok = (*verr == 0);
+      unsigned g0 = *vgen;
+      __threadfence();
+      unsigned t = atomicAdd(count, 1u);
+      if (t == nblocks - 1) {
+        atomicExch(count, 0u);
+        __threadfence();
+        atomicAdd(gen, 1u);
+      } else {
+        unsigned long long spins = 0;
+        while (*vgen == g0) {
+          if (*verr != 0) { ok = 0; break; }
+          if (++spins > kSpinLimit) { atomicExch(err, (int)N4_ERR_TIMEOUT); ok = 0; break; }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+      s_ok = ok && (*verr == 0);
+    }
+    __syncthreads();
+    return s_ok != 0;
+  }
+};
+
+}  // namespace n4

@@ -1,0 +1,505 @@
+// The N4 iteration for one volume, executed by a group of CTAs that share
+// the volume's rows (cudaN4.cu:1418-1747, N4.py:276-332).
+//
+// A group is either a thread-block cluster (the volume lives in the
+// cluster's distributed shared memory; partials are exchanged through DSMEM;
+// hardware cluster barriers) or the whole grid of a cooperative launch (the
+// volume lives in global memory/L2; partials are exchanged through global
+// memory; a bounded software barrier).  The algorithm below is written once
+// for both.
+//
+// Per level, with L the control lattice and G/Gd the per-row partial
+// evaluations of L and of the last update D:
+//   pass A  logU = im_log - eval(G), masked min/max, and the convergence
+//           value of the previous update from eval(Gd)       (group reduce)
+//   pass B  fractional histogram of logU                        (group reduce)
+//           Wiener sharpening map E (every CTA, in shared memory)
+//   pass C  residual R = logU - remap(logU)
+//   fit     separable contraction of R with the fit weights     (group reduce)
+//   update  D = num / (den + eps), L += D, G = rows(L), Gd = rows(D)
+#pragma once
+#include <cooperative_groups.h>
+
+#include "n4_device.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace n4 {
+
+// ------------------------------------------------------------------ layout
+// Byte offsets of one CTA's workspace.  "sm" offsets are always in shared
+// memory; "big" offsets are in shared memory for the cluster path and in a
+// per-CTA slice of global memory for the grid path.
+struct Plan {
+  // limits
+  int levels, nc0x, nc0y, nc0z, NCX, NCY, NCZ, NLAT;
+  int Xmax, Ymax, Zmax, slab_floats, rows_max, nvxl;
+  int bins, npad, hoff;
+  // shared
+  int o_ax, o_ay, o_az, o_L, o_D, o_den, o_tmp, o_aux, o_hist, o_H, o_E;
+  int o_fa, o_fb, o_tw, o_ff, o_red, o_misc;
+  int sm_bytes;
+  // big
+  int b_imlog, b_logu, b_G, b_Gd, b_T2, b_slotA, b_slotB, b_slotC, big_bytes;
+};
+
+struct Params {
+  int bins;
+  float wiener, fwhm, thr, eps;
+  int zero_den, ddof1;
+  int iters[N4_MAX_LEVELS];
+};
+
+struct VolJob {
+  int X, Y, Z;                  // fitting-resolution dimensions
+  const float *imlog;           // [X*Y*Z] log intensity, NaN outside the mask
+  float *logu;                  // grid path: [X*Y*Z] scratch
+  const float *warm;            // first-level lattice or nullptr
+  float *lattice_out;           // final lattice
+  n4_report_t *report;
+};
+
+// Statistics exchanged after pass A: min, max, sum y, sum y^2.
+struct Stats { double v[4]; };
+
+// ------------------------------------------------------------------ groups
+struct ClusterGroup {
+  __device__ int rank() const { return (int)cg::this_cluster().block_rank(); }
+  __device__ int size() const { return (int)cg::this_cluster().num_blocks(); }
+  __device__ bool sync() const { cg::this_cluster().sync(); return true; }
+  template <class T> __device__ const T *peer(const T *p, int r) const {
+    return cg::this_cluster().map_shared_rank(const_cast<T *>(p), r);
+  }
+  template <class T> __device__ T load(const T *p) const { return *p; }
+  static constexpr bool kGrid = false;
+};
+
+struct GridGroup {
+  GridBarrier bar;
+  char *big_base;      // per-CTA big regions, stride big_stride
+  size_t big_stride;
+  __device__ int rank() const { return (int)blockIdx.x; }
+  __device__ int size() const { return (int)gridDim.x; }
+  __device__ bool sync() const { return bar.sync(); }
+  template <class T> __device__ const T *peer(const T *p, int r) const {
+    const char *mine = big_base + (size_t)blockIdx.x * big_stride;
+    return (const T *)(big_base + (size_t)r * big_stride + ((const char *)p - mine));
+  }
+  template <class T> __device__ T load(const T *p) const { return __ldcg(p); }
+  static constexpr bool kGrid = true;
+};
+
+// ------------------------------------------------------------------ engine
+template <class Group>
+struct Engine {
+  Group g;
+  const Plan &pl;
+  const Params &pr;
+  char *sm;
+  char *big;
+  float *red_global;   // grid path: [NLAT] / [bins] slice-reduction buffer
+  // volume
+  int X, Y, Z, r0, r1, nrow, rank, K;
+  FastDiv divZ;
+  const float *imlog;
+  float *logu;
+  // level
+  int ncx, ncy, ncz, nlat;
+  Axis ax, ay, az;
+  // smem views
+  float *L, *D, *den, *tmp, *aux, *H, *E, *Ff;
+  unsigned long long *hist;
+  float2 *fa, *fb, *tw;
+  double *red;
+  float *G, *Gd, *T2, *slotC;
+  Stats *slotA;
+  unsigned long long *slotB;
+
+  __device__ Engine(const Group &g_, const Plan &p, const Params &r, char *sm_, char *big_, float *rg)
+      : g(g_), pl(p), pr(r), sm(sm_), big(big_), red_global(rg) {
+    L = (float *)(sm + pl.o_L); D = (float *)(sm + pl.o_D); den = (float *)(sm + pl.o_den);
+    tmp = (float *)(sm + pl.o_tmp); aux = (float *)(sm + pl.o_aux);
+    hist = (unsigned long long *)(sm + pl.o_hist); H = (float *)(sm + pl.o_H); E = (float *)(sm + pl.o_E);
+    fa = (float2 *)(sm + pl.o_fa); fb = (float2 *)(sm + pl.o_fb); tw = (float2 *)(sm + pl.o_tw);
+    Ff = (float *)(sm + pl.o_ff); red = (double *)(sm + pl.o_red);
+    G = (float *)(big + pl.b_G); Gd = (float *)(big + pl.b_Gd); T2 = (float *)(big + pl.b_T2);
+    slotA = (Stats *)(big + pl.b_slotA); slotB = (unsigned long long *)(big + pl.b_slotB);
+    slotC = (float *)(big + pl.b_slotC);
+  }
+
+  // ---- level geometry
+  __device__ void set_level(int level) {
+    ncx = ((pl.nc0x - 3) << level) + 3;
+    ncy = ((pl.nc0y - 3) << level) + 3;
+    ncz = ((pl.nc0z - 3) << level) + 3;
+    nlat = ncx * ncy * ncz;
+    ax = axis_at(sm + pl.o_ax, X, ncx);
+    ay = axis_at(sm + pl.o_ay, Y, ncy);
+    az = axis_at(sm + pl.o_az, Z, ncz);
+    build_axis(ax);
+    build_axis(ay);
+    build_axis(az);
+    __syncthreads();
+  }
+
+  // ---- rows(lat) -> Gt: x/y contraction of the lattice for every local row
+  __device__ void rowtab(const float *lat, float *Gt) {
+    const int ntask = nrow * ncz;
+    for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
+      const int rl = t / ncz, cz = t - rl * ncz;
+      const int row = r0 + rl;
+      const int vx = row / Y, vy = row - vx * Y;
+      const int sx = ax.s[vx], sy = ay.s[vy];
+      const float4 wx = ax.w[vx], wy = ay.w[vy];
+      const float wxa[4] = {wx.x, wx.y, wx.z, wx.w};
+      const float wya[4] = {wy.x, wy.y, wy.z, wy.w};
+      float acc = 0.0f;
+#pragma unroll
+      for (int jx = 0; jx < 4; ++jx) {
+        const float *lp = lat + ((sx + jx) * ncy + sy) * ncz + cz;
+        float s = 0.0f;
+#pragma unroll
+        for (int jy = 0; jy < 4; ++jy) s = __fmaf_rn(wya[jy], lp[jy * ncz], s);
+        acc = __fmaf_rn(wxa[jx], s, acc);
+      }
+      Gt[t] = acc;
+    }
+  }
+
+  __device__ __forceinline__ float eval(const float *Gt, int rl, int vz) const {
+    return dot4(az.w[vz], Gt + rl * ncz + az.s[vz]);
+  }
+
+  // ---- group reductions
+  // Stats: every CTA reads all K slots in the same order.
+  __device__ bool reduce_stats(const double in[4], double out[4]) {
+    if (threadIdx.x == 0) { for (int i = 0; i < 4; ++i) slotA->v[i] = in[i]; }
+    if (!g.sync()) return false;
+    if (threadIdx.x < 32) {
+      float mn = INFINITY, mx = -INFINITY;
+      double s0 = 0.0, s1 = 0.0;
+      for (int k = threadIdx.x; k < K; k += 32) {
+        const Stats *p = g.peer(slotA, k);
+        mn = fminf(mn, (float)g.load(&p->v[0]));
+        mx = fmaxf(mx, (float)g.load(&p->v[1]));
+        s0 += g.load(&p->v[2]);
+        s1 += g.load(&p->v[3]);
+      }
+      mn = warp_min(mn); mx = warp_max(mx); s0 = warp_sum(s0); s1 = warp_sum(s1);
+      if (threadIdx.x == 0) { red[0] = mn; red[1] = mx; red[2] = s0; red[3] = s1; }
+    }
+    __syncthreads();
+    for (int i = 0; i < 4; ++i) out[i] = red[i];
+    __syncthreads();
+    return true;
+  }
+
+  // Sum of every CTA's `mine[0..n)` into `out` (shared), identical in all CTAs.
+  template <class T>
+  __device__ bool allreduce(const T *mine, T *out, int n) {
+    if (!g.sync()) return false;
+    if (!Group::kGrid) {
+      for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        T acc = 0;
+        for (int k = 0; k < K; ++k) acc += g.load(g.peer(mine, k) + c);
+        out[c] = acc;
+      }
+      __syncthreads();
+      return true;
+    }
+    // grid: each CTA reduces a slice into global memory, then all copy it
+    T *rg = (T *)red_global;
+    const int per = (n + K - 1) / K;
+    const int c0 = rank * per, c1 = min(n, c0 + per);
+    for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+      T acc = 0;
+      for (int k = 0; k < K; ++k) acc += g.load(g.peer(mine, k) + c);
+      rg[c] = acc;
+    }
+    if (!g.sync()) return false;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) out[c] = __ldcg(rg + c);
+    __syncthreads();
+    return true;
+  }
+
+  // ---- separable fit contraction of the local rows into slotC (full lattice)
+  // num: values R (logu) with weights p; den: mask with weights q.
+  __device__ void contract(bool num_mode) {
+    float *T1 = Gd;   // Gd is dead between pass A and the next update
+    const float *P = num_mode ? az.p : az.q;
+    const int nt1 = nrow * ncz;
+    for (int t = threadIdx.x; t < nt1; t += blockDim.x) {
+      const int rl = t / ncz, cz = t - rl * ncz;
+      float acc = 0.0f;
+      for (int j = 0; j < 4; ++j) {
+        const int sp = cz - j;
+        if (sp < 0 || sp >= az.nsp) continue;
+        const float *wz = P + j * Z;
+        const int lo = az.lo[sp], hi = az.hi[sp];
+        if (num_mode) {
+          const float *rv = logu + (size_t)rl * Z;
+          for (int vz = lo; vz < hi; ++vz) acc = __fmaf_rn(wz[vz], rv[vz], acc);
+        } else {
+          const float *iv = imlog + (size_t)rl * Z;
+          for (int vz = lo; vz < hi; ++vz) acc += isnan(iv[vz]) ? 0.0f : wz[vz];
+        }
+      }
+      T1[t] = acc;
+    }
+    __syncthreads();
+    const float *PY = num_mode ? ay.p : ay.q;
+    const float *PX = num_mode ? ax.p : ax.q;
+    const int vx0 = r0 / Y, vx1 = (r1 - 1) / Y;
+    const int nvx = vx1 - vx0 + 1;
+    const int nt2 = nvx * ncy * ncz;
+    for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
+      const int cz = t % ncz, cy = (t / ncz) % ncy, xl = t / (ncz * ncy);
+      const int vx = vx0 + xl;
+      const int rbase = vx * Y - r0;        // local row of (vx, 0)
+      float acc = 0.0f;
+      for (int j = 0; j < 4; ++j) {
+        const int sp = cy - j;
+        if (sp < 0 || sp >= ay.nsp) continue;
+        const int lo = max(ay.lo[sp], -rbase), hi = min(ay.hi[sp], nrow - rbase);
+        const float *wy = PY + j * Y;
+        for (int vy = lo; vy < hi; ++vy) acc = __fmaf_rn(wy[vy], T1[(rbase + vy) * ncz + cz], acc);
+      }
+      T2[t] = acc;
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < nlat; c += blockDim.x) {
+      const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
+      float acc = 0.0f;
+      for (int j = 0; j < 4; ++j) {
+        const int sp = cx - j;
+        if (sp < 0 || sp >= ax.nsp) continue;
+        const int lo = max(ax.lo[sp], vx0), hi = min(ax.hi[sp], vx1 + 1);
+        const float *wx = PX + j * X;
+        for (int vx = lo; vx < hi; ++vx)
+          acc = __fmaf_rn(wx[vx], T2[((vx - vx0) * ncy + cy) * ncz + cz], acc);
+      }
+      slotC[c] = acc;
+    }
+  }
+
+  // ---- pass A: logU, masked min/max and the previous update's CV sums
+  __device__ bool pass_a(bool need_cv, double st[4]) {
+    float vmin = INFINITY, vmax = -INFINITY;
+    double sy = 0.0, syy = 0.0;
+    const int n = nrow * Z;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float v = imlog[i];
+      if (isnan(v)) { logu[i] = v; continue; }
+      const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
+      const float lu = __fsub_rn(v, eval(G, rl, vz));
+      logu[i] = lu;
+      vmin = fminf(vmin, lu);
+      vmax = fmaxf(vmax, lu);
+      if (need_cv) {
+        const float y = expm1f(-eval(Gd, rl, vz));
+        sy += (double)y;
+        syy += (double)y * (double)y;
+      }
+    }
+    double loc[4];
+    block_reduce4(vmin, vmax, sy, syy, red + 8, loc);
+    if (threadIdx.x == 0) for (int i = 0; i < 4; ++i) red[4 + i] = loc[i];
+    __syncthreads();
+    for (int i = 0; i < 4; ++i) loc[i] = red[4 + i];
+    __syncthreads();
+    return reduce_stats(loc, st);
+  }
+
+  // ---- pass B + sharpening: histogram of logU over the group, then E
+  __device__ bool pass_b(float bmin, float slope) {
+    const int bins = pr.bins;
+    for (int i = threadIdx.x; i < kHistCopies * bins; i += blockDim.x) hist[i] = 0ull;
+    __syncthreads();
+    unsigned long long *hc = hist + ((threadIdx.x >> 5) % kHistCopies) * bins;
+    const int n = nrow * Z;
+    for (int base = 0; base < n; base += blockDim.x) {
+      const int i = base + threadIdx.x;
+      int key = -1;
+      unsigned qlo = 0, qhi = 0;
+      if (i < n) {
+        const float lu = logu[i];
+        if (!isnan(lu)) key = hist_bin(lu, bmin, slope, bins, qlo, qhi);
+      }
+      hist_add_warp(hc, bins, key, qlo, qhi);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+      unsigned long long s = 0;
+      for (int c = 0; c < kHistCopies; ++c) s += hist[c * bins + b];
+      slotB[b] = s;
+    }
+    unsigned long long *Hs = hist;   // reuse copy 0 for the group sum
+    if (!allreduce(slotB, Hs, bins)) return false;
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (float)((double)Hs[b] * kHistInvScale);
+    __syncthreads();
+    SharpenBufs sb{fa, fb, tw, Ff};
+    sharpen_map(H, bins, pl.npad, pl.hoff, bmin, slope, pr.wiener, pr.fwhm, sb, E);
+    return true;
+  }
+
+  // ---- pass C: residual in place of logU (0 outside the mask)
+  __device__ void pass_c(float bmin, float slope, bool degenerate) {
+    const int n = nrow * Z;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float lu = logu[i];
+      float r = 0.0f;
+      if (!isnan(lu) && !degenerate) r = __fsub_rn(lu, remap_value(lu, bmin, slope, E, pr.bins));
+      logu[i] = r;
+    }
+    __syncthreads();
+  }
+
+  // ---- one sharpen + fit step from the current G; leaves the update in D
+  __device__ bool fit_step(const double st[4]) {
+    const float bmin = (float)st[0], bmax = (float)st[1];
+    const float slope = __fdiv_rn(__fsub_rn(bmax, bmin), (float)(pr.bins - 1));
+    const bool degenerate = !(slope > 0.0f) || isinf(slope);
+    if (!degenerate) { if (!pass_b(bmin, slope)) return false; }
+    pass_c(bmin, slope, degenerate);
+    contract(true);
+    if (!allreduce(slotC, D, nlat)) return false;
+    for (int c = threadIdx.x; c < nlat; c += blockDim.x) {
+      const float nu = D[c], de = den[c];
+      D[c] = pr.zero_den ? (de != 0.0f ? nu / de : 0.0f) : nu / (de + pr.eps);
+    }
+    __syncthreads();
+    return true;
+  }
+
+  __device__ float cv_from(const double st[4], double nfg) const {
+    const double mean_y = st[2] / nfg;
+    double var = st[3] / nfg - mean_y * mean_y;
+    if (pr.ddof1) var = nfg > 1.0 ? var * nfg / (nfg - 1.0) : 0.0;
+    return (float)(sqrt(var > 0.0 ? var : 0.0) / (1.0 + mean_y));
+  }
+
+  // ---- the whole volume
+  __device__ void run(const VolJob &job, const float *imlog_in, float *logu_in) {
+    X = job.X; Y = job.Y; Z = job.Z;
+    rank = g.rank(); K = g.size();
+    const int rows = X * Y;
+    r0 = (int)((long long)rows * rank / K);
+    r1 = (int)((long long)rows * (rank + 1) / K);
+    nrow = r1 - r0;
+    divZ = FastDiv((unsigned)Z);
+    imlog = imlog_in;
+    logu = logu_in;
+    const bool lead = (rank == 0 && threadIdx.x == 0);
+    n4_report_t *rep = job.report;
+
+    fft_twiddles(tw, pl.npad);
+    // foreground count of the group
+    float cnt = 0.0f;
+    double cntd = 0.0;
+    for (int i = threadIdx.x; i < nrow * Z; i += blockDim.x) cnt += isnan(imlog[i]) ? 0.0f : 1.0f;
+    cntd = cnt;
+    double loc[4], st[4];
+    block_reduce4(0.0f, 0.0f, cntd, 0.0, red + 8, loc);
+    if (threadIdx.x == 0) red[4] = loc[2];
+    __syncthreads();
+    loc[0] = 0.0; loc[1] = 0.0; loc[2] = red[4]; loc[3] = 0.0;
+    __syncthreads();
+    if (!reduce_stats(loc, st)) { if (lead) rep->status = N4_ERR_TIMEOUT; return; }
+    const double nfg = st[2];
+    if (lead) { rep->foreground = (long long)nfg; rep->levels = 0; rep->warm_start_used = 0; }
+    if (nfg < 1.0) {
+      if (rank == 0) {
+        for (int c = threadIdx.x; c < pl.NLAT; c += blockDim.x) job.lattice_out[c] = 0.0f;
+        if (threadIdx.x == 0) rep->status = N4_ERR_EMPTY_MASK;
+      }
+      return;
+    }
+
+    // first-level lattice
+    set_level(0);
+    for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] = job.warm ? job.warm[c] : 0.0f;
+    __syncthreads();
+
+    for (int level = 0; level < pl.levels; ++level) {
+      if (level > 0) {
+        const int pcx = ncx, pcy = ncy, pcz = ncz;
+        refine_lattice(L, pcx, pcy, pcz, tmp);
+        __syncthreads();
+        set_level(level);
+        for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] = tmp[c];
+        __syncthreads();
+      }
+      // constant denominator of the fit at this level
+      contract(false);
+      if (!allreduce(slotC, den, nlat)) goto timeout;
+      rowtab(L, G);
+      __syncthreads();
+      const int maxIt = pr.iters[level];
+      int it = 0;
+      float cv = 1e10f;
+      if (level == 0 && job.warm && maxIt > 0) {
+        // warm start: one iteration from the warm lattice and one from zero;
+        // keep the one whose first convergence value is not larger
+        for (int c = threadIdx.x; c < nlat; c += blockDim.x) aux[c] = L[c];   // warm
+        __syncthreads();
+        float cvs[2];
+        for (int arm = 0; arm < 2; ++arm) {
+          for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] = arm == 0 ? aux[c] : 0.0f;
+          __syncthreads();
+          rowtab(L, G);
+          __syncthreads();
+          if (!pass_a(false, st)) goto timeout;
+          if (!fit_step(st)) goto timeout;
+          rowtab(D, Gd);
+          for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] += D[c];
+          __syncthreads();
+          rowtab(L, G);
+          __syncthreads();
+          if (!pass_a(true, st)) goto timeout;
+          cvs[arm] = cv_from(st, nfg);
+          if (arm == 0) {   // keep the warm result in aux, its update in tmp
+            for (int c = threadIdx.x; c < nlat; c += blockDim.x) { aux[c] = L[c]; tmp[c] = D[c]; }
+            __syncthreads();
+          }
+        }
+        const bool use_warm = cvs[0] <= cvs[1];
+        if (use_warm) {
+          for (int c = threadIdx.x; c < nlat; c += blockDim.x) { L[c] = aux[c]; D[c] = tmp[c]; }
+          __syncthreads();
+          rowtab(L, G);
+          rowtab(D, Gd);
+          __syncthreads();
+        }
+        cv = use_warm ? cvs[0] : cvs[1];
+        it = 1;
+        if (lead) {
+          rep->warm_start_used = use_warm ? 1 : 0;
+          rep->first_cv_warm = cvs[0];
+          rep->first_cv_plain = cvs[1];
+        }
+      }
+      for (;;) {
+        if (!pass_a(it > 0, st)) goto timeout;
+        if (it > 0) cv = cv_from(st, nfg);
+        if (!(cv > pr.thr) || it >= maxIt) break;
+        if (!fit_step(st)) goto timeout;
+        for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] += D[c];
+        __syncthreads();
+        rowtab(D, Gd);
+        rowtab(L, G);
+        __syncthreads();
+        ++it;
+      }
+      if (lead) { rep->iterations[level] = it; rep->final_cv[level] = cv; rep->levels = level + 1; }
+    }
+    if (rank == 0) {
+      for (int c = threadIdx.x; c < nlat; c += blockDim.x) job.lattice_out[c] = L[c];
+      if (threadIdx.x == 0) rep->status = N4_OK;
+    }
+    return;
+  timeout:
+    if (lead) rep->status = N4_ERR_TIMEOUT;
+  }
+};
+
+}  // namespace n4

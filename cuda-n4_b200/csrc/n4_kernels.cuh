@@ -1,0 +1,493 @@
+// Kernels of n4b200 (sm_100a).
+//
+//   k_prologue        full resolution -> fitting grid: threshold, shrink, log
+//                     (cudaN4.cu:639-652, 131-147; N4.py:284-287)
+//   k_n4_cluster      persistent N4 over a queue of volumes, one thread-block
+//                     cluster per volume, the volume resident in DSMEM
+//   k_n4_grid         N4 on one large volume with the whole GPU
+//   k_axis_tables     per-axis B-spline tables in global memory
+//   k_correct         final dense evaluation at full resolution fused with
+//                     im / exp(b) and the optional exp(b) output
+//                     (cudaN4.cu:1697-1729, N4.py:329-330)
+//   k_fit_*           standalone separable B-spline fit (FitBspline3D)
+//   k_refine          lattice refinement (upsampleLattice3D_gpu)
+//   k_minmax/k_hist/k_sharpen/k_remap   standalone sharpenImage
+//   k_cv              standalone convergence measurement
+#pragma once
+#include "n4_engine.cuh"
+
+namespace n4 {
+
+// ------------------------------------------------------------------ prologue
+struct PrologueVol {
+  const float *im, *mask;   // full resolution (mask may be null)
+  float *im_w, *mask_w;     // optional in-place threshold write-back
+  int FX, FY, FZ, s;        // full dims, shrink
+  int X, Y, Z;              // fitting dims
+  float *imlog;             // [X*Y*Z]
+  long long start;          // first fitting voxel of this volume in the batch
+};
+
+__device__ __forceinline__ int find_volume(const long long *starts, int n, long long gi) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) { int m = (lo + hi + 1) >> 1; if (starts[m] <= gi) lo = m; else hi = m - 1; }
+  return lo;
+}
+
+__global__ void k_prologue(const PrologueVol *vols, const long long *starts, int nvol,
+                           long long total, float low, int *flag_nonfinite) {
+  for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < total;
+       gi += (long long)gridDim.x * blockDim.x) {
+    const int v = find_volume(starts, nvol, gi);
+    const PrologueVol &P = vols[v];
+    const long long li = gi - P.start;
+    const int z = (int)(li % P.Z), y = (int)((li / P.Z) % P.Y), x = (int)(li / ((long long)P.Z * P.Y));
+    const int s = P.s;
+    float out;
+    if (s == 1) {
+      const float val = P.im[li];
+      const bool m = (P.mask ? P.mask[li] != 0.0f : true) && val > low;
+      if (m && !isfinite(val)) atomicExch(flag_nonfinite, 1);
+      out = m ? logf(val) : __int_as_float(0x7fc00000);
+      if (P.im_w && !(val > low)) { P.im_w[li] = 0.0f; if (P.mask_w) P.mask_w[li] = 0.0f; }
+    } else {
+      float sum = 0.0f;
+      int cnt = 0;
+      for (int dx = 0; dx < s; ++dx)
+        for (int dy = 0; dy < s; ++dy) {
+          const long long rowb = ((long long)(x * s + dx) * P.FY + (y * s + dy)) * P.FZ + (long long)z * s;
+          for (int dz = 0; dz < s; ++dz) {
+            const float val = P.im[rowb + dz];
+            const bool m = (P.mask ? P.mask[rowb + dz] != 0.0f : true) && val > low;
+            if (m) { sum += val; ++cnt; if (!isfinite(val)) atomicExch(flag_nonfinite, 1); }
+          }
+        }
+      const float mean = cnt ? sum / (float)cnt : 0.0f;
+      out = (2 * cnt > s * s * s && mean > low) ? logf(mean) : __int_as_float(0x7fc00000);
+    }
+    P.imlog[li] = out;
+  }
+}
+
+// In-place threshold of the caller's full-resolution buffers (shrink > 1).
+__global__ void k_threshold_inplace(float *im, float *mask, long long n, float low) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (!(im[i] > low)) { im[i] = 0.0f; if (mask) mask[i] = 0.0f; }
+  }
+}
+
+// ------------------------------------------------------------------ N4 kernels
+__device__ __forceinline__ void row_range(int rows, int rank, int K, int &r0, int &r1) {
+  r0 = (int)((long long)rows * rank / K);
+  r1 = (int)((long long)rows * (rank + 1) / K);
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// Bounded wait for the given phase of an mbarrier; 1 when it completed.
+__device__ unsigned mbar_wait(unsigned long long *mbar, unsigned phase) {
+  unsigned done = 0;
+  unsigned long long spins = 0;
+  while (!done) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(mbar)), "r"(phase)
+        : "memory");
+    if (!done && ++spins > kSpinLimit) break;
+  }
+  return done;
+}
+
+// Copy `nfl` floats from global `src` into shared memory with 1-D bulk
+// (TMA) copies; returns the shared pointer at which src[0] landed.  The
+// global buffer must be readable up to 16 bytes past its end.  Every wait is
+// bounded; returns nullptr on timeout.
+__device__ float *stage_slab(const float *src, int nfl, float *dst_base, unsigned long long *mbar,
+                             unsigned &phase, bool use_tma) {
+  if (!use_tma) {
+    for (int i = threadIdx.x; i < nfl; i += blockDim.x) dst_base[i] = src[i];
+    __syncthreads();
+    return dst_base;
+  }
+  const uintptr_t sa = (uintptr_t)src;
+  const int mis = (int)((sa & 15u) >> 2);
+  const char *src_al = (const char *)(sa & ~(uintptr_t)15);
+  const unsigned bytes = (unsigned)(((mis + nfl) * 4 + 15) & ~15);
+  if (threadIdx.x == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+                 : "memory");
+    const unsigned chunk = 32768;
+    for (unsigned off = 0; off < bytes; off += chunk) {
+      const unsigned sz = bytes - off < chunk ? bytes - off : chunk;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_u32((char *)dst_base + off)),
+          "l"(src_al + off), "r"(sz), "r"(smem_u32(mbar))
+          : "memory");
+    }
+  }
+  const unsigned done = mbar_wait(mbar, phase);
+  phase ^= 1u;
+  __syncthreads();
+  return done ? dst_base + mis : nullptr;
+}
+
+struct ClusterArgs {
+  Plan pl;
+  Params pr;
+  const VolJob *jobs;
+  const int *order;
+  int njobs;
+  int *queue;
+  int use_tma;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) k_n4_cluster(const __grid_constant__ ClusterArgs a) {
+  extern __shared__ __align__(128) char smem[];
+  __shared__ Plan s_pl;
+  __shared__ Params s_pr;
+  __shared__ int s_job;
+  __shared__ __align__(8) unsigned long long s_mbar;
+  if (threadIdx.x == 0) {
+    s_pl = a.pl;
+    s_pr = a.pr;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_mbar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  ClusterGroup g;
+  char *sm = smem;
+  char *big = smem + s_pl.sm_bytes;
+  unsigned phase = 0;
+  for (;;) {
+    if (g.rank() == 0 && threadIdx.x == 0) s_job = atomicAdd(a.queue, 1);
+    g.sync();
+    const int j = *g.peer(&s_job, 0);
+    g.sync();
+    if (j >= a.njobs) break;
+    const VolJob &job = a.jobs[a.order[j]];
+    int r0, r1;
+    row_range(job.X * job.Y, g.rank(), g.size(), r0, r1);
+    float *slab = stage_slab(job.imlog + (size_t)r0 * job.Z, (r1 - r0) * job.Z,
+                             (float *)(big + s_pl.b_imlog), &s_mbar, phase, a.use_tma != 0);
+    int ok = slab != nullptr;
+    if (!ok && threadIdx.x == 0) job.report->status = N4_ERR_TIMEOUT;
+    // all CTAs of the cluster must agree before starting the volume
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) s_ok = ok;
+    g.sync();
+    int all_ok = 1;
+    for (int k = 0; k < g.size(); ++k) all_ok &= *g.peer(&s_ok, k);
+    g.sync();
+    if (!all_ok) {
+      // a bulk copy did not complete in time: wait once more (bounded) for
+      // this CTA's copies still in flight, then stop taking volumes
+      if (!ok) mbar_wait(&s_mbar, phase ^ 1u);
+      break;
+    }
+    Engine<ClusterGroup> e(g, s_pl, s_pr, sm, big, nullptr);
+    e.run(job, slab, (float *)(big + s_pl.b_logu));
+  }
+}
+
+struct GridArgs {
+  Plan pl;
+  Params pr;
+  VolJob job;
+  char *big_base;
+  size_t big_stride;
+  GridBarrier bar;
+  float *red_global;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) k_n4_grid(const __grid_constant__ GridArgs a) {
+  extern __shared__ __align__(128) char smem[];
+  __shared__ Plan s_pl;
+  __shared__ Params s_pr;
+  if (threadIdx.x == 0) { s_pl = a.pl; s_pr = a.pr; }
+  __syncthreads();
+  GridGroup g{a.bar, a.big_base, a.big_stride};
+  char *big = a.big_base + (size_t)blockIdx.x * a.big_stride;
+  int r0, r1;
+  row_range(a.job.X * a.job.Y, g.rank(), g.size(), r0, r1);
+  Engine<GridGroup> e(g, s_pl, s_pr, smem, big, a.red_global);
+  e.run(a.job, a.job.imlog + (size_t)r0 * a.job.Z, a.job.logu + (size_t)r0 * a.job.Z);
+}
+
+// ------------------------------------------------------------------ tables
+struct TableJob {
+  char *base;     // axis table memory
+  int n, nc;
+};
+
+__global__ void k_axis_tables(const TableJob *jobs) {
+  const TableJob t = jobs[blockIdx.x];
+  build_axis(axis_at(t.base, t.n, t.nc));
+}
+
+// ------------------------------------------------------------------ final correction
+struct CorrectVol {
+  const float *im;       // full resolution input (null: output the log field)
+  float *out;            // im / exp(b)  or b
+  float *bias;           // optional exp(b)
+  const float *lattice;
+  char *tx, *ty, *tz;    // axis tables (full resolution, final lattice)
+  int FX, FY, FZ, ncx, ncy, ncz;
+  long long tile0;       // first row tile of this volume in the batch
+  int vec4;              // FZ % 4 == 0 and every pointer 16-byte aligned
+};
+
+constexpr int kRowsPerTile = 16;
+constexpr int kMaxNcz = 64;
+
+// One CTA per tile of kRowsPerTile full-resolution rows: x/y-contract the
+// lattice for its rows into shared memory, then evaluate z per voxel with
+// float4 I/O.  HBM traffic: read im, write out (+ bias).
+__global__ void __launch_bounds__(256) k_correct(const CorrectVol *vols, const long long *tile_starts,
+                                                 int nvol, float low) {
+  __shared__ float Gs[kRowsPerTile * kMaxNcz];
+  const int v = find_volume(tile_starts, nvol, blockIdx.x);
+  const CorrectVol &C = vols[v];
+  const Axis ax = axis_at(C.tx, C.FX, C.ncx), ay = axis_at(C.ty, C.FY, C.ncy), az = axis_at(C.tz, C.FZ, C.ncz);
+  const long long rows = (long long)C.FX * C.FY;
+  const long long row0 = (blockIdx.x - C.tile0) * (long long)kRowsPerTile;
+  const int nr = (int)min((long long)kRowsPerTile, rows - row0);
+  const int ncz = C.ncz, ncy = C.ncy;
+  for (int t = threadIdx.x; t < nr * ncz; t += blockDim.x) {
+    const int r = t / ncz, cz = t - r * ncz;
+    const long long row = row0 + r;
+    const int vx = (int)(row / C.FY), vy = (int)(row - (long long)vx * C.FY);
+    const int sx = ax.s[vx], sy = ay.s[vy];
+    const float4 wx = ax.w[vx], wy = ay.w[vy];
+    const float wxa[4] = {wx.x, wx.y, wx.z, wx.w}, wya[4] = {wy.x, wy.y, wy.z, wy.w};
+    float acc = 0.0f;
+#pragma unroll
+    for (int jx = 0; jx < 4; ++jx) {
+      const float *lp = C.lattice + ((sx + jx) * ncy + sy) * ncz + cz;
+      float s = 0.0f;
+#pragma unroll
+      for (int jy = 0; jy < 4; ++jy) s = __fmaf_rn(wya[jy], __ldg(lp + jy * ncz), s);
+      acc = __fmaf_rn(wxa[jx], s, acc);
+    }
+    Gs[t] = acc;
+  }
+  __syncthreads();
+  const int FZ = C.FZ;
+  const long long base = row0 * FZ;
+  if (C.vec4) {
+    const int nz4 = FZ >> 2;
+    for (int t = threadIdx.x; t < nr * nz4; t += blockDim.x) {
+      const int r = t / nz4, z4 = (t - r * nz4) * 4;
+      const long long off = base + (long long)r * FZ + z4;
+      float bz[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) bz[k] = dot4(az.w[z4 + k], Gs + r * ncz + az.s[z4 + k]);
+      if (C.im) {
+        const float4 x = __ldcs((const float4 *)(C.im + off));
+        const float xa[4] = {x.x, x.y, x.z, x.w};
+        float o[4], e[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { e[k] = expf(bz[k]); o[k] = xa[k] > low ? xa[k] / e[k] : 0.0f; }
+        __stcs((float4 *)(C.out + off), make_float4(o[0], o[1], o[2], o[3]));
+        if (C.bias) __stcs((float4 *)(C.bias + off), make_float4(e[0], e[1], e[2], e[3]));
+      } else {
+        __stcs((float4 *)(C.out + off), make_float4(bz[0], bz[1], bz[2], bz[3]));
+      }
+    }
+  } else {
+    for (int t = threadIdx.x; t < nr * FZ; t += blockDim.x) {
+      const int r = t / FZ, z = t - r * FZ;
+      const long long off = base + (long long)r * FZ + z;
+      const float b = dot4(az.w[z], Gs + r * ncz + az.s[z]);
+      if (C.im) {
+        const float x = C.im[off];
+        const float e = expf(b);
+        C.out[off] = x > low ? x / e : 0.0f;
+        if (C.bias) C.bias[off] = e;
+      } else {
+        C.out[off] = b;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ standalone fit
+// T1[row][cz] (numerator and denominator) for every row of the field.
+__global__ void k_fit_rows(const float *field, const float *mask, int X, int Y, int Z, Axis az,
+                           float *t1n, float *t1d) {
+  const int ncz = az.nc;
+  const long long ntask = (long long)X * Y * ncz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntask;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long row = t / ncz;
+    const int cz = (int)(t - row * ncz);
+    const float *f = field + row * Z;
+    const float *m = mask ? mask + row * Z : nullptr;
+    float an = 0.0f, ad = 0.0f;
+    for (int j = 0; j < 4; ++j) {
+      const int sp = cz - j;
+      if (sp < 0 || sp >= az.nsp) continue;
+      for (int vz = az.lo[sp]; vz < az.hi[sp]; ++vz) {
+        if (m && m[vz] == 0.0f) continue;
+        an = __fmaf_rn(az.p[j * Z + vz], f[vz], an);
+        ad += az.q[j * Z + vz];
+      }
+    }
+    t1n[t] = an;
+    t1d[t] = ad;
+  }
+}
+
+// T2[vx][cy][cz] from T1.
+__global__ void k_fit_planes(const float *t1n, const float *t1d, int X, int Y, Axis ay, int ncz,
+                             float *t2n, float *t2d) {
+  const int ncy = ay.nc;
+  const long long ntask = (long long)X * ncy * ncz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntask;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int cz = (int)(t % ncz), cy = (int)((t / ncz) % ncy);
+    const long long vx = t / ((long long)ncz * ncy);
+    float an = 0.0f, ad = 0.0f;
+    for (int j = 0; j < 4; ++j) {
+      const int sp = cy - j;
+      if (sp < 0 || sp >= ay.nsp) continue;
+      for (int vy = ay.lo[sp]; vy < ay.hi[sp]; ++vy) {
+        const long long i = (vx * Y + vy) * ncz + cz;
+        an = __fmaf_rn(ay.p[j * Y + vy], t1n[i], an);
+        ad = __fmaf_rn(ay.q[j * Y + vy], t1d[i], ad);
+      }
+    }
+    t2n[t] = an;
+    t2d[t] = ad;
+  }
+}
+
+__global__ void k_fit_final(const float *t2n, const float *t2d, int X, Axis ax, int ncy, int ncz,
+                            float eps, int zero_den, float *lattice) {
+  const int ncx = ax.nc;
+  const int nlat = ncx * ncy * ncz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nlat; c += gridDim.x * blockDim.x) {
+    const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
+    float an = 0.0f, ad = 0.0f;
+    for (int j = 0; j < 4; ++j) {
+      const int sp = cx - j;
+      if (sp < 0 || sp >= ax.nsp) continue;
+      for (int vx = ax.lo[sp]; vx < ax.hi[sp]; ++vx) {
+        const long long i = ((long long)vx * ncy + cy) * ncz + cz;
+        an = __fmaf_rn(ax.p[j * X + vx], t2n[i], an);
+        ad = __fmaf_rn(ax.q[j * X + vx], t2d[i], ad);
+      }
+    }
+    lattice[c] = zero_den ? (ad != 0.0f ? an / ad : 0.0f) : an / (ad + eps);
+  }
+}
+
+__global__ void k_refine(const float *in, int ncx, int ncy, int ncz, float *out) {
+  refine_lattice(in, ncx, ncy, ncz, out);
+}
+
+// ------------------------------------------------------------------ standalone sharpen
+__global__ void k_minmax(const float *x, const float *mask, long long n, float *part) {
+  float vmin = INFINITY, vmax = -INFINITY;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (mask && mask[i] == 0.0f) continue;
+    vmin = fminf(vmin, x[i]);
+    vmax = fmaxf(vmax, x[i]);
+  }
+  __shared__ double scratch[160];
+  double out[4];
+  block_reduce4(vmin, vmax, 0.0, 0.0, scratch + 8, out);
+  if (threadIdx.x == 0) { part[2 * blockIdx.x] = (float)out[0]; part[2 * blockIdx.x + 1] = (float)out[1]; }
+}
+
+// stats[0] = min, stats[1] = max, stats[2] = slope
+__global__ void k_minmax_final(const float *part, int nb, int bins, float *stats) {
+  float vmin = INFINITY, vmax = -INFINITY;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) { vmin = fminf(vmin, part[2 * i]); vmax = fmaxf(vmax, part[2 * i + 1]); }
+  __shared__ double scratch[160];
+  double out[4];
+  block_reduce4(vmin, vmax, 0.0, 0.0, scratch + 8, out);
+  if (threadIdx.x == 0) {
+    stats[0] = (float)out[0];
+    stats[1] = (float)out[1];
+    stats[2] = __fdiv_rn(__fsub_rn((float)out[1], (float)out[0]), (float)(bins - 1));
+  }
+}
+
+__global__ void k_hist(const float *x, const float *mask, long long n, const float *stats, int bins,
+                       unsigned long long *hist) {
+  extern __shared__ unsigned long long hs[];
+  for (int i = threadIdx.x; i < bins; i += blockDim.x) hs[i] = 0ull;
+  __syncthreads();
+  const float bmin = stats[0], slope = stats[2];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = blockIdx.x * (long long)blockDim.x; base < n; base += stride) {
+    const long long i = base + threadIdx.x;
+    int key = -1;
+    unsigned qlo = 0, qhi = 0;
+    if (i < n && slope > 0.0f && (!mask || mask[i] != 0.0f)) key = hist_bin(x[i], bmin, slope, bins, qlo, qhi);
+    hist_add_warp(hs, bins, key, qlo, qhi);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < bins; i += blockDim.x)
+    if (hs[i]) atomicAdd(&hist[i], hs[i]);
+}
+
+__global__ void k_sharpen(const unsigned long long *hist, const float *stats, int bins, int npad, int hoff,
+                          float wiener, float fwhm, float *E_out) {
+  extern __shared__ __align__(16) char sm[];
+  float2 *fa = (float2 *)sm, *fb = fa + npad, *tw = fb + npad;
+  float *Ff = (float *)(tw + npad);
+  float *H = Ff + npad;
+  float *E = H + bins;
+  fft_twiddles(tw, npad);
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (float)((double)hist[b] * kHistInvScale);
+  __syncthreads();
+  if (stats[2] > 0.0f) {
+    SharpenBufs sb{fa, fb, tw, Ff};
+    sharpen_map(H, bins, npad, hoff, stats[0], stats[2], wiener, fwhm, sb, E);
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) E_out[b] = E[b];
+  } else {
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) E_out[b] = 0.0f;
+  }
+}
+
+__global__ void k_remap(const float *x, const float *mask, long long n, const float *stats, const float *E,
+                        int bins, float *out) {
+  const float bmin = stats[0], slope = stats[2];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (mask && mask[i] == 0.0f) { out[i] = 0.0f; continue; }
+    out[i] = slope > 0.0f ? remap_value(x[i], bmin, slope, E, bins) : x[i];
+  }
+}
+
+// ------------------------------------------------------------------ standalone convergence
+__global__ void k_cv(const float *f1, const float *f2, const float *mask, long long n, double *part) {
+  double s0 = 0.0, s1 = 0.0, c = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (mask && mask[i] == 0.0f) continue;
+    const double y = (double)expm1f(__fsub_rn(f1[i], f2[i]));
+    s0 += y; s1 += y * y; c += 1.0;
+  }
+  s0 = warp_sum(s0); s1 = warp_sum(s1); c = warp_sum(c);
+  __shared__ double ws[3][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { ws[0][wid] = s0; ws[1][wid] = s1; ws[2][wid] = c; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0, d = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { a += ws[0][w]; b += ws[1][w]; d += ws[2][w]; }
+    part[3 * blockIdx.x] = a;
+    part[3 * blockIdx.x + 1] = b;
+    part[3 * blockIdx.x + 2] = d;
+  }
+}
+
+}  // namespace n4

@@ -1,0 +1,373 @@
+"""n4b200: N4 bias-field correction on NVIDIA B200, drop-in for the reference
+CUDA-N4 interface.
+
+The functions mirror the reference entry points (``cudaN4.h``) and its
+numpy twin (``N4.py``) by name and argument meaning:
+
+=================================  ==========================================
+here                               reference
+=================================  ==========================================
+``N4Param``                        ``struct N4Param`` (cudaN4.h:24-94)
+``N4``                             ``N4()`` / ``testN4()`` (cudaN4.h:343-387),
+                                   ``N4()`` (N4.py:276-332)
+``N4Batch``                        (new) many volumes in one launch
+``FitBspline3D``                   ``FitBspline3D`` (cudaN4.h:313, N4.py:186)
+``EvaluateBspline3D``              ``EvaluateBspline3D`` (cudaN4.h:288, N4.py:241)
+``UpsampleLattice3D``              ``upsampleLattice3D_gpu`` (cudaN4.h:269), N4.py:132
+``sharpenImage``                   ``sharpenImage`` (cudaN4.h:198, N4.py:9)
+``CalculateConvergenceMeasurement````calculateConvergenceMeasurement`` (cudaN4.h:249),
+                                   N4.py:121
+=================================  ==========================================
+
+Every call goes through ``libn4b200.so`` (hand-written sm_100a kernels); there
+is no CPU fallback.  Inputs may be CUDA tensors (device path, outputs are
+CUDA tensors) or numpy arrays (host path, outputs are numpy arrays).
+Volumes are float32 ``[fx][fy][fz]`` with the last axis fastest.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import N4Error, check, n4_params_t, n4_report_t, n4_volume_t
+
+__all__ = [
+    "N4Param", "N4", "N4Batch", "N4Result", "Context", "FitBspline3D",
+    "EvaluateBspline3D", "UpsampleLattice3D", "upsampleLattice3D", "sharpenImage",
+    "CalculateConvergenceMeasurement", "calculateConvergenceMeasurement", "N4Error",
+    "lattice_dims", "library",
+]
+
+
+def library():
+    """The loaded ``libn4b200.so`` (raises ImportError when it is not built)."""
+    return _lib.load()
+
+
+# ---------------------------------------------------------------- parameters
+class N4Param:
+    """Parameters of N4, with the field names of the reference's ``N4Param``.
+
+    Defaults are the reference's (``cudaN4.h:24-94``), including
+    ``low_value = 10``; synthetic phantoms with intensities around 1 need
+    ``low_value = 0``.  ``MaximumNumberOfIterations`` is one count for every
+    level (the CUDA reference) or a list with one count per level (N4.py).
+    """
+
+    _FIELDS = ("NumberOfHistogramBins", "WienerFilterNoise", "BiasFieldFullWidthAtHalfMaximum",
+               "NumberOfControlPoints_x", "NumberOfControlPoints_y", "NumberOfControlPoints_z",
+               "NumberOfFittingLevels", "MaximumNumberOfIterations", "ConvergenceThreshold",
+               "low_value", "ShrinkFactor", "SplineOrder", "FitEpsilon", "flags")
+
+    def __init__(self, **kw):
+        c = n4_params_t()
+        _lib.load().n4_params_default(C.byref(c))
+        self.NumberOfHistogramBins = c.NumberOfHistogramBins
+        self.WienerFilterNoise = c.WienerFilterNoise
+        self.BiasFieldFullWidthAtHalfMaximum = c.BiasFieldFullWidthAtHalfMaximum
+        self.NumberOfControlPoints_x = c.NumberOfControlPoints_x
+        self.NumberOfControlPoints_y = c.NumberOfControlPoints_y
+        self.NumberOfControlPoints_z = c.NumberOfControlPoints_z
+        self.NumberOfFittingLevels = c.NumberOfFittingLevels
+        self.MaximumNumberOfIterations = c.MaximumNumberOfIterations[0]
+        self.ConvergenceThreshold = c.ConvergenceThreshold
+        self.low_value = c.low_value
+        self.ShrinkFactor = c.ShrinkFactor
+        self.SplineOrder = c.SplineOrder
+        self.FitEpsilon = c.FitEpsilon
+        self.flags = c.flags
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+    def __setattr__(self, k, v):
+        if k == "NumberOfControlPoints":
+            for a in ("x", "y", "z"):
+                object.__setattr__(self, f"NumberOfControlPoints_{a}", int(v))
+            return
+        if k not in self._FIELDS:
+            raise AttributeError(f"N4Param has no field {k!r}")
+        object.__setattr__(self, k, v)
+
+    def to_c(self) -> n4_params_t:
+        c = n4_params_t()
+        for k in self._FIELDS:
+            if k == "MaximumNumberOfIterations":
+                it = self.MaximumNumberOfIterations
+                its = [int(it)] * _lib.N4_MAX_LEVELS if np.isscalar(it) else list(it)
+                if len(its) < self.NumberOfFittingLevels:
+                    raise ValueError("one iteration count per fitting level is required")
+                its = (its + [0] * _lib.N4_MAX_LEVELS)[:_lib.N4_MAX_LEVELS]
+                c.MaximumNumberOfIterations[:] = [int(i) for i in its]
+            else:
+                setattr(c, k, getattr(self, k))
+        return c
+
+    def lattice_dims(self):
+        return lattice_dims(self)
+
+    def __repr__(self):
+        return "N4Param(" + ", ".join(f"{k}={getattr(self, k)!r}" for k in self._FIELDS) + ")"
+
+
+def lattice_dims(param: N4Param):
+    """Control points per axis at the last level (``cudaN4.h:359``)."""
+    dims = (C.c_uint * 3)()
+    n = C.c_size_t()
+    c = param.to_c()
+    check(_lib.load().n4_lattice_dims(C.byref(c), dims, C.byref(n)))
+    return tuple(int(d) for d in dims)
+
+
+# ---------------------------------------------------------------- context
+class Context:
+    """Owns the device workspaces of n4b200 (``n4_create`` / ``n4_destroy``)."""
+
+    _default = {}
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        self.device = device
+        check(_lib.load().n4_create(C.byref(self._h), device))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            _lib.load().n4_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @classmethod
+    def default(cls, device: int = 0) -> "Context":
+        if device not in cls._default:
+            cls._default[device] = cls(device)
+        return cls._default[device]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _is_cuda(x) -> bool:
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        return False
+    return isinstance(x, torch.Tensor) and x.is_cuda
+
+
+def _dev_f32(x, device=None):
+    """CUDA float32 contiguous tensor view/copy of x (numpy or tensor)."""
+    torch = _torch()
+    if isinstance(x, torch.Tensor):
+        t = x
+        if not t.is_cuda:
+            t = t.to(device or "cuda")
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(x, dtype=np.float32))).to(device or "cuda")
+    if t.dtype != torch.float32:
+        t = t.float()
+    return t.contiguous()
+
+
+def _ptr(t) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _stream(device=None) -> int:
+    return _torch().cuda.current_stream(device).cuda_stream
+
+
+def _ctx_for(t, ctx):
+    return ctx or Context.default(t.device.index or 0)
+
+
+# ---------------------------------------------------------------- N4
+@dataclass
+class N4Result:
+    im_normalized: object
+    lattice: object
+    bias_field: object = None
+    report: dict = field(default_factory=dict)
+
+
+def _report_dict(r: n4_report_t) -> dict:
+    lv = r.levels
+    return dict(status=_lib.STATUS.get(r.status, r.status), levels=lv,
+                iterations=list(r.iterations[:lv]), final_cv=list(r.final_cv[:lv]),
+                warm_start_used=bool(r.warm_start_used), first_cv_warm=r.first_cv_warm,
+                first_cv_plain=r.first_cv_plain, foreground=r.foreground,
+                path={1: "cluster", 2: "grid"}.get(r.path, r.path), cluster_size=r.cluster_size)
+
+
+def N4(im, mask=None, param: Optional[N4Param] = None, warm_lattice=None, return_bias=False,
+       ctx: Optional[Context] = None, synchronous: bool = True) -> N4Result:
+    """Bias-correct one volume.
+
+    ``im``/``mask``: float32 ``[fx][fy][fz]`` (mask != 0 is foreground; None
+    = every voxel).  CUDA tensors run on their device and stream; numpy arrays
+    take the host path (``n4_run_host``).  Returns the corrected volume, the
+    final control lattice and, with ``return_bias``, ``exp(log bias)``.
+    """
+    param = param or N4Param()
+    cpar = param.to_c()
+    fx, fy, fz = (int(d) for d in im.shape)
+    dims = lattice_dims(param)
+    lib = _lib.load()
+    rep = n4_report_t()
+    if _is_cuda(im):
+        torch = _torch()
+        imt = _dev_f32(im)
+        mk = None if mask is None else _dev_f32(mask, imt.device)
+        wl = None if warm_lattice is None else _dev_f32(warm_lattice, imt.device)
+        out = torch.empty_like(imt)
+        lat = torch.empty(dims, dtype=torch.float32, device=imt.device)
+        bias = torch.empty_like(imt) if return_bias else None
+        c = _ctx_for(imt, ctx)
+        st = lib.n4_run(c.handle, C.byref(cpar), _ptr(imt), _ptr(mk), fx, fy, fz, _ptr(out), _ptr(lat),
+                        _ptr(bias), _ptr(wl), _stream(imt.device), C.byref(rep) if synchronous else None)
+        check(st)
+        return N4Result(out, lat, bias, _report_dict(rep) if synchronous else {})
+    imh = np.ascontiguousarray(np.asarray(im, dtype=np.float32))
+    mkh = None if mask is None else np.ascontiguousarray(np.asarray(mask, dtype=np.float32))
+    wlh = None if warm_lattice is None else np.ascontiguousarray(np.asarray(warm_lattice, dtype=np.float32))
+    out = np.empty_like(imh)
+    lat = np.empty(dims, dtype=np.float32)
+    bias = np.empty_like(imh) if return_bias else None
+    c = ctx or Context.default(0)
+    p = lambda a: None if a is None else a.ctypes.data
+    st = lib.n4_run_host(c.handle, C.byref(cpar), p(imh), p(mkh), fx, fy, fz, p(out), p(lat), p(bias), p(wlh),
+                         C.byref(rep))
+    check(st)
+    return N4Result(out, lat, bias, _report_dict(rep))
+
+
+def N4Batch(volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=None, return_bias=False,
+            ctx: Optional[Context] = None, synchronous: bool = True):
+    """Bias-correct many volumes (CUDA tensors, any sizes) in one persistent
+    launch.  ``volumes``: sequence of ``(im, mask)``.  Returns a list of
+    ``N4Result``."""
+    torch = _torch()
+    param = param or N4Param()
+    cpar = param.to_c()
+    dims = lattice_dims(param)
+    n = len(volumes)
+    arr = (n4_volume_t * n)()
+    keep, results = [], []
+    dev = None
+    for i, (im, mask) in enumerate(volumes):
+        imt = _dev_f32(im)
+        dev = imt.device
+        mk = None if mask is None else _dev_f32(mask, dev)
+        wl = None if warm_lattices is None or warm_lattices[i] is None else _dev_f32(warm_lattices[i], dev)
+        out = torch.empty_like(imt)
+        lat = torch.empty(dims, dtype=torch.float32, device=dev)
+        bias = torch.empty_like(imt) if return_bias else None
+        keep += [imt, mk, wl]
+        fx, fy, fz = (int(d) for d in imt.shape)
+        arr[i] = n4_volume_t(_ptr(imt), _ptr(mk), fx, fy, fz, _ptr(out), _ptr(lat), _ptr(bias), _ptr(wl))
+        results.append(N4Result(out, lat, bias, {}))
+    reps = (n4_report_t * n)()
+    c = ctx or Context.default(dev.index or 0)
+    st = _lib.load().n4_run_batched(c.handle, C.byref(cpar), n, arr, _stream(dev), reps if synchronous else None)
+    check(st)
+    if synchronous:
+        for r, rep in zip(results, reps):
+            r.report = _report_dict(rep)
+    return results
+
+
+# ---------------------------------------------------------------- components
+def _out_like(x, t):
+    return t if _is_cuda(x) else t.cpu().numpy()
+
+
+def FitBspline3D(field, mask, numberOfControlPoints, eps: float = 1e-3, zero_den: bool = False,
+                 ctx: Optional[Context] = None):
+    """Lattice fitted to ``field`` over ``mask != 0`` (``N4.py:186-237``;
+    ``zero_den`` gives ``cudaN4.cu:123-127``'s division)."""
+    torch = _torch()
+    f = _dev_f32(field)
+    m = None if mask is None else _dev_f32(mask, f.device)
+    nc = tuple(int(c) for c in numberOfControlPoints)
+    lat = torch.empty(nc, dtype=torch.float32, device=f.device)
+    X, Y, Z = f.shape
+    check(_lib.load().n4_fit_bspline3d(_ctx_for(f, ctx).handle, _ptr(f), _ptr(m), *nc, X, Y, Z, float(eps),
+                                       int(bool(zero_den)), _ptr(lat), _stream(f.device)))
+    return _out_like(field, lat)
+
+
+def EvaluateBspline3D(lattice, numberOfControlPoints, size, ctx: Optional[Context] = None):
+    """Dense evaluation of the lattice on ``size`` voxels (``N4.py:241-273``)."""
+    torch = _torch()
+    L = _dev_f32(lattice)
+    nc = tuple(int(c) for c in numberOfControlPoints)
+    X, Y, Z = (int(s) for s in size)
+    out = torch.empty((X, Y, Z), dtype=torch.float32, device=L.device)
+    check(_lib.load().n4_evaluate_bspline3d(_ctx_for(L, ctx).handle, _ptr(L), *nc, X, Y, Z, _ptr(out),
+                                            _stream(L.device)))
+    return _out_like(lattice, out)
+
+
+def UpsampleLattice3D(lattice, ctx: Optional[Context] = None):
+    """(n+3) -> (2n+3) control points per axis (``N4.py:132-165``)."""
+    torch = _torch()
+    L = _dev_f32(lattice)
+    nx, ny, nz = (int(s) for s in L.shape)
+    out = torch.empty((2 * nx - 3, 2 * ny - 3, 2 * nz - 3), dtype=torch.float32, device=L.device)
+    check(_lib.load().n4_upsample_lattice3d(_ctx_for(L, ctx).handle, _ptr(L), nx, ny, nz, _ptr(out),
+                                            _stream(L.device)))
+    return _out_like(lattice, out)
+
+
+upsampleLattice3D = UpsampleLattice3D
+
+
+def sharpenImage(im_before_sharpen, mask, numberOfHistogramBins: int = 200, WienerFilterNoise: float = 0.01,
+                 BiasFieldFullWidthAtHalfMaximum: float = 0.15, details: bool = False,
+                 ctx: Optional[Context] = None):
+    """Histogram sharpening of a log image over the mask (``N4.py:9-118``).
+    With ``details`` also returns ``dict(binMin, binMax, E)``."""
+    torch = _torch()
+    x = _dev_f32(im_before_sharpen)
+    m = None if mask is None else _dev_f32(mask, x.device)
+    out = torch.empty_like(x)
+    bmin, bmax = C.c_float(), C.c_float()
+    E = np.zeros(int(numberOfHistogramBins), dtype=np.float32)
+    torch.cuda.synchronize(x.device)
+    check(_lib.load().n4_sharpen_image(_ctx_for(x, ctx).handle, _ptr(x), _ptr(m), x.numel(),
+                                       int(numberOfHistogramBins), float(WienerFilterNoise),
+                                       float(BiasFieldFullWidthAtHalfMaximum), _ptr(out), C.byref(bmin),
+                                       C.byref(bmax), E.ctypes.data))
+    res = _out_like(im_before_sharpen, out)
+    if details:
+        return res, dict(binMin=bmin.value, binMax=bmax.value, E=E)
+    return res
+
+
+def CalculateConvergenceMeasurement(field1, field2, mask, ddof: int = 0, ctx: Optional[Context] = None) -> float:
+    """std / mean of exp(field1 - field2) over the mask (``N4.py:121-126``;
+    ``ddof=1`` is ``cudaN4.cu:979``)."""
+    a = _dev_f32(field1)
+    b = _dev_f32(field2, a.device)
+    m = None if mask is None else _dev_f32(mask, a.device)
+    out = C.c_double()
+    _torch().cuda.synchronize(a.device)
+    check(_lib.load().n4_convergence(_ctx_for(a, ctx).handle, _ptr(a), _ptr(b), _ptr(m), a.numel(), int(ddof),
+                                     C.byref(out)))
+    return out.value
+
+
+calculateConvergenceMeasurement = CalculateConvergenceMeasurement

@@ -1,0 +1,128 @@
+"""ctypes binding of the C ABI declared in ``include/n4b200.h``.
+
+Loading fails loudly when ``libn4b200.so`` has not been built: there is no
+CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+N4_MAX_LEVELS = 8
+
+N4_OK = 0
+STATUS = {
+    0: "N4_OK", 1: "N4_ERR_INVALID_ARG", 2: "N4_ERR_UNSUPPORTED_SPLINE_ORDER",
+    3: "N4_ERR_EMPTY_MASK", 4: "N4_ERR_OOM", 5: "N4_ERR_CUDA", 6: "N4_ERR_TIMEOUT",
+    7: "N4_ERR_NONFINITE", 8: "N4_ERR_TOO_LARGE", 9: "N4_ERR_NO_DEVICE",
+}
+
+FLAG_CV_DDOF1 = 0x1
+FLAG_FIT_ZERO_DEN = 0x2
+FLAG_INPLACE_THRESH = 0x4
+FLAG_FORCE_GRID = 0x8
+FLAG_FORCE_CLUSTER = 0x10
+
+
+class n4_params_t(C.Structure):
+    _fields_ = [
+        ("NumberOfHistogramBins", C.c_uint),
+        ("WienerFilterNoise", C.c_float),
+        ("BiasFieldFullWidthAtHalfMaximum", C.c_float),
+        ("NumberOfControlPoints_x", C.c_uint),
+        ("NumberOfControlPoints_y", C.c_uint),
+        ("NumberOfControlPoints_z", C.c_uint),
+        ("NumberOfFittingLevels", C.c_uint),
+        ("MaximumNumberOfIterations", C.c_uint * N4_MAX_LEVELS),
+        ("ConvergenceThreshold", C.c_float),
+        ("low_value", C.c_float),
+        ("ShrinkFactor", C.c_uint),
+        ("SplineOrder", C.c_uint),
+        ("FitEpsilon", C.c_float),
+        ("flags", C.c_uint),
+    ]
+
+
+class n4_report_t(C.Structure):
+    _fields_ = [
+        ("status", C.c_int),
+        ("levels", C.c_int),
+        ("iterations", C.c_int * N4_MAX_LEVELS),
+        ("final_cv", C.c_float * N4_MAX_LEVELS),
+        ("warm_start_used", C.c_int),
+        ("first_cv_warm", C.c_float),
+        ("first_cv_plain", C.c_float),
+        ("foreground", C.c_longlong),
+        ("path", C.c_int),
+        ("cluster_size", C.c_int),
+    ]
+
+
+class n4_volume_t(C.Structure):
+    _fields_ = [
+        ("im", C.c_void_p), ("mask", C.c_void_p),
+        ("fx", C.c_uint), ("fy", C.c_uint), ("fz", C.c_uint),
+        ("im_normalized", C.c_void_p), ("lattice", C.c_void_p),
+        ("bias_field", C.c_void_p), ("warm_lattice", C.c_void_p),
+    ]
+
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libn4b200.so")
+
+# (name, restype, argtypes) of every exported entry point of include/n4b200.h
+_P = C.c_void_p
+_U = C.c_uint
+SIGNATURES = [
+    ("n4_params_default", None, [C.POINTER(n4_params_t)]),
+    ("n4_lattice_dims", C.c_int, [C.POINTER(n4_params_t), C.POINTER(C.c_uint), C.POINTER(C.c_size_t)]),
+    ("n4_status_string", C.c_char_p, [C.c_int]),
+    ("n4_last_error_string", C.c_char_p, []),
+    ("n4_version", C.c_char_p, []),
+    ("n4_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
+    ("n4_destroy", C.c_int, [_P]),
+    ("n4_run", C.c_int, [_P, C.POINTER(n4_params_t), _P, _P, _U, _U, _U, _P, _P, _P, _P, _P,
+                         C.POINTER(n4_report_t)]),
+    ("n4_run_host", C.c_int, [_P, C.POINTER(n4_params_t), _P, _P, _U, _U, _U, _P, _P, _P, _P,
+                              C.POINTER(n4_report_t)]),
+    ("n4_run_batched", C.c_int, [_P, C.POINTER(n4_params_t), C.c_int, C.POINTER(n4_volume_t), _P,
+                                 C.POINTER(n4_report_t)]),
+    ("n4_sync", C.c_int, [_P, C.POINTER(n4_report_t), C.c_int]),
+    ("n4_fit_bspline3d", C.c_int, [_P, _P, _P, _U, _U, _U, _U, _U, _U, C.c_float, C.c_int, _P, _P]),
+    ("n4_evaluate_bspline3d", C.c_int, [_P, _P, _U, _U, _U, _U, _U, _U, _P, _P]),
+    ("n4_upsample_lattice3d", C.c_int, [_P, _P, _U, _U, _U, _P, _P]),
+    ("n4_sharpen_image", C.c_int, [_P, _P, _P, _U, _U, C.c_float, C.c_float, _P,
+                                   C.POINTER(C.c_float), C.POINTER(C.c_float), _P]),
+    ("n4_convergence", C.c_int, [_P, _P, _P, _P, _U, C.c_int, C.POINTER(C.c_double)]),
+]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (once) and declare every entry point."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build it with `python cuda-n4_b200/n4b200/build.py` "
+            "(n4b200 has no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class N4Error(RuntimeError):
+    def __init__(self, status: int, message: str = ""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+
+
+def check(status: int):
+    if status != N4_OK:
+        msg = load().n4_last_error_string().decode(errors="replace")
+        raise N4Error(status, msg)

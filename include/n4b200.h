@@ -1,0 +1,174 @@
+/*
+ * n4b200 - N4 bias-field correction for NVIDIA B200 (sm_100a).
+ *
+ * C ABI.  Plain pointers and sizes only; every call returns an n4_status_t
+ * and never exits or traps.  Volumes are float32, row-major [fx][fy][fz]
+ * with fz fastest, exactly the layout of the reference N4 (cudaN4.cu:476).
+ * A mask voxel is foreground when it is non-zero (float masks, as in the
+ * reference) or when its byte is non-zero (uint8 masks).
+ *
+ * Device-pointer calls are asynchronous on the given stream (NULL = the
+ * legacy default stream) unless a report is requested; host-pointer calls
+ * are synchronous.  One context per host thread; a context owns every
+ * workspace, so no call allocates inside the iteration loop.
+ */
+#ifndef N4B200_H
+#define N4B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define N4_MAX_LEVELS 8
+
+typedef enum {
+  N4_OK = 0,
+  N4_ERR_INVALID_ARG = 1,
+  N4_ERR_UNSUPPORTED_SPLINE_ORDER = 2,
+  N4_ERR_EMPTY_MASK = 3,
+  N4_ERR_OOM = 4,
+  N4_ERR_CUDA = 5,
+  N4_ERR_TIMEOUT = 6,        /* a bounded device-side wait gave up */
+  N4_ERR_NONFINITE = 7,      /* non-finite intensity inside the mask */
+  N4_ERR_TOO_LARGE = 8,      /* request exceeds a documented limit */
+  N4_ERR_NO_DEVICE = 9
+} n4_status_t;
+
+/* Flags (n4_params_t.flags).  Defaults follow N4.py. */
+#define N4_FLAG_CV_DDOF1        0x1u  /* CV standard deviation over N-1 (cudaN4.cu:979)          */
+#define N4_FLAG_FIT_ZERO_DEN    0x2u  /* lattice = den != 0 ? num/den : 0 (cudaN4.cu:123-127)     */
+#define N4_FLAG_INPLACE_THRESH  0x4u  /* write im = mask = 0 where im <= low_value back into the   */
+                                      /* caller's buffers, as the reference does (cudaN4.cu:1459) */
+#define N4_FLAG_FORCE_GRID      0x8u  /* run the whole-GPU path even when a cluster path fits      */
+#define N4_FLAG_FORCE_CLUSTER   0x10u /* fail with N4_ERR_TOO_LARGE rather than use the grid path */
+
+/* Mirrors N4Param (cudaN4.h:24-94).  Obtain defaults from n4_params_default. */
+typedef struct {
+  unsigned int NumberOfHistogramBins;            /* 200                                */
+  float WienerFilterNoise;                       /* 0.01                               */
+  float BiasFieldFullWidthAtHalfMaximum;         /* 0.15                               */
+  unsigned int NumberOfControlPoints_x;          /* 4 (first level)                    */
+  unsigned int NumberOfControlPoints_y;          /* 4                                  */
+  unsigned int NumberOfControlPoints_z;          /* 4                                  */
+  unsigned int NumberOfFittingLevels;            /* 4                                  */
+  unsigned int MaximumNumberOfIterations[N4_MAX_LEVELS]; /* 50 at every level          */
+  float ConvergenceThreshold;                    /* 0.001                              */
+  float low_value;                               /* 10 (reference default)             */
+  unsigned int ShrinkFactor;                     /* 1 (not in the reference)           */
+  unsigned int SplineOrder;                      /* 3; no other order is supported     */
+  float FitEpsilon;                              /* 1e-3: num/(den+eps) as in N4.py    */
+  unsigned int flags;                            /* N4_FLAG_*                          */
+} n4_params_t;
+
+/* Per-volume outcome. */
+typedef struct {
+  int status;                                    /* n4_status_t                        */
+  int levels;                                    /* levels run                         */
+  int iterations[N4_MAX_LEVELS];                 /* iterations run per level           */
+  float final_cv[N4_MAX_LEVELS];                 /* last convergence value per level   */
+  int warm_start_used;                           /* 1 if the warm lattice was kept     */
+  float first_cv_warm, first_cv_plain;           /* first-iteration CVs (warm start)   */
+  long long foreground;                          /* masked voxels at fitting resolution*/
+  int path;                                      /* 1 = cluster, 2 = whole-GPU grid    */
+  int cluster_size;                              /* CTAs per volume                    */
+} n4_report_t;
+
+/* One volume of a batch (device pointers). */
+typedef struct {
+  const float *im;            /* [fx][fy][fz]                                    */
+  const float *mask;          /* float mask or NULL (NULL = every voxel)         */
+  unsigned int fx, fy, fz;
+  float *im_normalized;       /* [fx][fy][fz] output                             */
+  float *lattice;             /* final lattice, n4_lattice_size() floats         */
+  float *bias_field;          /* optional exp(log bias) output, may be NULL      */
+  const float *warm_lattice;  /* optional first-level lattice, may be NULL       */
+} n4_volume_t;
+
+typedef struct n4_context n4_context_t;
+
+/* Defaults of N4Param (cudaN4.h:24-94). */
+void n4_params_default(n4_params_t *p);
+
+/* Number of control points per axis at the last level and their product
+ * (cudaN4.h:359, main.cpp:87-92). */
+n4_status_t n4_lattice_dims(const n4_params_t *p, unsigned int dims[3], size_t *count);
+
+const char *n4_status_string(int status);
+/* Message of the last failed call on this thread. */
+const char *n4_last_error_string(void);
+const char *n4_version(void);
+
+n4_status_t n4_create(n4_context_t **ctx, int device);
+n4_status_t n4_destroy(n4_context_t *ctx);
+
+/*
+ * Whole N4 on one volume, device pointers.  Replaces
+ *   void N4(float *d_im, float *d_mask, unsigned fx, fy, fz, N4Param&, N4Data&,
+ *           float *d_im_normalized, float *d_lattice, float *d_biasField)
+ * (cudaN4.h:343-365).  Inputs are not modified unless N4_FLAG_INPLACE_THRESH.
+ * `stream` is a cudaStream_t.  With `report` non-NULL the call waits for the
+ * result and returns the volume's status; with NULL it only enqueues.
+ */
+n4_status_t n4_run(n4_context_t *ctx, const n4_params_t *p,
+                   const float *d_im, const float *d_mask,
+                   unsigned int fx, unsigned int fy, unsigned int fz,
+                   float *d_im_normalized, float *d_lattice, float *d_bias_field,
+                   const float *d_warm_lattice, void *stream, n4_report_t *report);
+
+/* Host-pointer twin; replaces testN4 (cudaN4.h:367-387).  Synchronous. */
+n4_status_t n4_run_host(n4_context_t *ctx, const n4_params_t *p,
+                        const float *h_im, const float *h_mask,
+                        unsigned int fx, unsigned int fy, unsigned int fz,
+                        float *h_im_normalized, float *h_lattice, float *h_bias_field,
+                        const float *h_warm_lattice, n4_report_t *report);
+
+/* Many volumes of uneven sizes in one persistent launch (no counterpart in
+ * the reference, which corrects one volume per call).  `reports` (n entries)
+ * may be NULL for a fully asynchronous call. */
+n4_status_t n4_run_batched(n4_context_t *ctx, const n4_params_t *p, int n,
+                           const n4_volume_t *vols, void *stream, n4_report_t *reports);
+
+/* Wait for the context's last asynchronous run and fill its reports. */
+n4_status_t n4_sync(n4_context_t *ctx, n4_report_t *reports, int n);
+
+/* ---- components (unit-level parity with the reference's entry points) ---- */
+
+/* Replaces FitBspline3D (cudaN4.h:313-325): lattice[ncpt] fitted to `field`
+ * over the voxels where mask != 0.  eps as n4_params_t.FitEpsilon;
+ * zero_den selects N4_FLAG_FIT_ZERO_DEN semantics. */
+n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const float *d_mask,
+                             unsigned int ncpt_x, unsigned int ncpt_y, unsigned int ncpt_z,
+                             unsigned int fx, unsigned int fy, unsigned int fz,
+                             float eps, int zero_den, float *d_lattice, void *stream);
+
+/* Replaces EvaluateBspline3D (cudaN4.h:288-298). */
+n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice,
+                                  unsigned int ncpt_x, unsigned int ncpt_y, unsigned int ncpt_z,
+                                  unsigned int fx, unsigned int fy, unsigned int fz,
+                                  float *d_fitted, void *stream);
+
+/* Replaces upsampleLattice3D_gpu (cudaN4.h:269-276): (n+3) -> (2n+3) per axis. */
+n4_status_t n4_upsample_lattice3d(n4_context_t *ctx, const float *d_lattice,
+                                  unsigned int ncpt_x, unsigned int ncpt_y, unsigned int ncpt_z,
+                                  float *d_lattice_upsample, void *stream);
+
+/* Replaces sharpenImage (cudaN4.h:198-234): histogram sharpening of the log
+ * image over the mask; masked-out voxels of the output are 0.  Optional
+ * outputs: bin range and the n_bins-entry intensity map E.  Synchronous. */
+n4_status_t n4_sharpen_image(n4_context_t *ctx, const float *d_before, const float *d_mask,
+                             unsigned int n, unsigned int bins, float wiener, float fwhm,
+                             float *d_after, float *bin_min, float *bin_max, float *h_E);
+
+/* Replaces calculateConvergenceMeasurement (cudaN4.h:249-257): std/mean of
+ * exp(field1 - field2) over the mask, ddof 0 (N4.py) or 1 (cudaN4).
+ * Synchronous; the result is returned, not written into the threshold. */
+n4_status_t n4_convergence(n4_context_t *ctx, const float *d_field1, const float *d_field2,
+                           const float *d_mask, unsigned int n, int ddof, double *cv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* N4B200_H */

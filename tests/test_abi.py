@@ -1,0 +1,98 @@
+"""The C ABI loads and exports every symbol include/n4b200.h declares, and
+its host-side logic (defaults, sizes, validation) works without a GPU."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "n4b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(n4_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_the_entry_points():
+    names = declared_functions()
+    for n in ("n4_run", "n4_run_host", "n4_run_batched", "n4_fit_bspline3d", "n4_evaluate_bspline3d",
+              "n4_upsample_lattice3d", "n4_sharpen_image", "n4_convergence", "n4_create", "n4_destroy"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    import n4b200
+    from n4b200 import _lib
+    lib = n4b200.library()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+    # and the binding declares exactly those
+    assert sorted(n for n, _, _ in _lib.SIGNATURES) == declared_functions()
+
+
+def test_struct_layouts_match_header():
+    from n4b200 import _lib
+    # n4_params_t: 7 x 4 B + 8 x 4 B + 6 x 4 B
+    assert C.sizeof(_lib.n4_params_t) == 4 * (7 + 8 + 6)
+    assert C.sizeof(_lib.n4_report_t) == 4 * 2 + 4 * 8 * 2 + 4 * 3 + 4 + 8 + 4 * 2
+
+
+def test_defaults_match_reference_n4param():
+    """Defaults of N4Param (cudaN4.h:24-94)."""
+    import n4b200
+    p = n4b200.N4Param()
+    assert p.NumberOfHistogramBins == 200
+    assert p.WienerFilterNoise == pytest.approx(0.01)
+    assert p.BiasFieldFullWidthAtHalfMaximum == pytest.approx(0.15)
+    assert (p.NumberOfControlPoints_x, p.NumberOfControlPoints_y, p.NumberOfControlPoints_z) == (4, 4, 4)
+    assert p.NumberOfFittingLevels == 4
+    assert p.MaximumNumberOfIterations == 50
+    assert p.ConvergenceThreshold == pytest.approx(0.001)
+    assert p.low_value == pytest.approx(10.0)
+    assert p.SplineOrder == 3 and p.ShrinkFactor == 1
+
+
+def test_lattice_dims():
+    """(2^(L-1)(ncpt-3)+3) per axis, cudaN4.h:359 / main.cpp:87-91."""
+    import n4b200
+    assert n4b200.lattice_dims(n4b200.N4Param()) == (11, 11, 11)
+    p = n4b200.N4Param(NumberOfFittingLevels=3, NumberOfControlPoints_x=5)
+    assert n4b200.lattice_dims(p) == (11, 7, 7)
+
+
+def test_validation_without_a_gpu():
+    import n4b200
+    from n4b200 import N4Error
+    with pytest.raises(N4Error, match="UNSUPPORTED_SPLINE_ORDER"):
+        n4b200.lattice_dims(n4b200.N4Param(SplineOrder=2))
+    with pytest.raises(N4Error, match="INVALID_ARG"):
+        n4b200.lattice_dims(n4b200.N4Param(NumberOfHistogramBins=1))
+    with pytest.raises(N4Error, match="INVALID_ARG"):
+        n4b200.lattice_dims(n4b200.N4Param(NumberOfControlPoints=3))
+    with pytest.raises(N4Error, match="TOO_LARGE"):
+        n4b200.lattice_dims(n4b200.N4Param(NumberOfFittingLevels=8))
+    with pytest.raises(AttributeError):
+        n4b200.N4Param(NotAField=1)
+
+
+def test_status_strings():
+    import n4b200
+    lib = n4b200.library()
+    assert lib.n4_status_string(3) == b"empty mask"
+    assert lib.n4_version().startswith(b"n4b200")
+
+
+def test_create_reports_missing_device():
+    """n4_create returns a status instead of crashing when no GPU is visible."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    import n4b200
+    lib = n4b200.library()
+    h = C.c_void_p()
+    assert lib.n4_create(C.byref(h), 0) == 9   # N4_ERR_NO_DEVICE
+    assert lib.n4_destroy(None) == 0

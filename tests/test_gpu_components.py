@@ -1,0 +1,110 @@
+"""Component kernels (through the C ABI) against N4.py's golden vectors.
+
+Tolerance: the kernels compute in FP32 against FP64 references, so results
+are compared relative to the reference's largest magnitude
+(``max|gpu - ref| / max|ref|``) with the bound stated per test.
+"""
+import numpy as np
+import pytest
+
+import n4_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def nrel(a, b):
+    a = a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+    return float(np.abs(a.astype(np.float64) - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_fit(cuda, golden_components, k):
+    import n4b200
+    g = golden_components
+    f, m, nc = g[f"fit_field_{k}"], g[f"fit_mask_{k}"], g[f"fit_ncpt_{k}"]
+    lat = n4b200.FitBspline3D(cuda.tensor(f, dtype=cuda.float32, device="cuda"),
+                              cuda.tensor(m, dtype=cuda.float32, device="cuda"), nc)
+    assert nrel(lat, g[f"fit_out_{k}"]) < 1e-5
+
+
+def test_fit_zero_den_semantics(cuda):
+    """cudaN4.cu:123-127: control points without support get 0."""
+    import n4b200
+    rng = np.random.default_rng(1)
+    f = rng.normal(size=(20, 16, 12))
+    m = np.zeros_like(f)
+    m[:10] = 1.0                      # the upper half of x has no voxels
+    a = n4b200.FitBspline3D(f, m, (7, 5, 5), zero_den=True)
+    ref = O.FitBspline3D(f, m, (7, 5, 5), zero_den=True)
+    assert nrel(a, ref) < 1e-5
+    assert np.all(np.asarray(a)[-1] == 0.0)
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_evaluate(cuda, golden_components, k):
+    import n4b200
+    g = golden_components
+    nc, shape = g[f"fit_ncpt_{k}"], g[f"fit_field_{k}"].shape
+    out = n4b200.EvaluateBspline3D(cuda.tensor(g[f"eval_lat_{k}"], dtype=cuda.float32, device="cuda"), nc, shape)
+    assert nrel(out, g[f"eval_out_{k}"]) < 1e-5
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 48), (37, 29, 23), (256, 256, 176)])
+def test_evaluate_sizes(cuda, shape):
+    """float4 (z % 4 == 0) and scalar paths, full-resolution size."""
+    import n4b200
+    rng = np.random.default_rng(2)
+    lat = rng.normal(0, 0.3, size=(11, 11, 11))
+    out = n4b200.EvaluateBspline3D(lat, lat.shape, shape)
+    assert nrel(out, O.EvaluateBspline3D(lat, lat.shape, shape)) < 1e-5
+
+
+@pytest.mark.parametrize("n", [4, 5, 7])
+def test_upsample(cuda, golden_components, n):
+    import n4b200
+    g = golden_components
+    out = n4b200.UpsampleLattice3D(g[f"up_in_{n}"])
+    assert nrel(out, g[f"up_out_{n}"]) < 1e-6
+
+
+def test_upsample_anisotropic(cuda):
+    import n4b200
+    lat = np.random.default_rng(5).normal(size=(4, 6, 5))
+    assert nrel(n4b200.UpsampleLattice3D(lat), O.UpsampleLattice3D(lat)) < 1e-6
+
+
+@pytest.mark.parametrize("tag,fwhm", [("a", 0.15), ("b", 0.3)])
+@pytest.mark.parametrize("bins", [200, 64])
+def test_sharpen(cuda, golden_components, tag, fwhm, bins):
+    import n4b200
+    g = golden_components
+    x = g["sharp_in"].astype(np.float32)
+    out, det = n4b200.sharpenImage(x, g["sharp_mask"], bins, 0.01, fwhm, details=True)
+    # same FP32 input through the FP64 oracle, and the N4.py golden output
+    ref = O.sharpenImage(x.astype(np.float64), g["sharp_mask"], bins, 0.01, fwhm)
+    assert nrel(out, ref) < 2e-5
+    assert nrel(out, g[f"sharp_out_{tag}{bins}"]) < 1e-4
+    m = g["sharp_mask"] != 0
+    assert det["binMin"] == x[m].min() and det["binMax"] == x[m].max()
+
+
+def test_sharpen_map_matches_oracle(cuda, golden_components):
+    import n4b200
+    g = golden_components
+    x = g["sharp_in"].astype(np.float32)
+    m = g["sharp_mask"]
+    _, det = n4b200.sharpenImage(x, m, 200, 0.01, 0.15, details=True)
+    _, od = O.sharpenImage(x.astype(np.float64), m, 200, 0.01, 0.15, details=True)
+    E = det["E"].astype(np.float64)
+    live = od["H"] > 0          # bins that voxels actually map through
+    assert np.abs(E - od["E"])[live].max() / np.abs(od["E"]).max() < 2e-5
+
+
+def test_convergence(cuda, golden_components):
+    import n4b200
+    g = golden_components
+    cv = n4b200.CalculateConvergenceMeasurement(g["cv_f1"], g["cv_f2"], g["cv_mask"])
+    assert cv == pytest.approx(float(g["cv_out"]), rel=1e-4)
+    cv1 = n4b200.CalculateConvergenceMeasurement(g["cv_f1"], g["cv_f2"], g["cv_mask"], ddof=1)
+    ref1 = O.CalculateConvergenceMeasurement(g["cv_f1"], g["cv_f2"], g["cv_mask"], ddof=1)
+    assert cv1 == pytest.approx(ref1, rel=1e-4)

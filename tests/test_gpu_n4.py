@@ -1,0 +1,245 @@
+"""Whole-N4 parity through the C ABI against the FP64 oracle and N4.py.
+
+Tolerance (from the target): corrected volume and log bias field within
+1e-4 relative of the FP64 reference, measured as
+``max|gpu - ref| / max|ref|``; the lattice to the same bound.  Iteration
+counts must match exactly where the reference stops on the threshold.
+"""
+import numpy as np
+import pytest
+
+import n4_oracle as O
+from n4b200.phantom import make_phantom
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def nrel(a, b):
+    a = a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+    return float(np.abs(a.astype(np.float64) - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def param(levels, iters, thr, **kw):
+    import n4b200
+    return n4b200.N4Param(NumberOfFittingLevels=levels, MaximumNumberOfIterations=list(iters),
+                          ConvergenceThreshold=thr, low_value=0.0, **kw)
+
+
+def log_bias(lat, shape):
+    return O.EvaluateBspline3D(np.asarray(lat, dtype=np.float64), np.shape(lat), shape)
+
+
+@pytest.mark.parametrize("tag", ["fixed", "thresh"])
+@pytest.mark.parametrize("force", [0, 0x8])
+def test_small_vs_reference_n4py(cuda, golden_small, tag, force):
+    """Against N4.py itself (golden), cluster path and whole-GPU path."""
+    import n4b200
+    s = golden_small
+    levels, iters, thr = int(s[f"{tag}_levels"]), list(s[f"{tag}_iters"]), float(s[f"{tag}_thr"])
+    im = cuda.tensor(s[f"{tag}_im"], device="cuda")
+    mk = cuda.tensor(s[f"{tag}_mask"], device="cuda")
+    res = n4b200.N4(im, mk, param(levels, iters, thr, flags=force), return_bias=True)
+    rep = {}
+    O.N4(s[f"{tag}_im"], s[f"{tag}_mask"], low_value=0, maximumNumberOfLevels=levels,
+         maximumNumberOfIterations=iters, ConvergenceThreshold=thr, report=rep)
+    assert res.report["status"] == "N4_OK"
+    assert res.report["iterations"] == rep["iterations"]
+    assert res.report["path"] == ("grid" if force else "cluster")
+    lat_ref = s[f"{tag}_lattice"]
+    assert nrel(res.lattice, lat_ref) < TOL
+    assert nrel(log_bias(res.lattice.cpu().numpy(), im.shape), log_bias(lat_ref, im.shape)) < TOL
+    assert nrel(res.im_normalized, s[f"{tag}_norm"]) < TOL
+    b = res.bias_field.cpu().numpy()
+    assert nrel(np.log(b), log_bias(lat_ref, im.shape)) < TOL
+
+
+def test_c1_fixed_iterations(cuda, golden_c1):
+    """64x64x48 phantom, 3 levels x 50 iterations, against N4.py's run."""
+    import n4b200
+    g = golden_c1
+    ph = make_phantom((64, 64, 48), seed=int(g["seed"]), sigma=0.03, grid=4, coeff_std=0.15)
+    res = n4b200.N4(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"),
+                    param(3, [50, 50, 50], 0.0))
+    assert res.report["iterations"] == [50, 50, 50]
+    assert nrel(res.lattice, g["lattice"]) < TOL
+    assert nrel(res.im_normalized.cpu().numpy().reshape(-1)[::97], g["norm_sample"]) < TOL
+
+
+@pytest.mark.parametrize("force", [0, 0x8])
+def test_c1_against_oracle(cuda, force):
+    ph = make_phantom((64, 64, 48), seed=1, sigma=0.03, grid=4, coeff_std=0.15)
+    import n4b200
+    res = n4b200.N4(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"),
+                    param(3, [12, 12, 12], 0.0, flags=force))
+    out, lat, lb = O.N4(ph.im, ph.mask, low_value=0, maximumNumberOfLevels=3,
+                        maximumNumberOfIterations=[12, 12, 12], ConvergenceThreshold=0.0,
+                        return_log_bias=True)
+    assert nrel(res.lattice, lat) < TOL
+    assert nrel(log_bias(res.lattice.cpu().numpy(), ph.im.shape), lb) < TOL
+    assert nrel(res.im_normalized, out) < TOL
+
+
+def test_c2_shape_shrink4(cuda):
+    """256x256x176 at shrink 4, 4 levels; fixed iterations for exact parity,
+    then to convergence 0.001."""
+    import n4b200
+    ph = make_phantom((256, 256, 176), seed=2, sigma=0.02, grid=6, coeff_std=0.25)
+    im, mk = cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")
+    res = n4b200.N4(im, mk, param(4, [8] * 4, 0.0, ShrinkFactor=4), return_bias=True)
+    out, lat, lb = O.N4Shrink(ph.im, ph.mask, 4, low_value=0, maximumNumberOfLevels=4,
+                              maximumNumberOfIterations=[8] * 4, ConvergenceThreshold=0.0,
+                              return_log_bias=True)
+    assert nrel(res.lattice, lat) < TOL
+    assert nrel(np.log(res.bias_field.cpu().numpy()), lb) < TOL
+    assert nrel(res.im_normalized, out) < TOL
+    conv = n4b200.N4(im, mk, param(4, [50] * 4, 0.001, ShrinkFactor=4))
+    rep = {}
+    _, lat2 = O.N4Shrink(ph.im, ph.mask, 4, low_value=0, maximumNumberOfLevels=4,
+                         maximumNumberOfIterations=[50] * 4, ConvergenceThreshold=0.001, report=rep)
+    got = conv.report["iterations"]
+    assert all(abs(a - b) <= 1 for a, b in zip(got, rep["iterations"])), (got, rep["iterations"])
+    if got == rep["iterations"]:
+        assert nrel(conv.lattice, lat2) < TOL
+
+
+def test_cluster_and_grid_paths_agree(cuda):
+    import n4b200
+    ph = make_phantom((96, 80, 72), seed=9, sigma=0.03, grid=4, coeff_std=0.2)
+    im, mk = cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")
+    a = n4b200.N4(im, mk, param(3, [10] * 3, 0.0))
+    b = n4b200.N4(im, mk, param(3, [10] * 3, 0.0, flags=0x8))
+    assert a.report["path"] == "cluster" and b.report["path"] == "grid"
+    assert nrel(a.lattice, b.lattice.cpu().numpy().astype(np.float64)) < 1e-5
+
+
+def test_deterministic(cuda):
+    import n4b200
+    ph = make_phantom((48, 40, 36), seed=4)
+    im, mk = cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")
+    p = param(2, [6, 6], 0.0)
+    a = n4b200.N4(im, mk, p)
+    b = n4b200.N4(im, mk, p)
+    assert cuda.equal(a.lattice, b.lattice) and cuda.equal(a.im_normalized, b.im_normalized)
+
+
+def test_batched_matches_single(cuda):
+    import n4b200
+    shapes = [(40, 48, 32), (64, 56, 40), (24, 32, 48), (56, 56, 56), (32, 24, 40)]
+    vols = []
+    for i, sh in enumerate(shapes):
+        ph = make_phantom(sh, seed=100 + i, sigma=0.03, grid=4, coeff_std=0.15)
+        vols.append((cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")))
+    p = param(3, [20] * 3, 0.001)
+    batch = n4b200.N4Batch(vols, p)
+    for (im, mk), r in zip(vols, batch):
+        s = n4b200.N4(im, mk, p)
+        assert r.report["status"] == "N4_OK"
+        assert r.report["iterations"] == s.report["iterations"]
+        assert nrel(r.lattice, s.lattice.cpu().numpy().astype(np.float64)) < 1e-6
+        assert nrel(r.im_normalized, s.im_normalized.cpu().numpy().astype(np.float64)) < 1e-6
+
+
+def test_host_path_matches_device_path(cuda):
+    import n4b200
+    ph = make_phantom((32, 28, 24), seed=6)
+    p = param(2, [5, 5], 0.0)
+    h = n4b200.N4(ph.im, ph.mask, p, return_bias=True)
+    d = n4b200.N4(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"), p, return_bias=True)
+    assert np.array_equal(h.lattice, d.lattice.cpu().numpy())
+    assert np.array_equal(h.im_normalized, d.im_normalized.cpu().numpy())
+    assert np.array_equal(h.bias_field, d.bias_field.cpu().numpy())
+
+
+def test_warm_start(cuda):
+    """A good warm lattice is kept and converges in fewer iterations; a bad
+    one is discarded (first-iteration CV rule), as the oracle decides."""
+    import n4b200
+    ph = make_phantom((64, 64, 48), seed=11, sigma=0.03, grid=4, coeff_std=0.2)
+    im, mk = cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")
+    p1 = param(1, [50], 0.001)
+    plain = n4b200.N4(im, mk, p1)
+    good = n4b200.N4(im, mk, p1, warm_lattice=plain.lattice)
+    assert good.report["warm_start_used"]
+    assert good.report["iterations"][0] < plain.report["iterations"][0]
+    bad = n4b200.N4(im, mk, p1, warm_lattice=cuda.full((4, 4, 4), 2.0, device="cuda"))
+    assert not bad.report["warm_start_used"]
+    assert bad.report["iterations"] == plain.report["iterations"]
+    assert nrel(bad.lattice, plain.lattice.cpu().numpy().astype(np.float64)) < 1e-6
+    rep = {}
+    _, lat = O.N4(ph.im, ph.mask, low_value=0, maximumNumberOfLevels=1, maximumNumberOfIterations=[4],
+                  ConvergenceThreshold=0.0, initial_lattice=plain.lattice.cpu().numpy(), report=rep)
+    g4 = n4b200.N4(im, mk, param(1, [4], 0.0), warm_lattice=plain.lattice)
+    assert g4.report["warm_start_used"] == rep["warm_start_used"]
+    assert nrel(g4.lattice, lat) < TOL
+
+
+# ------------------------------------------------------------------ edge cases
+def test_empty_mask(cuda):
+    import n4b200
+    ph = make_phantom((16, 16, 16), seed=1)
+    with pytest.raises(n4b200.N4Error, match="EMPTY_MASK"):
+        n4b200.N4(cuda.tensor(ph.im, device="cuda"), cuda.zeros((16, 16, 16), device="cuda"), param(1, [3], 0.0))
+
+
+def test_constant_image(cuda):
+    """A constant masked image has no histogram range: nothing to fit."""
+    import n4b200
+    im = np.full((20, 20, 20), 0.7, dtype=np.float32)
+    res = n4b200.N4(cuda.tensor(im, device="cuda"), None, param(2, [5, 5], 0.0))
+    assert float(res.lattice.abs().max()) == 0.0
+    assert nrel(res.im_normalized, im.astype(np.float64)) < 1e-7
+
+
+@pytest.mark.parametrize("shape,nc", [((17, 13, 11), (4, 4, 4)), ((23, 19, 30), (5, 4, 6))])
+def test_ragged_shapes_and_anisotropic_lattice(cuda, shape, nc):
+    import n4b200
+    ph = make_phantom(shape, seed=8)
+    p = param(2, [4, 4], 0.0, NumberOfControlPoints_x=nc[0], NumberOfControlPoints_y=nc[1],
+              NumberOfControlPoints_z=nc[2])
+    for force in (0, 0x8):
+        p.flags = force
+        res = n4b200.N4(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"), p)
+        out, lat = O.N4(ph.im, ph.mask, low_value=0, maximumNumberOfLevels=2, maximumNumberOfIterations=[4, 4],
+                        ConvergenceThreshold=0.0, numberOfControlPoints=nc)
+        assert nrel(res.lattice, lat) < TOL
+        assert nrel(res.im_normalized, out) < TOL
+
+
+def test_low_value_threshold_and_inplace(cuda):
+    """Voxels at or below low_value leave the mask and are zero in the
+    output; N4_FLAG_INPLACE_THRESH writes that back like cudaN4.cu:1459."""
+    import n4b200
+    ph = make_phantom((32, 32, 24), seed=12)
+    low = 0.5
+    p = param(2, [4, 4], 0.0)
+    p.low_value = low
+    out, lat = O.N4(ph.im, ph.mask, low_value=low, maximumNumberOfLevels=2, maximumNumberOfIterations=[4, 4],
+                    ConvergenceThreshold=0.0)
+    im, mk = cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")
+    res = n4b200.N4(im, mk, p)
+    assert nrel(res.lattice, lat) < TOL and nrel(res.im_normalized, out) < TOL
+    assert float(res.im_normalized[im <= low].abs().max()) == 0.0
+    assert float((im <= low).sum()) > 0 and float(im[im <= low].abs().max()) > 0.0
+    p.flags = 0x4
+    n4b200.N4(im, mk, p)
+    assert float(im[cuda.tensor(ph.im, device="cuda") <= low].abs().max()) == 0.0
+    assert float(mk[cuda.tensor(ph.im, device="cuda") <= low].abs().max()) == 0.0
+
+
+def test_invalid_arguments(cuda):
+    import n4b200
+    im = cuda.ones((16, 16, 18), device="cuda")
+    with pytest.raises(n4b200.N4Error, match="INVALID_ARG"):
+        n4b200.N4(im, None, param(1, [2], 0.0, ShrinkFactor=4))   # 18 % 4 != 0
+    with pytest.raises(n4b200.N4Error, match="UNSUPPORTED_SPLINE_ORDER"):
+        n4b200.N4(im, None, param(1, [2], 0.0, SplineOrder=2))
+
+
+def test_nonfinite_input_is_reported(cuda):
+    import n4b200
+    ph = make_phantom((16, 16, 16), seed=3)
+    im = ph.im.copy()
+    im[8, 8, 8] = np.inf
+    with pytest.raises(n4b200.N4Error, match="NONFINITE"):
+        n4b200.N4(cuda.tensor(im, device="cuda"), cuda.tensor(ph.mask, device="cuda"), param(1, [2], 0.0))

@@ -1,0 +1,72 @@
+"""The oracle against outputs of the reference's own N4.py (golden vectors).
+
+These pin ``oracle/n4_oracle.py``: every function agrees with N4.py to FP64
+round-off (the sharpening map bitwise) on seeded inputs, including shapes
+where voxel centres fall exactly on span boundaries (44 voxels / 8 spans).
+"""
+import numpy as np
+import pytest
+
+import n4_oracle as O
+
+
+def rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("tag,fwhm", [("a", 0.15), ("b", 0.3)])
+@pytest.mark.parametrize("bins", [200, 64])
+def test_sharpen(golden_components, tag, fwhm, bins):
+    g = golden_components
+    out = O.sharpenImage(g["sharp_in"], g["sharp_mask"], bins, 0.01, fwhm)
+    assert rel(out, g[f"sharp_out_{tag}{bins}"]) < 1e-13
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_fit_and_evaluate(golden_components, k):
+    g = golden_components
+    f, m, nc = g[f"fit_field_{k}"], g[f"fit_mask_{k}"], g[f"fit_ncpt_{k}"]
+    assert rel(O.FitBspline3D(f, m, nc), g[f"fit_out_{k}"]) < 1e-12
+    assert rel(O.FitBspline3D_literal(f, m, nc), g[f"fit_out_{k}"]) < 1e-12
+    lat = g[f"eval_lat_{k}"]
+    assert rel(O.EvaluateBspline3D(lat, nc, f.shape), g[f"eval_out_{k}"]) < 1e-12
+    assert rel(O.EvaluateBspline3D_literal(lat, nc, f.shape), g[f"eval_out_{k}"]) < 1e-12
+
+
+@pytest.mark.parametrize("n", [4, 5, 7])
+def test_upsample(golden_components, n):
+    g = golden_components
+    assert rel(O.UpsampleLattice3D(g[f"up_in_{n}"]), g[f"up_out_{n}"]) < 1e-13
+
+
+def test_bspline_and_cv(golden_components):
+    g = golden_components
+    w = np.stack([O.cubicBspline(t) for t in g["bspline_t"]])
+    assert np.array_equal(w, g["bspline_w"])
+    cv = O.CalculateConvergenceMeasurement(g["cv_f1"], g["cv_f2"], g["cv_mask"])
+    assert cv == pytest.approx(float(g["cv_out"]), rel=1e-14)
+
+
+@pytest.mark.parametrize("tag", ["fixed", "thresh"])
+def test_n4_small(golden_small, tag):
+    s = golden_small
+    rep = {}
+    norm, lat = O.N4(s[f"{tag}_im"], s[f"{tag}_mask"], low_value=0,
+                     maximumNumberOfLevels=int(s[f"{tag}_levels"]),
+                     maximumNumberOfIterations=list(s[f"{tag}_iters"]),
+                     ConvergenceThreshold=float(s[f"{tag}_thr"]), report=rep)
+    assert rel(lat, s[f"{tag}_lattice"]) < 1e-10
+    assert rel(norm, s[f"{tag}_norm"]) < 1e-12
+
+
+def test_n4_c1(golden_c1):
+    """N4.py on the 64x64x48 phantom, 3 levels x 50 fixed iterations."""
+    from n4b200.phantom import make_phantom
+    g = golden_c1
+    ph = make_phantom((64, 64, 48), seed=int(g["seed"]), sigma=0.03, grid=4, coeff_std=0.15)
+    rep = {}
+    norm, lat = O.N4(ph.im, ph.mask, low_value=0, maximumNumberOfLevels=3,
+                     maximumNumberOfIterations=[50, 50, 50], ConvergenceThreshold=0.0, report=rep)
+    assert rep["iterations"] == list(g["iterations"])
+    assert rel(lat, g["lattice"]) < 1e-9
+    assert rel(norm.reshape(-1)[::97], g["norm_sample"]) < 1e-9
