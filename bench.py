@@ -1,0 +1,343 @@
+#!/usr/bin/env python
+"""Benchmark: N4 volumes/s to CV < 1e-3 at 256x256x176 on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+
+One step = one batch of B synthetic 256x256x176 phantoms (shrink 4, 4 levels,
+<= 50 iterations per level, convergence 0.001, 200 bins, FWHM 0.15, Wiener
+0.01) bias-corrected to convergence through ``n4_run_batched`` (one persistent
+launch).  ``value`` is whole-job volumes/s with the inputs resident in HBM;
+``e2e`` is the same metric with the inputs copied from pinned host memory and
+the corrected volumes copied back inside the timed region; ``plain`` is the
+single-volume path (``n4_run``, one volume per call).
+
+Multi-GPU: one process per GPU (torchrun); volumes are independent, so each
+rank corrects its own batch (replicas, weak scaling, no collective on the data
+path); the timed region is bracketed by barriers and the time is the maximum
+over ranks.
+
+``--impl reference`` times the reference algorithm on the host cores: the
+FP64 restatement of N4.py in ``oracle/`` (N4.py itself cannot run here: its
+per-voxel Python loops take ~3 minutes per volume), one volume per process
+on every available core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cuda-n4_b200"))
+
+METRIC = "N4 volumes/s to CV<1e-3 at 256²×176, batched+warm-start vs plain; fit GB/s"
+SHAPE = (256, 256, 176)
+GEN = dict(sigma=0.02, grid=6, coeff_std=0.25)
+SHRINK, LEVELS, ITERS, THR = 4, 4, 50, 0.001
+# per-iteration algorithmic bytes per fitting voxel of an HBM-streaming N4
+# iteration: fit 5 (logU 4 + mask 1) + histogram 5 + evaluate/CV/update 17
+ITER_BYTES_PER_VOXEL = 27
+# final correction: read im 4 + write corrected 4 per full-resolution voxel
+CORRECT_BYTES_PER_VOXEL = 8
+
+
+def workload_desc(batch):
+    return dict(workload="c2: 256x256x176 float32 phantoms, shrink 4 -> 64x64x44, 4 levels, <=50 it/level, "
+                         "CV<0.001, 200 bins, FWHM 0.15, Wiener 0.01, low_value 0",
+                batch_per_gpu=batch, parallelism="replicas (volume-parallel)",
+                l2="inputs larger than L2: each step reads B distinct volumes (B x 92 MB)")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples SM clocks and throttle reasons every 100 ms (NVML)."""
+
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, index):
+        self.index = index
+        self.samples, self.reasons = [], set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            return self
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    for bit, name in self.REASONS.items():
+                        if r & bit:
+                            self.reasons.add(name)
+                except Exception:
+                    pass
+                self._stop.wait(0.1)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+        s = sorted(self.samples)
+        med = s[len(s) // 2] if s else None
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(s)}
+
+
+# ---------------------------------------------------------------- reference arm
+def _ref_init(seed):
+    global _REF_VOL
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from n4b200.phantom import make_phantom
+    ph = make_phantom(SHAPE, seed=seed, **GEN)
+    _REF_VOL = (ph.im, ph.mask)
+
+
+def _ref_one(_):
+    import n4_oracle as O
+    im, mask = _REF_VOL
+    rep = {}
+    O.N4Shrink(im, mask, SHRINK, low_value=0, maximumNumberOfLevels=LEVELS,
+               maximumNumberOfIterations=[ITERS] * LEVELS, ConvergenceThreshold=THR, report=rep)
+    return sum(rep["iterations"])
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+    cores = min(os.cpu_count() or 1, 64)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_ref_init, initargs=(7,)) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_one, range(cores))
+        t0 = time.perf_counter()
+        iters = []
+        for _ in range(args.steps):
+            iters += pool.map(_ref_one, range(cores))
+        dt = time.perf_counter() - t0
+    value = cores * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "volumes/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_desc(cores),
+        "cpu_baseline": {"value": value, "unit": "volumes/s", "cores": cores, "kind": "port",
+                         "sample": f"each step: {cores} phantoms, one per process, FP64 numpy restatement "
+                                   f"of N4.py run to convergence (mean {sum(iters) / len(iters):.1f} iterations)"},
+        "e2e": {"value": value, "unit": "volumes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_single(seconds=12.0):
+    """The oracle on one host core over a bounded sample (whole volumes)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import n4_oracle as O
+    from n4b200.phantom import make_phantom
+    n, t_total, iters = 0, 0.0, 0
+    while t_total < seconds and n < 32:
+        ph = make_phantom(SHAPE, seed=500 + n, **GEN)
+        rep = {}
+        t0 = time.perf_counter()
+        O.N4Shrink(ph.im, ph.mask, SHRINK, low_value=0, maximumNumberOfLevels=LEVELS,
+                   maximumNumberOfIterations=[ITERS] * LEVELS, ConvergenceThreshold=THR, report=rep)
+        t_total += time.perf_counter() - t0
+        iters += sum(rep["iterations"])
+        n += 1
+    return {"value": n / t_total, "unit": "volumes/s", "cores": 1, "kind": "port",
+            "sample": f"{n} phantoms 256x256x176 corrected to convergence by the FP64 restatement of N4.py "
+                      f"on one core ({iters / n:.1f} iterations per volume, phantom generation untimed)"}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import n4b200
+    from n4b200.phantom import make_phantom
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    B = args.batch
+    vols_host, vols_dev = [], []
+    for i in range(B):
+        ph = make_phantom(SHAPE, seed=1000 * rank + i, **GEN)
+        im_h = torch.from_numpy(ph.im).pin_memory()
+        mk_h = torch.from_numpy(ph.mask).pin_memory()
+        vols_host.append((im_h, mk_h))
+        vols_dev.append((im_h.to(dev), mk_h.to(dev)))
+    p = n4b200.N4Param(NumberOfFittingLevels=LEVELS, MaximumNumberOfIterations=ITERS,
+                       ConvergenceThreshold=THR, low_value=0.0, ShrinkFactor=SHRINK)
+    ctx = n4b200.Context(local_rank)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident batched path (the headline `value`)
+    def step_batched():
+        return n4b200.N4Batch(vols_dev, p, ctx=ctx, synchronous=False)
+
+    for _ in range(args.warmup):
+        step_batched()
+    torch.cuda.synchronize(dev)
+    res = n4b200.N4Batch(vols_dev, p, ctx=ctx)        # reports (untimed)
+    iters = [sum(r.report["iterations"]) for r in res]
+    assert all(r.report["status"] == "N4_OK" for r in res), [r.report for r in res]
+    clocks = ClockSampler(local_rank).start()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_batched()
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * B * args.steps / (ms / 1000.0)
+
+    # ---- stage times of one batched run (events recorded by the library on
+    # the launching stream)
+    ctx.set_profiling(True)
+    step_batched()
+    t = ctx.last_timings()
+    ctx.set_profiling(False)
+    total_iters = sum(iters)
+    n4_bytes = ITER_BYTES_PER_VOXEL * t["fit_voxels"] / B * total_iters
+    achieved = n4_bytes / (t["n4_ms"] / 1000.0) / 1e9
+    hbm_peak, peak_kind = peaks()
+    corr_gbs = CORRECT_BYTES_PER_VOXEL * t["full_voxels"] / (t["correct_ms"] / 1000.0) / 1e9
+    pro_gbs = (8 * t["full_voxels"] + 4 * t["fit_voxels"]) / (t["prologue_ms"] / 1000.0) / 1e9
+
+    # ---- plain single-volume path (n4_run, one volume per call)
+    for _ in range(args.warmup):
+        n4b200.N4(*vols_dev[0], p, ctx=ctx, synchronous=False)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        for im, mk in vols_dev:
+            n4b200.N4(im, mk, p, ctx=ctx, synchronous=False)
+    e1.record(stream)
+    barrier()
+    ms_plain = max_over_ranks(e0.elapsed_time(e1))
+    plain = world * B * args.steps / (ms_plain / 1000.0)
+
+    # ---- end to end: pinned host inputs -> device -> batched N4 -> host outputs
+    dev_in = [(torch.empty_like(a, device=dev), torch.empty_like(b, device=dev)) for a, b in vols_host]
+    out_h = [torch.empty_like(a).pin_memory() for a, _ in vols_host]
+    lat_h = [torch.empty(n4b200.lattice_dims(p), dtype=torch.float32).pin_memory() for _ in vols_host]
+
+    def step_e2e():
+        for (ih, mh), (idv, mdv) in zip(vols_host, dev_in):
+            idv.copy_(ih, non_blocking=True)
+            mdv.copy_(mh, non_blocking=True)
+        rs = n4b200.N4Batch(dev_in, p, ctx=ctx, synchronous=False)
+        for r, o, l in zip(rs, out_h, lat_h):
+            o.copy_(r.im_normalized, non_blocking=True)
+            l.copy_(r.lattice, non_blocking=True)
+
+    for _ in range(min(args.warmup, 2)):
+        step_e2e()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_e2e()
+    e1.record(stream)
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    h2d = sum(a.numel() * 4 + b.numel() * 4 for a, b in vols_host)
+    d2h = sum(o.numel() * 4 for o in out_h) + sum(l.numel() * 4 for l in lat_h)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "volumes/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_desc(B),
+        "roofline": {
+            "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": achieved / hbm_peak, "traffic": None,
+            "kernel": "k_n4_cluster (all levels/iterations of a batch)",
+            "basis": f"{ITER_BYTES_PER_VOXEL} B per fitting voxel per iteration "
+                     f"(fit 5 + histogram 5 + evaluate/CV/update 17) x iterations / kernel time; "
+                     f"peak {peak_kind}",
+        },
+        "e2e": {"value": world * B * args.steps / (ms_e2e / 1000.0), "unit": "volumes/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": t["launches"] * args.steps,
+        "clocks": clk,
+        "plain": {"value": plain, "unit": "volumes/s", "ms_per_volume": ms_plain / (args.steps * B)},
+        "stages_ms_per_batch": {k: t[k] for k in ("prologue_ms", "n4_ms", "tables_ms", "correct_ms")},
+        "stage_gbs": {"correct": corr_gbs, "prologue": pro_gbs},
+        "iterations_per_volume": total_iters / B,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_single()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+    return run_ours(args, rank, world if "RANK" in os.environ else 1, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

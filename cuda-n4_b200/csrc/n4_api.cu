@@ -114,6 +114,12 @@ struct n4_context {
   cudaStream_t last_stream = nullptr;
   cudaEvent_t last_done = nullptr;
   std::map<TuneKey, TuneVal> tune;
+  // profiling
+  int profiling = 0;
+  cudaEvent_t ev[5] = {};
+  int prof_launches = 0;
+  long long prof_fit = 0, prof_full = 0;
+  bool prof_valid = false;
 };
 
 namespace {
@@ -140,8 +146,8 @@ int final_nc(unsigned nc0, unsigned levels) { return (int)(((nc0 - 3) << (levels
 n4_status_t check_params(const n4_params_t *p) {
   if (!p) return fail(N4_ERR_INVALID_ARG, "params is NULL");
   if (p->SplineOrder != 3) return fail(N4_ERR_UNSUPPORTED_SPLINE_ORDER, "only cubic B-splines (SplineOrder 3) are supported");
-  if (p->NumberOfHistogramBins < 2 || p->NumberOfHistogramBins > 2048)
-    return fail(N4_ERR_INVALID_ARG, "NumberOfHistogramBins must be in [2, 2048]");
+  if (p->NumberOfHistogramBins < 2 || p->NumberOfHistogramBins > 1024)
+    return fail(N4_ERR_INVALID_ARG, "NumberOfHistogramBins must be in [2, 1024]");
   if (p->NumberOfFittingLevels < 1 || p->NumberOfFittingLevels > N4_MAX_LEVELS)
     return fail(N4_ERR_INVALID_ARG, "NumberOfFittingLevels must be in [1, 8]");
   if (p->NumberOfControlPoints_x < 4 || p->NumberOfControlPoints_y < 4 || p->NumberOfControlPoints_z < 4)
@@ -172,12 +178,20 @@ n4_status_t make_dims(const n4_params_t *p, unsigned fx, unsigned fy, unsigned f
   return N4_OK;
 }
 
+// The decimal number a float parameter was written as (0.01f -> 0.01), so
+// that the FP64 parts of the algorithm use the same constants as N4.py.
+double decimal_of(float f) {
+  char buf[32];
+  std::snprintf(buf, sizeof(buf), "%.7g", (double)f);
+  return std::strtod(buf, nullptr);
+}
+
 Params make_dev_params(const n4_params_t *p) {
   Params r{};
   r.bins = (int)p->NumberOfHistogramBins;
-  r.wiener = p->WienerFilterNoise;
-  r.fwhm = p->BiasFieldFullWidthAtHalfMaximum;
-  r.thr = p->ConvergenceThreshold;
+  r.wiener = decimal_of(p->WienerFilterNoise);
+  r.fwhm = decimal_of(p->BiasFieldFullWidthAtHalfMaximum);
+  r.thr = decimal_of(p->ConvergenceThreshold);
   r.eps = p->FitEpsilon;
   r.zero_den = (p->flags & N4_FLAG_FIT_ZERO_DEN) ? 1 : 0;
   r.ddof1 = (p->flags & N4_FLAG_CV_DDOF1) ? 1 : 0;
@@ -225,12 +239,12 @@ Plan make_plan(const n4_params_t *p, int K, const std::vector<Dims> &vols, bool 
   pl.o_tmp = take((size_t)pl.NLAT * 4);
   pl.o_aux = take((size_t)pl.NLAT * 4);
   pl.o_hist = take((size_t)kHistCopies * pl.bins * 8);
-  pl.o_H = take((size_t)pl.bins * 4);
-  pl.o_E = take((size_t)pl.bins * 4);
-  pl.o_fa = take((size_t)pl.npad * 8);
-  pl.o_fb = take((size_t)pl.npad * 8);
-  pl.o_tw = take((size_t)pl.npad * 8);
-  pl.o_ff = take((size_t)pl.npad * 4);
+  pl.o_H = take((size_t)pl.bins * 8);
+  pl.o_E = take((size_t)pl.bins * 8);
+  pl.o_fa = take((size_t)pl.npad * 16);
+  pl.o_fb = take((size_t)pl.npad * 16);
+  pl.o_tw = take((size_t)pl.npad * 16);
+  pl.o_ff = take((size_t)pl.npad * 8);
   pl.o_red = take(160 * 8);
   pl.o_misc = take(64);
   pl.sm_bytes = (int)align_up(o, 128);
@@ -339,6 +353,13 @@ n4_status_t end_run(n4_context *ctx, cudaStream_t st, Upload &u) {
   u.slot->pending = true;
   ctx->last_slot = u.index;
   ctx->last_stream = st;
+  return N4_OK;
+}
+
+n4_status_t prof_mark(n4_context *ctx, int k, cudaStream_t st) {
+  if (!ctx->profiling) return N4_OK;
+  if (!ctx->ev[k]) CK(cudaEventCreate(&ctx->ev[k]));
+  CK(cudaEventRecord(ctx->ev[k], st));
   return N4_OK;
 }
 
@@ -544,8 +565,11 @@ n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector
   TRY(begin_run(ctx, st));
   CK(cudaMemcpyAsync(u.slot->d.p, u.slot->h, o, cudaMemcpyHostToDevice, st));
   int *flags = u.dp<int>(o_flg);
+  int launches = 0;
+  TRY(prof_mark(ctx, 0, st));
   // ---- prologue
   {
+    ++launches;
     const int blocks = (int)std::min<long long>((fit_total + 255) / 256, (long long)ctx->nsm * 16);
     k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(u.dp<PrologueVol>(o_pro), u.dp<long long>(o_pst), n, fit_total,
                                                      p->low_value, flags);
@@ -556,11 +580,13 @@ n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector
         if (rvs[i].im_w) {
           k_threshold_inplace<<<(int)std::min<long long>((nf + 255) / 256, ctx->nsm * 16LL), 256, 0, st>>>(
               rvs[i].im_w, rvs[i].mask_w, nf, p->low_value);
+          ++launches;
           CK(cudaGetLastError());
         }
       }
     }
   }
+  TRY(prof_mark(ctx, 1, st));
   // ---- N4
   Slot &slot = *u.slot;
   slot.nrep = n;
@@ -588,6 +614,7 @@ n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector
     if (ch.nt == 1024) TRY(launch_cluster_kernel<1024>(a, ch.K, ncl, smem, st));
     else TRY(launch_cluster_kernel<512>(a, ch.K, ncl, smem, st));
     for (int i : in_cluster) { slot.path[i] = 1; slot.csize[i] = ch.K; }
+    ++launches;
   }
   for (int i : in_grid) {
     VolJob j = jb[i];
@@ -595,12 +622,22 @@ n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector
     TRY(launch_grid_path(ctx, p, pr, rvs[i], j, ch.nt ? ch.nt : 1024, st));
     slot.path[i] = 2;
     slot.csize[i] = ctx->nsm;
+    ++launches;
   }
+  TRY(prof_mark(ctx, 2, st));
   // ---- final correction at full resolution
   k_axis_tables<<<3 * n, 256, 0, st>>>(u.dp<TableJob>(o_tab));
   CK(cudaGetLastError());
+  TRY(prof_mark(ctx, 3, st));
   k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(o_cor), u.dp<long long>(o_tst), n, p->low_value);
   CK(cudaGetLastError());
+  TRY(prof_mark(ctx, 4, st));
+  launches += 2;
+  ctx->prof_launches = launches;
+  ctx->prof_fit = fit_total;
+  ctx->prof_full = 0;
+  for (const Dims &d : dims) ctx->prof_full += (long long)d.FX * d.FY * d.FZ;
+  ctx->prof_valid = ctx->profiling != 0;
   // reports back to the slot's pinned buffer
   CK(cudaMemcpyAsync(u.slot->h + o_rep, u.dp<char>(o_rep), sizeof(n4_report_t) * n + 0, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(u.slot->h + o_flg, u.dp<char>(o_flg), 4 * n, cudaMemcpyDeviceToHost, st));
@@ -713,6 +750,8 @@ n4_status_t n4_destroy(n4_context_t *c) {
     if (s.ev) cudaEventDestroy(s.ev);
   }
   if (c->last_done) cudaEventDestroy(c->last_done);
+  for (cudaEvent_t e : c->ev)
+    if (e) cudaEventDestroy(e);
   delete c;
   return N4_OK;
 }
@@ -756,6 +795,29 @@ n4_status_t n4_run_batched(n4_context_t *ctx, const n4_params_t *p, int n, const
   }
   TRY(run_volumes(ctx, p, v, (cudaStream_t)stream, nullptr));
   if (reports) return collect(ctx, reports, n);
+  return N4_OK;
+}
+
+n4_status_t n4_set_profiling(n4_context_t *ctx, int enable) {
+  if (!ctx) return fail(N4_ERR_INVALID_ARG, "ctx is NULL");
+  ctx->profiling = enable ? 1 : 0;
+  ctx->prof_valid = false;
+  return N4_OK;
+}
+
+n4_status_t n4_last_timings(n4_context_t *ctx, n4_timings_t *t) {
+  if (!ctx || !t) return fail(N4_ERR_INVALID_ARG, "NULL argument");
+  if (!ctx->prof_valid) return fail(N4_ERR_INVALID_ARG, "no profiled run");
+  CK(cudaEventSynchronize(ctx->ev[4]));
+  float ms[4];
+  for (int k = 0; k < 4; ++k) CK(cudaEventElapsedTime(&ms[k], ctx->ev[k], ctx->ev[k + 1]));
+  t->prologue_ms = ms[0];
+  t->n4_ms = ms[1];
+  t->tables_ms = ms[2];
+  t->correct_ms = ms[3];
+  t->launches = ctx->prof_launches;
+  t->fit_voxels = ctx->prof_fit;
+  t->full_voxels = ctx->prof_full;
   return N4_OK;
 }
 
@@ -884,32 +946,35 @@ n4_status_t n4_sharpen_image(n4_context_t *ctx, const float *d_before, const flo
                              unsigned int bins, float wiener, float fwhm, float *d_after, float *bin_min,
                              float *bin_max, float *h_E) {
   if (!ctx || !d_before || !d_after || n == 0) return fail(N4_ERR_INVALID_ARG, "bad arguments");
-  if (bins < 2 || bins > 2048) return fail(N4_ERR_INVALID_ARG, "bins must be in [2, 2048]");
+  if (bins < 2 || bins > 1024) return fail(N4_ERR_INVALID_ARG, "bins must be in [2, 1024]");
   CK(cudaSetDevice(ctx->device));
   cudaStream_t st = nullptr;
   const int nb = std::min<int>((int)((n + 255) / 256), ctx->nsm * 8);
   TRY(ctx->s1.ensure((size_t)nb * 8 + 64, "partials"));
-  TRY(ctx->s2.ensure((size_t)bins * 8 + (size_t)bins * 4 + 64, "histogram"));
+  TRY(ctx->s2.ensure((size_t)bins * 16 + 64, "histogram"));
+  TRY(ctx->s3.ensure(64, "statistics"));
   float *part = ctx->s1.as<float>();
-  float *stats = part + 2 * nb;
+  double *stats = ctx->s3.as<double>();
   unsigned long long *hist = ctx->s2.as<unsigned long long>();
-  float *E = (float *)(hist + bins);
+  double *E = (double *)(hist + bins);
   k_minmax<<<nb, 256, 0, st>>>(d_before, d_mask, n, part);
   k_minmax_final<<<1, 256, 0, st>>>(part, nb, bins, stats);
   CK(cudaMemsetAsync(hist, 0, (size_t)bins * 8, st));
   k_hist<<<nb, 256, bins * 8, st>>>(d_before, d_mask, n, stats, bins, hist);
   const int npad = npad_of(bins), hoff = (int)(0.5 * (npad - bins));
-  const int smem = npad * (8 * 3 + 4) + bins * 8;
+  const int smem = npad * (16 * 3 + 8) + bins * 16;
   CK(cudaFuncSetAttribute(k_sharpen, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_sharpen<<<1, 512, smem, st>>>(hist, stats, bins, npad, hoff, wiener, fwhm, E);
+  k_sharpen<<<1, 512, smem, st>>>(hist, stats, bins, npad, hoff, decimal_of(wiener), decimal_of(fwhm), E);
   k_remap<<<nb, 256, 0, st>>>(d_before, d_mask, n, stats, E, bins, d_after);
   CK(cudaGetLastError());
-  float hs[3];
+  double hs[4];
+  std::vector<double> hE(bins);
   CK(cudaMemcpyAsync(hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, st));
-  if (h_E) CK(cudaMemcpyAsync(h_E, E, (size_t)bins * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(hE.data(), E, (size_t)bins * 8, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  if (bin_min) *bin_min = hs[0];
-  if (bin_max) *bin_max = hs[1];
+  if (bin_min) *bin_min = (float)hs[0];
+  if (bin_max) *bin_max = (float)hs[1];
+  if (h_E) for (unsigned b = 0; b < bins; ++b) h_E[b] = (float)hE[b];
   if (!(hs[0] <= hs[1])) return fail(N4_ERR_EMPTY_MASK, "no voxel in the mask");
   return N4_OK;
 }

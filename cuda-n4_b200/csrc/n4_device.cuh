@@ -159,31 +159,36 @@ __device__ void block_reduce4(float vmin, float vmax, double s0, double s1,
   __syncthreads();
 }
 
-// ---------------------------------------------------------------- FFT
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// ---------------------------------------------------------------- FFT (FP64)
+// The sharpening map is computed in double precision: N4 accumulates the
+// residual logU - E(logU), a small difference of O(1) values, so a relative
+// error of 1e-6 in E moves the fitted lattice by ~2e-4 after a few dozen
+// iterations.  The map is O(bins) work per iteration; every volume-sized
+// quantity stays in FP32.
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }  // a * (-i)
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 mul_mi(double2 a) { return make_double2(a.y, -a.x); }  // a * (-i)
 
-__device__ __forceinline__ void dft2(float2 *v) {
-  float2 a = v[0], b = v[1];
+__device__ __forceinline__ void dft2(double2 *v) {
+  double2 a = v[0], b = v[1];
   v[0] = cadd(a, b); v[1] = csub(a, b);
 }
-__device__ __forceinline__ void dft4(float2 &v0, float2 &v1, float2 &v2, float2 &v3) {
-  float2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = mul_mi(csub(v1, v3));
+__device__ __forceinline__ void dft4(double2 &v0, double2 &v1, double2 &v2, double2 &v3) {
+  double2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = mul_mi(csub(v1, v3));
   v0 = cadd(t0, t2); v2 = csub(t0, t2); v1 = cadd(t1, t3); v3 = csub(t1, t3);
 }
-__device__ __forceinline__ void dft8(float2 *v) {
-  const float c = 0.70710678118654752f;
-  float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-  float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+__device__ __forceinline__ void dft8(double2 *v) {
+  const double c = 0.70710678118654752440;
+  double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
   dft4(e0, e1, e2, e3);
   dft4(o0, o1, o2, o3);
-  o1 = make_float2(c * (o1.x + o1.y), c * (o1.y - o1.x));   // * e^{-i pi/4}
-  o2 = mul_mi(o2);                                           // * e^{-i pi/2}
-  o3 = make_float2(c * (o3.y - o3.x), -c * (o3.x + o3.y));  // * e^{-3i pi/4}
+  o1 = make_double2(c * (o1.x + o1.y), c * (o1.y - o1.x));   // * e^{-i pi/4}
+  o2 = mul_mi(o2);                                            // * e^{-i pi/2}
+  o3 = make_double2(c * (o3.y - o3.x), -c * (o3.x + o3.y));  // * e^{-3i pi/4}
   v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
   v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
   v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
@@ -191,23 +196,23 @@ __device__ __forceinline__ void dft8(float2 *v) {
 }
 
 // tw[m] = exp(-2 pi i m / N), m in [0, N).
-__device__ void fft_twiddles(float2 *tw, int N) {
+__device__ void fft_twiddles(double2 *tw, int N) {
   for (int m = threadIdx.x; m < N; m += blockDim.x) {
-    float s, c;
-    sincospif(-2.0f * (float)m / (float)N, &s, &c);
-    tw[m] = make_float2(c, s);
+    double s, c;
+    sincospi(-2.0 * (double)m / (double)N, &s, &c);
+    tw[m] = make_double2(c, s);
   }
 }
 
 // One Stockham pass of radix R (Govindaraju et al., SC'08, "High performance
 // discrete Fourier transforms on graphics processors"): x -> y.
 template <int R>
-__device__ void stockham_pass(const float2 *x, float2 *y, int N, int Ns, const float2 *tw) {
+__device__ void stockham_pass(const double2 *x, double2 *y, int N, int Ns, const double2 *tw) {
   const int T = N / R;
   const int tstep = N / (Ns * R);
   for (int j = threadIdx.x; j < T; j += blockDim.x) {
     const int k = j & (Ns - 1);
-    float2 v[R];
+    double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       v[r] = x[j + r * T];
@@ -224,7 +229,7 @@ __device__ void stockham_pass(const float2 *x, float2 *y, int N, int Ns, const f
 
 // Forward FFT of a (length N = 2^m, 4 <= N <= 4096).  Ping-pongs between a
 // and b; returns the buffer that holds the result.  Caller synchronised.
-__device__ float2 *fft_forward(float2 *a, float2 *b, int N, const float2 *tw) {
+__device__ double2 *fft_forward(double2 *a, double2 *b, int N, const double2 *tw) {
   int Ns = 1;
   int rem = N;
   while (rem > 1) {
@@ -232,91 +237,94 @@ __device__ float2 *fft_forward(float2 *a, float2 *b, int N, const float2 *tw) {
     else if (rem % 4 == 0) { stockham_pass<4>(a, b, N, Ns, tw); Ns *= 4; rem /= 4; }
     else { stockham_pass<2>(a, b, N, Ns, tw); Ns *= 2; rem /= 2; }
     __syncthreads();
-    float2 *t = a; a = b; b = t;
+    double2 *t = a; a = b; b = t;
   }
   return a;
 }
 
 // ---------------------------------------------------------------- sharpening
 struct SharpenBufs {
-  float2 *a, *b;     // [N] work buffers
-  float2 *tw;        // [N] twiddles (filled by the caller once)
-  float *Ff;         // [N] real Fourier transform of the Gaussian
+  double2 *a, *b;    // [N] work buffers
+  double2 *tw;       // [N] twiddles (filled by the caller once)
+  double *Ff;        // [N] real Fourier transform of the Gaussian
 };
 
-// E[0..bins) from the fractional histogram H (N4.py:32-101, cudaN4.cu:733-817).
-// H, E in shared memory; all threads of the CTA call it.
-__device__ void sharpen_map(const float *H, int bins, int N, int off, float binMin, float slope,
-                            float wiener, float fwhm, const SharpenBufs &sb, float *E) {
-  const float ln2 = 0.69314718055994531f;
-  const float scaledFWHM = fwhm / slope;
-  const float expFactor = 4.0f * ln2 / (scaledFWHM * scaledFWHM);
-  const float scaleFactor = 2.0f * sqrtf(ln2 / 3.14159265358979324f) / scaledFWHM;
+// E[0..bins) from the fractional histogram H (N4.py:32-101, cudaN4.cu:733-817),
+// all in FP64.  H, E in shared memory; all threads of the CTA call it.
+__device__ void sharpen_map(const double *H, int bins, int N, int off, double binMin, double slope,
+                            double wiener, double fwhm, const SharpenBufs &sb, double *E) {
+  const double ln2 = 0.69314718055994530942;
+  const double scaledFWHM = fwhm / slope;
+  const double expFactor = 4.0 * ln2 / (scaledFWHM * scaledFWHM);
+  const double scaleFactor = 2.0 * sqrt(ln2 / 3.14159265358979323846) / scaledFWHM;
   // z = V + i F : the padded histogram and the periodic Gaussian in one FFT
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    int d = i <= N / 2 ? i : N - i;
-    float F = scaleFactor * expf(-(float)(d * d) * expFactor);
-    float V = (i >= off && i < off + bins) ? H[i - off] : 0.0f;
-    sb.a[i] = make_float2(V, F);
+    const int d = i <= N / 2 ? i : N - i;
+    const double F = scaleFactor * exp(-(double)d * (double)d * expFactor);
+    const double V = (i >= off && i < off + bins) ? H[i - off] : 0.0;
+    sb.a[i] = make_double2(V, F);
   }
   __syncthreads();
-  float2 *Z = fft_forward(sb.a, sb.b, N, sb.tw);
-  float2 *W = (Z == sb.a) ? sb.b : sb.a;
+  double2 *Z = fft_forward(sb.a, sb.b, N, sb.tw);
+  double2 *W = (Z == sb.a) ? sb.b : sb.a;
   // split the packed transform; Wiener filter Re(conj(Ff)/(|Ff|^2 + w)) with Ff real
   for (int k = threadIdx.x; k < N; k += blockDim.x) {
-    float2 zk = Z[k], zn = Z[(N - k) & (N - 1)];
-    float2 Vf = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-    float Ff = 0.5f * (zk.y + zn.y);
-    float g = Ff / (Ff * Ff + wiener);
+    const double2 zk = Z[k], zn = Z[(N - k) & (N - 1)];
+    const double2 Vf = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y - zn.y));
+    const double Ff = 0.5 * (zk.y + zn.y);
+    const double g = Ff / (Ff * Ff + wiener);
     sb.Ff[k] = Ff;
-    // inverse transform by conjugation: store conj(Uf)
-    W[k] = make_float2(Vf.x * g, -Vf.y * g);
+    W[k] = make_double2(Vf.x * g, -Vf.y * g);   // conj(Uf): inverse by conjugation
   }
   __syncthreads();
-  float2 *Y = fft_forward(W, Z, N, sb.tw);
-  float2 *Y2 = (Y == W) ? Z : W;
-  // U = max(Re(ifft(Uf)), 0); pack numerator (real) and U (imaginary)
-  const float invN = 1.0f / (float)N;
+  double2 *Y = fft_forward(W, Z, N, sb.tw);
+  double2 *Y2 = (Y == W) ? Z : W;
+  // U = max(Re(ifft(Uf)), 0); pack the numerator c_i U_i (real) and U (imaginary)
+  const double invN = 1.0 / (double)N;
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    float U = fmaxf(Y[i].x * invN, 0.0f);
-    float c = binMin + (float)(i - off) * slope;
-    Y2[i] = make_float2(c * U, U);
+    const double U = fmax(Y[i].x * invN, 0.0);
+    const double c = binMin + (double)(i - off) * slope;
+    Y2[i] = make_double2(c * U, U);
   }
   __syncthreads();
-  float2 *P = fft_forward(Y2, Y, N, sb.tw);
-  float2 *P2 = (P == Y2) ? Y : Y2;
+  // Gaussian smoothing of both: multiply by the (real) Ff, inverse transform
+  double2 *P = fft_forward(Y2, Y, N, sb.tw);
+  double2 *P2 = (P == Y2) ? Y : Y2;
   for (int k = threadIdx.x; k < N; k += blockDim.x) {
-    float2 v = P[k];
-    float f = sb.Ff[k];
-    P2[k] = make_float2(v.x * f, -v.y * f);   // conj for the inverse transform
+    const double2 v = P[k];
+    const double f = sb.Ff[k];
+    P2[k] = make_double2(v.x * f, -v.y * f);
   }
   __syncthreads();
-  float2 *S = fft_forward(P2, P, N, sb.tw);
-  // smoothed numerator = Re, smoothed denominator = Im (after conj and 1/N)
+  double2 *S = fft_forward(P2, P, N, sb.tw);
   for (int b = threadIdx.x; b < bins; b += blockDim.x) {
-    float2 v = S[off + b];
-    float nu = v.x * invN, de = -v.y * invN;
-    E[b] = (de != 0.0f) ? nu / de : 0.0f;
+    const double2 v = S[off + b];
+    const double nu = v.x * invN, de = -v.y * invN;
+    E[b] = (de != 0.0) ? nu / de : 0.0;
   }
   __syncthreads();
 }
 
-// Fractional histogram contribution of one value (N4.py:21-29), as 2^24
-// fixed-point weights.  Returns the bin or -1 when the value adds nothing.
-__device__ __forceinline__ int hist_bin(float x, float binMin, float slope, int bins,
-                                        unsigned &qlo, unsigned &qhi) {
-  float c = __fdiv_rn(__fsub_rn(x, binMin), slope);
-  float fc = floorf(c);
-  float off = __fsub_rn(c, fc);
-  int idx = (int)fc;
-  if (!(c >= 0.0f) || idx >= bins) return -1;   // NaN / out of range (defensive)
-  if (off == 0.0f) { qlo = 16777216u; qhi = 0u; return idx; }
+// Bin coordinate of a value, (x - binMin) / slope, in FP64.
+__device__ __forceinline__ double bin_coord(float x, double binMin, double inv_slope) {
+  return ((double)x - binMin) * inv_slope;
+}
+
+// Fractional histogram contribution of one value (N4.py:21-29) from its
+// FP64 bin coordinate, as 2^24 fixed-point weights.  Returns the bin or -1
+// when the value adds nothing.
+__device__ __forceinline__ int hist_bin(double c, int bins, unsigned &qlo, unsigned &qhi) {
+  if (!(c >= 0.0) || !(c < (double)bins)) return -1;   // NaN / out of range (defensive)
+  const double fc = floor(c);
+  const double off = c - fc;
+  const int idx = (int)fc;
+  if (off == 0.0) { qlo = 16777216u; qhi = 0u; return idx; }
   if (idx < bins - 1) {
-    qhi = (unsigned)__float2uint_rn(off * kHistScale);
+    qhi = (unsigned)__double2uint_rn(off * 16777216.0);
     qlo = 16777216u - qhi;
     return idx;
   }
-  return -1;                                      // the reference drops it
+  return -1;                                             // the reference drops it
 }
 
 // Warp-aggregated add of one value into a shared u64 histogram.  All 32
@@ -334,15 +342,15 @@ __device__ __forceinline__ void hist_add_warp(unsigned long long *h, int bins, i
   }
 }
 
-// Piecewise-linear remap through E (N4.py:107-113).
-__device__ __forceinline__ float remap_value(float x, float binMin, float slope, const float *E, int bins) {
-  float c = __fdiv_rn(__fsub_rn(x, binMin), slope);
-  float fc = floorf(c);
+// Piecewise-linear remap through E (N4.py:107-113) from the FP64 bin
+// coordinate c of the value.
+__device__ __forceinline__ double sharpened_value(double c, const double *E, int bins) {
+  const double fc = floor(c);
   int idx = (int)fc;
-  if (idx < 0) idx = 0;   // unreachable for x >= binMin; keeps the access in range
+  if (!(c >= 0.0)) idx = 0;   // unreachable for values >= binMin; keeps the access in range
   if (idx < bins - 1) {
-    float e0 = E[idx], e1 = E[idx + 1];
-    return __fadd_rn(e0, __fmul_rn(__fsub_rn(e1, e0), __fsub_rn(c, fc)));
+    const double e0 = E[idx], e1 = E[idx + 1];
+    return e0 + (e1 - e0) * (c - fc);
   }
   return E[bins - 1];
 }

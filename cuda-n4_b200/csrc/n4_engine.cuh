@@ -45,7 +45,8 @@ struct Plan {
 
 struct Params {
   int bins;
-  float wiener, fwhm, thr, eps;
+  double wiener, fwhm, thr;   // decimal values of the float parameters
+  float eps;
   int zero_den, ddof1;
   int iters[N4_MAX_LEVELS];
 };
@@ -107,9 +108,10 @@ struct Engine {
   int ncx, ncy, ncz, nlat;
   Axis ax, ay, az;
   // smem views
-  float *L, *D, *den, *tmp, *aux, *H, *E, *Ff;
+  float *L, *D, *den, *tmp, *aux;
+  double *H, *E, *Ff;
   unsigned long long *hist;
-  float2 *fa, *fb, *tw;
+  double2 *fa, *fb, *tw;
   double *red;
   float *G, *Gd, *T2, *slotC;
   Stats *slotA;
@@ -119,9 +121,9 @@ struct Engine {
       : g(g_), pl(p), pr(r), sm(sm_), big(big_), red_global(rg) {
     L = (float *)(sm + pl.o_L); D = (float *)(sm + pl.o_D); den = (float *)(sm + pl.o_den);
     tmp = (float *)(sm + pl.o_tmp); aux = (float *)(sm + pl.o_aux);
-    hist = (unsigned long long *)(sm + pl.o_hist); H = (float *)(sm + pl.o_H); E = (float *)(sm + pl.o_E);
-    fa = (float2 *)(sm + pl.o_fa); fb = (float2 *)(sm + pl.o_fb); tw = (float2 *)(sm + pl.o_tw);
-    Ff = (float *)(sm + pl.o_ff); red = (double *)(sm + pl.o_red);
+    hist = (unsigned long long *)(sm + pl.o_hist); H = (double *)(sm + pl.o_H); E = (double *)(sm + pl.o_E);
+    fa = (double2 *)(sm + pl.o_fa); fb = (double2 *)(sm + pl.o_fb); tw = (double2 *)(sm + pl.o_tw);
+    Ff = (double *)(sm + pl.o_ff); red = (double *)(sm + pl.o_red);
     G = (float *)(big + pl.b_G); Gd = (float *)(big + pl.b_Gd); T2 = (float *)(big + pl.b_T2);
     slotA = (Stats *)(big + pl.b_slotA); slotB = (unsigned long long *)(big + pl.b_slotB);
     slotC = (float *)(big + pl.b_slotC);
@@ -311,7 +313,7 @@ struct Engine {
   }
 
   // ---- pass B + sharpening: histogram of logU over the group, then E
-  __device__ bool pass_b(float bmin, float slope) {
+  __device__ bool pass_b(double bmin, double slope, double inv_slope) {
     const int bins = pr.bins;
     for (int i = threadIdx.x; i < kHistCopies * bins; i += blockDim.x) hist[i] = 0ull;
     __syncthreads();
@@ -323,7 +325,7 @@ struct Engine {
       unsigned qlo = 0, qhi = 0;
       if (i < n) {
         const float lu = logu[i];
-        if (!isnan(lu)) key = hist_bin(lu, bmin, slope, bins, qlo, qhi);
+        if (!isnan(lu)) key = hist_bin(bin_coord(lu, bmin, inv_slope), bins, qlo, qhi);
       }
       hist_add_warp(hc, bins, key, qlo, qhi);
     }
@@ -335,7 +337,7 @@ struct Engine {
     }
     unsigned long long *Hs = hist;   // reuse copy 0 for the group sum
     if (!allreduce(slotB, Hs, bins)) return false;
-    for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (float)((double)Hs[b] * kHistInvScale);
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (double)Hs[b] * kHistInvScale;
     __syncthreads();
     SharpenBufs sb{fa, fb, tw, Ff};
     sharpen_map(H, bins, pl.npad, pl.hoff, bmin, slope, pr.wiener, pr.fwhm, sb, E);
@@ -343,12 +345,13 @@ struct Engine {
   }
 
   // ---- pass C: residual in place of logU (0 outside the mask)
-  __device__ void pass_c(float bmin, float slope, bool degenerate) {
+  __device__ void pass_c(double bmin, double inv_slope, bool degenerate) {
     const int n = nrow * Z;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const float lu = logu[i];
       float r = 0.0f;
-      if (!isnan(lu) && !degenerate) r = __fsub_rn(lu, remap_value(lu, bmin, slope, E, pr.bins));
+      if (!isnan(lu) && !degenerate)
+        r = (float)((double)lu - sharpened_value(bin_coord(lu, bmin, inv_slope), E, pr.bins));
       logu[i] = r;
     }
     __syncthreads();
@@ -356,11 +359,13 @@ struct Engine {
 
   // ---- one sharpen + fit step from the current G; leaves the update in D
   __device__ bool fit_step(const double st[4]) {
-    const float bmin = (float)st[0], bmax = (float)st[1];
-    const float slope = __fdiv_rn(__fsub_rn(bmax, bmin), (float)(pr.bins - 1));
-    const bool degenerate = !(slope > 0.0f) || isinf(slope);
-    if (!degenerate) { if (!pass_b(bmin, slope)) return false; }
-    pass_c(bmin, slope, degenerate);
+    // bin range of the masked logU (N4.py:14-15); st holds FP32 values
+    const double bmin = st[0], bmax = st[1];
+    const double slope = (bmax - bmin) / (double)(pr.bins - 1);
+    const bool degenerate = !(slope > 0.0) || !isfinite(slope);
+    const double inv_slope = degenerate ? 0.0 : 1.0 / slope;
+    if (!degenerate) { if (!pass_b(bmin, slope, inv_slope)) return false; }
+    pass_c(bmin, inv_slope, degenerate);
     contract(true);
     if (!allreduce(slotC, D, nlat)) return false;
     for (int c = threadIdx.x; c < nlat; c += blockDim.x) {
@@ -481,7 +486,7 @@ struct Engine {
       for (;;) {
         if (!pass_a(it > 0, st)) goto timeout;
         if (it > 0) cv = cv_from(st, nfg);
-        if (!(cv > pr.thr) || it >= maxIt) break;
+        if (!((double)cv > pr.thr) || it >= maxIt) break;
         if (!fit_step(st)) goto timeout;
         for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] += D[c];
         __syncthreads();

@@ -407,32 +407,34 @@ __global__ void k_minmax(const float *x, const float *mask, long long n, float *
   if (threadIdx.x == 0) { part[2 * blockIdx.x] = (float)out[0]; part[2 * blockIdx.x + 1] = (float)out[1]; }
 }
 
-// stats[0] = min, stats[1] = max, stats[2] = slope
-__global__ void k_minmax_final(const float *part, int nb, int bins, float *stats) {
+// stats[0] = min, stats[1] = max, stats[2] = slope, stats[3] = 1 / slope (FP64)
+__global__ void k_minmax_final(const float *part, int nb, int bins, double *stats) {
   float vmin = INFINITY, vmax = -INFINITY;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) { vmin = fminf(vmin, part[2 * i]); vmax = fmaxf(vmax, part[2 * i + 1]); }
   __shared__ double scratch[160];
   double out[4];
   block_reduce4(vmin, vmax, 0.0, 0.0, scratch + 8, out);
   if (threadIdx.x == 0) {
-    stats[0] = (float)out[0];
-    stats[1] = (float)out[1];
-    stats[2] = __fdiv_rn(__fsub_rn((float)out[1], (float)out[0]), (float)(bins - 1));
+    const double slope = (out[1] - out[0]) / (double)(bins - 1);
+    stats[0] = out[0];
+    stats[1] = out[1];
+    stats[2] = slope;
+    stats[3] = (slope > 0.0 && isfinite(slope)) ? 1.0 / slope : 0.0;
   }
 }
 
-__global__ void k_hist(const float *x, const float *mask, long long n, const float *stats, int bins,
+__global__ void k_hist(const float *x, const float *mask, long long n, const double *stats, int bins,
                        unsigned long long *hist) {
   extern __shared__ unsigned long long hs[];
   for (int i = threadIdx.x; i < bins; i += blockDim.x) hs[i] = 0ull;
   __syncthreads();
-  const float bmin = stats[0], slope = stats[2];
+  const double bmin = stats[0], inv = stats[3];
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long base = blockIdx.x * (long long)blockDim.x; base < n; base += stride) {
     const long long i = base + threadIdx.x;
     int key = -1;
     unsigned qlo = 0, qhi = 0;
-    if (i < n && slope > 0.0f && (!mask || mask[i] != 0.0f)) key = hist_bin(x[i], bmin, slope, bins, qlo, qhi);
+    if (i < n && inv > 0.0 && (!mask || mask[i] != 0.0f)) key = hist_bin(bin_coord(x[i], bmin, inv), bins, qlo, qhi);
     hist_add_warp(hs, bins, key, qlo, qhi);
   }
   __syncthreads();
@@ -440,31 +442,31 @@ __global__ void k_hist(const float *x, const float *mask, long long n, const flo
     if (hs[i]) atomicAdd(&hist[i], hs[i]);
 }
 
-__global__ void k_sharpen(const unsigned long long *hist, const float *stats, int bins, int npad, int hoff,
-                          float wiener, float fwhm, float *E_out) {
+__global__ void k_sharpen(const unsigned long long *hist, const double *stats, int bins, int npad, int hoff,
+                          double wiener, double fwhm, double *E_out) {
   extern __shared__ __align__(16) char sm[];
-  float2 *fa = (float2 *)sm, *fb = fa + npad, *tw = fb + npad;
-  float *Ff = (float *)(tw + npad);
-  float *H = Ff + npad;
-  float *E = H + bins;
+  double2 *fa = (double2 *)sm, *fb = fa + npad, *tw = fb + npad;
+  double *Ff = (double *)(tw + npad);
+  double *H = Ff + npad;
+  double *E = H + bins;
   fft_twiddles(tw, npad);
-  for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (float)((double)hist[b] * kHistInvScale);
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (double)hist[b] * kHistInvScale;
   __syncthreads();
-  if (stats[2] > 0.0f) {
+  if (stats[3] > 0.0) {
     SharpenBufs sb{fa, fb, tw, Ff};
     sharpen_map(H, bins, npad, hoff, stats[0], stats[2], wiener, fwhm, sb, E);
     for (int b = threadIdx.x; b < bins; b += blockDim.x) E_out[b] = E[b];
   } else {
-    for (int b = threadIdx.x; b < bins; b += blockDim.x) E_out[b] = 0.0f;
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) E_out[b] = 0.0;
   }
 }
 
-__global__ void k_remap(const float *x, const float *mask, long long n, const float *stats, const float *E,
+__global__ void k_remap(const float *x, const float *mask, long long n, const double *stats, const double *E,
                         int bins, float *out) {
-  const float bmin = stats[0], slope = stats[2];
+  const double bmin = stats[0], inv = stats[3];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     if (mask && mask[i] == 0.0f) { out[i] = 0.0f; continue; }
-    out[i] = slope > 0.0f ? remap_value(x[i], bmin, slope, E, bins) : x[i];
+    out[i] = inv > 0.0 ? (float)sharpened_value(bin_coord(x[i], bmin, inv), E, bins) : x[i];
   }
 }
 

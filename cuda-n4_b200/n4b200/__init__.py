@@ -148,6 +148,14 @@ class Context:
         except Exception:
             pass
 
+    def set_profiling(self, enable: bool = True):
+        check(_lib.load().n4_set_profiling(self._h, int(bool(enable))))
+
+    def last_timings(self) -> dict:
+        t = _lib.n4_timings_t()
+        check(_lib.load().n4_last_timings(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
     @classmethod
     def default(cls, device: int = 0) -> "Context":
         if device not in cls._default:

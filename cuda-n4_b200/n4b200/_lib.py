@@ -67,6 +67,14 @@ class n4_volume_t(C.Structure):
     ]
 
 
+class n4_timings_t(C.Structure):
+    _fields_ = [
+        ("prologue_ms", C.c_float), ("n4_ms", C.c_float), ("tables_ms", C.c_float),
+        ("correct_ms", C.c_float), ("launches", C.c_int), ("fit_voxels", C.c_longlong),
+        ("full_voxels", C.c_longlong),
+    ]
+
+
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libn4b200.so")
 
 # (name, restype, argtypes) of every exported entry point of include/n4b200.h
@@ -87,6 +95,8 @@ SIGNATURES = [
     ("n4_run_batched", C.c_int, [_P, C.POINTER(n4_params_t), C.c_int, C.POINTER(n4_volume_t), _P,
                                  C.POINTER(n4_report_t)]),
     ("n4_sync", C.c_int, [_P, C.POINTER(n4_report_t), C.c_int]),
+    ("n4_set_profiling", C.c_int, [_P, C.c_int]),
+    ("n4_last_timings", C.c_int, [_P, C.POINTER(n4_timings_t)]),
     ("n4_fit_bspline3d", C.c_int, [_P, _P, _P, _U, _U, _U, _U, _U, _U, C.c_float, C.c_int, _P, _P]),
     ("n4_evaluate_bspline3d", C.c_int, [_P, _P, _U, _U, _U, _U, _U, _U, _P, _P]),
     ("n4_upsample_lattice3d", C.c_int, [_P, _P, _U, _U, _U, _P, _P]),

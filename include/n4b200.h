@@ -134,6 +134,23 @@ n4_status_t n4_run_batched(n4_context_t *ctx, const n4_params_t *p, int n,
 /* Wait for the context's last asynchronous run and fill its reports. */
 n4_status_t n4_sync(n4_context_t *ctx, n4_report_t *reports, int n);
 
+/* ---- measurement (no counterpart in the reference) ----
+ * With profiling enabled, every run records CUDA events around its kernels
+ * on the run's stream; n4_last_timings waits for the last run and returns
+ * the device time of each stage and how many kernels it launched. */
+typedef struct {
+  float prologue_ms;   /* threshold / shrink / log                        */
+  float n4_ms;         /* all levels and iterations (cluster or grid)     */
+  float tables_ms;     /* full-resolution B-spline tables                 */
+  float correct_ms;    /* fused evaluation + im / exp(b) at full size     */
+  int launches;        /* kernels launched by the run                     */
+  long long fit_voxels;    /* fitting-grid voxels of the run              */
+  long long full_voxels;   /* full-resolution voxels of the run           */
+} n4_timings_t;
+
+n4_status_t n4_set_profiling(n4_context_t *ctx, int enable);
+n4_status_t n4_last_timings(n4_context_t *ctx, n4_timings_t *t);
+
 /* ---- components (unit-level parity with the reference's entry points) ---- */
 
 /* Replaces FitBspline3D (cudaN4.h:313-325): lattice[ncpt] fitted to `field`

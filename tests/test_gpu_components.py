@@ -1,5 +1,9 @@
 """Component kernels (through the C ABI) against N4.py's golden vectors.
 
+The sharpening map is computed in FP64 on the device (an FP32 map differs
+from the FP64 oracle by ~2e-5 of its range in sparse bins, which N4's
+residual accumulation amplifies ~200-fold); it is compared at 1e-6.
+
 Tolerance: the kernels compute in FP32 against FP64 references, so results
 are compared relative to the reference's largest magnitude
 (``max|gpu - ref| / max|ref|``) with the bound stated per test.
@@ -82,8 +86,8 @@ def test_sharpen(cuda, golden_components, tag, fwhm, bins):
     out, det = n4b200.sharpenImage(x, g["sharp_mask"], bins, 0.01, fwhm, details=True)
     # same FP32 input through the FP64 oracle, and the N4.py golden output
     ref = O.sharpenImage(x.astype(np.float64), g["sharp_mask"], bins, 0.01, fwhm)
-    assert nrel(out, ref) < 2e-5
-    assert nrel(out, g[f"sharp_out_{tag}{bins}"]) < 1e-4
+    assert nrel(out, ref) < 1e-6
+    assert nrel(out, g[f"sharp_out_{tag}{bins}"]) < 1e-5
     m = g["sharp_mask"] != 0
     assert det["binMin"] == x[m].min() and det["binMax"] == x[m].max()
 
@@ -97,7 +101,7 @@ def test_sharpen_map_matches_oracle(cuda, golden_components):
     _, od = O.sharpenImage(x.astype(np.float64), m, 200, 0.01, 0.15, details=True)
     E = det["E"].astype(np.float64)
     live = od["H"] > 0          # bins that voxels actually map through
-    assert np.abs(E - od["E"])[live].max() / np.abs(od["E"]).max() < 2e-5
+    assert np.abs(E - od["E"])[live].max() / np.abs(od["E"]).max() < 1e-6
 
 
 def test_convergence(cuda, golden_components):

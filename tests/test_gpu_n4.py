@@ -105,7 +105,7 @@ def test_c2_shape_shrink4(cuda):
 
 def test_cluster_and_grid_paths_agree(cuda):
     import n4b200
-    ph = make_phantom((96, 80, 72), seed=9, sigma=0.03, grid=4, coeff_std=0.2)
+    ph = make_phantom((64, 64, 48), seed=9, sigma=0.03, grid=4, coeff_std=0.2)
     im, mk = cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")
     a = n4b200.N4(im, mk, param(3, [10] * 3, 0.0))
     b = n4b200.N4(im, mk, param(3, [10] * 3, 0.0, flags=0x8))
