@@ -305,10 +305,20 @@ __device__ void sharpen_map(const double *H, int bins, int N, int off, double bi
   __syncthreads();
 }
 
-// Bin coordinate of a value, (x - binMin) / slope, in FP64.
-__device__ __forceinline__ double bin_coord(float x, double binMin, double inv_slope) {
-  return ((double)x - binMin) * inv_slope;
-}
+// Bin coordinate of a value, (x - binMin) / slope, in FP64.  The reciprocal
+// product is within an ulp of the quotient; near the last bin the quotient
+// itself is taken, because there one ulp decides whether the reference
+// counts or drops the maximum voxel (N4.py:27).
+struct BinMap {
+  double binMin, slope, inv_slope, top;
+  __device__ BinMap(double mn, double sl, int bins)
+      : binMin(mn), slope(sl), inv_slope(1.0 / sl), top((double)bins - 1.5) {}
+  __device__ __forceinline__ double coord(float x) const {
+    const double d = (double)x - binMin;
+    const double c = d * inv_slope;
+    return c > top ? d / slope : c;
+  }
+};
 
 // Fractional histogram contribution of one value (N4.py:21-29) from its
 // FP64 bin coordinate, as 2^24 fixed-point weights.  Returns the bin or -1

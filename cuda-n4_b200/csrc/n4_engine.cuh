@@ -313,7 +313,7 @@ struct Engine {
   }
 
   // ---- pass B + sharpening: histogram of logU over the group, then E
-  __device__ bool pass_b(double bmin, double slope, double inv_slope) {
+  __device__ bool pass_b(const BinMap &bm) {
     const int bins = pr.bins;
     for (int i = threadIdx.x; i < kHistCopies * bins; i += blockDim.x) hist[i] = 0ull;
     __syncthreads();
@@ -325,7 +325,7 @@ struct Engine {
       unsigned qlo = 0, qhi = 0;
       if (i < n) {
         const float lu = logu[i];
-        if (!isnan(lu)) key = hist_bin(bin_coord(lu, bmin, inv_slope), bins, qlo, qhi);
+        if (!isnan(lu)) key = hist_bin(bm.coord(lu), bins, qlo, qhi);
       }
       hist_add_warp(hc, bins, key, qlo, qhi);
     }
@@ -340,18 +340,18 @@ struct Engine {
     for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (double)Hs[b] * kHistInvScale;
     __syncthreads();
     SharpenBufs sb{fa, fb, tw, Ff};
-    sharpen_map(H, bins, pl.npad, pl.hoff, bmin, slope, pr.wiener, pr.fwhm, sb, E);
+    sharpen_map(H, bins, pl.npad, pl.hoff, bm.binMin, bm.slope, pr.wiener, pr.fwhm, sb, E);
     return true;
   }
 
   // ---- pass C: residual in place of logU (0 outside the mask)
-  __device__ void pass_c(double bmin, double inv_slope, bool degenerate) {
+  __device__ void pass_c(const BinMap &bm, bool degenerate) {
     const int n = nrow * Z;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const float lu = logu[i];
       float r = 0.0f;
       if (!isnan(lu) && !degenerate)
-        r = (float)((double)lu - sharpened_value(bin_coord(lu, bmin, inv_slope), E, pr.bins));
+        r = (float)((double)lu - sharpened_value(bm.coord(lu), E, pr.bins));
       logu[i] = r;
     }
     __syncthreads();
@@ -363,9 +363,9 @@ struct Engine {
     const double bmin = st[0], bmax = st[1];
     const double slope = (bmax - bmin) / (double)(pr.bins - 1);
     const bool degenerate = !(slope > 0.0) || !isfinite(slope);
-    const double inv_slope = degenerate ? 0.0 : 1.0 / slope;
-    if (!degenerate) { if (!pass_b(bmin, slope, inv_slope)) return false; }
-    pass_c(bmin, inv_slope, degenerate);
+    const BinMap bm(bmin, degenerate ? 1.0 : slope, pr.bins);
+    if (!degenerate) { if (!pass_b(bm)) return false; }
+    pass_c(bm, degenerate);
     contract(true);
     if (!allreduce(slotC, D, nlat)) return false;
     for (int c = threadIdx.x; c < nlat; c += blockDim.x) {

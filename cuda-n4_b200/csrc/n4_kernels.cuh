@@ -428,13 +428,14 @@ __global__ void k_hist(const float *x, const float *mask, long long n, const dou
   extern __shared__ unsigned long long hs[];
   for (int i = threadIdx.x; i < bins; i += blockDim.x) hs[i] = 0ull;
   __syncthreads();
-  const double bmin = stats[0], inv = stats[3];
+  const double inv = stats[3];
+  const BinMap bm(stats[0], inv > 0.0 ? stats[2] : 1.0, bins);
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long base = blockIdx.x * (long long)blockDim.x; base < n; base += stride) {
     const long long i = base + threadIdx.x;
     int key = -1;
     unsigned qlo = 0, qhi = 0;
-    if (i < n && inv > 0.0 && (!mask || mask[i] != 0.0f)) key = hist_bin(bin_coord(x[i], bmin, inv), bins, qlo, qhi);
+    if (i < n && inv > 0.0 && (!mask || mask[i] != 0.0f)) key = hist_bin(bm.coord(x[i]), bins, qlo, qhi);
     hist_add_warp(hs, bins, key, qlo, qhi);
   }
   __syncthreads();
@@ -463,10 +464,11 @@ __global__ void k_sharpen(const unsigned long long *hist, const double *stats, i
 
 __global__ void k_remap(const float *x, const float *mask, long long n, const double *stats, const double *E,
                         int bins, float *out) {
-  const double bmin = stats[0], inv = stats[3];
+  const double inv = stats[3];
+  const BinMap bm(stats[0], inv > 0.0 ? stats[2] : 1.0, bins);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     if (mask && mask[i] == 0.0f) { out[i] = 0.0f; continue; }
-    out[i] = inv > 0.0 ? (float)sharpened_value(bin_coord(x[i], bmin, inv), E, bins) : x[i];
+    out[i] = inv > 0.0 ? (float)sharpened_value(bm.coord(x[i]), E, bins) : x[i];
   }
 }
 

@@ -110,7 +110,9 @@ def test_cluster_and_grid_paths_agree(cuda):
     a = n4b200.N4(im, mk, param(3, [10] * 3, 0.0))
     b = n4b200.N4(im, mk, param(3, [10] * 3, 0.0, flags=0x8))
     assert a.report["path"] == "cluster" and b.report["path"] == "grid"
-    assert nrel(a.lattice, b.lattice.cpu().numpy().astype(np.float64)) < 1e-5
+    # different partitions sum in different orders; N4 amplifies the FP32
+    # difference (~2e-5 here), so the paths are compared at the parity bound
+    assert nrel(a.lattice, b.lattice.cpu().numpy().astype(np.float64)) < TOL
 
 
 def test_deterministic(cuda):
@@ -162,7 +164,10 @@ def test_warm_start(cuda):
     good = n4b200.N4(im, mk, p1, warm_lattice=plain.lattice)
     assert good.report["warm_start_used"]
     assert good.report["iterations"][0] < plain.report["iterations"][0]
-    bad = n4b200.N4(im, mk, p1, warm_lattice=cuda.full((4, 4, 4), 2.0, device="cuda"))
+    # a constant lattice only rescales the intensities (invisible to N4); a
+    # spatially varying wrong one is what the first-iteration rule rejects
+    wrong = cuda.tensor(np.random.default_rng(0).normal(0.0, 1.0, (4, 4, 4)), dtype=cuda.float32, device="cuda")
+    bad = n4b200.N4(im, mk, p1, warm_lattice=wrong)
     assert not bad.report["warm_start_used"]
     assert bad.report["iterations"] == plain.report["iterations"]
     assert nrel(bad.lattice, plain.lattice.cpu().numpy().astype(np.float64)) < 1e-6

