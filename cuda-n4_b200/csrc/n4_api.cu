@@ -12,6 +12,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "n4_kernels.cuh"
@@ -114,6 +115,9 @@ struct n4_context {
   cudaStream_t last_stream = nullptr;
   cudaEvent_t last_done = nullptr;
   std::map<TuneKey, TuneVal> tune;
+  // max co-resident clusters per (threads, cluster size, shared bytes)
+  std::map<std::tuple<int, int, int>, int> cluster_cap;
+  int attr_smem[2] = {0, 0};   // dynamic shared memory already granted (512, 1024 threads)
   // profiling
   int profiling = 0;
   cudaEvent_t ev[5] = {};
@@ -220,10 +224,13 @@ Plan make_plan(const n4_params_t *p, int K, const std::vector<Dims> &vols, bool 
     pl.Ymax = std::max(pl.Ymax, d.Y);
     pl.Zmax = std::max(pl.Zmax, d.Z);
     const long long rows = (long long)d.X * d.Y;
-    const long long rpc = (rows + K - 1) / K;
+    // grid: contiguous rows; cluster: whole x-planes, ceil(X / K) per CTA
+    const long long rpc = grid ? (rows + K - 1) / K : ((long long)d.X + K - 1) / K * d.Y;
     rows_max = std::max(rows_max, rpc);
     slab = std::max(slab, rpc * d.Z);
-    nvxl = std::max(nvxl, (rpc - 1) / d.Y + 2);
+    // the y contraction spans every x-plane a CTA touches: all of them when
+    // rows are interleaved (cluster), a contiguous range otherwise (grid)
+    nvxl = std::max(nvxl, grid ? (rpc - 1) / d.Y + 2 : ((long long)d.X + K - 1) / K);
   }
   pl.slab_floats = (int)slab;
   pl.rows_max = (int)rows_max;
@@ -238,7 +245,8 @@ Plan make_plan(const n4_params_t *p, int K, const std::vector<Dims> &vols, bool 
   pl.o_den = take((size_t)pl.NLAT * 4);
   pl.o_tmp = take((size_t)pl.NLAT * 4);
   pl.o_aux = take((size_t)pl.NLAT * 4);
-  pl.o_hist = take((size_t)kHistCopies * pl.bins * 8);
+  pl.o_hist = take((size_t)kHistCopies * pl.bins * 4);
+  pl.o_H64 = take((size_t)pl.bins * 8);
   pl.o_H = take((size_t)pl.bins * 8);
   pl.o_E = take((size_t)pl.bins * 8);
   pl.o_fa = take((size_t)pl.npad * 16);
@@ -259,7 +267,11 @@ Plan make_plan(const n4_params_t *p, int K, const std::vector<Dims> &vols, bool 
   pl.b_slotA = take(sizeof(Stats));
   pl.b_slotB = take((size_t)pl.bins * 8);
   pl.b_slotC = take((size_t)pl.NLAT * 4);
+  pl.b_slice = take(std::max((size_t)(pl.NLAT + K - 1) / K * 4, (size_t)(pl.bins + K - 1) / K * 8));
   pl.big_bytes = (int)align_up(o, 128);
+  // a histogram copy (one per 8th warp) receives at most n/8 + NT/8 of a
+  // CTA's n voxels (NT <= 1024 threads); its 32-bit bins must not overflow
+  pl.hist_shift = hist_shift_for(((long long)rows_max * pl.Zmax + 7) / 8 + 160);
   return pl;
 }
 
@@ -270,8 +282,12 @@ bool cluster_fits(const n4_context *ctx, const Plan &pl) {
 template <int NT>
 n4_status_t cluster_capacity(n4_context *ctx, int K, int smem, int *nclusters) {
   auto kern = k_n4_cluster<NT>;
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  int &granted = ctx->attr_smem[NT == 1024 ? 1 : 0];
+  if (smem > granted) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    granted = smem;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(K);
   cfg.blockDim = dim3(NT);
@@ -290,7 +306,12 @@ n4_status_t cluster_capacity(n4_context *ctx, int K, int smem, int *nclusters) {
 }
 
 n4_status_t capacity(n4_context *ctx, int nt, int K, int smem, int *n) {
-  return nt == 1024 ? cluster_capacity<1024>(ctx, K, smem, n) : cluster_capacity<512>(ctx, K, smem, n);
+  const auto key = std::make_tuple(nt, K, smem);
+  auto it = ctx->cluster_cap.find(key);
+  if (it != ctx->cluster_cap.end()) { *n = it->second; return N4_OK; }
+  TRY(nt == 1024 ? cluster_capacity<1024>(ctx, K, smem, n) : cluster_capacity<512>(ctx, K, smem, n));
+  ctx->cluster_cap[key] = *n;
+  return N4_OK;
 }
 
 // Largest cluster (<= 16 CTAs) whose per-CTA share of every volume fits.
@@ -418,10 +439,15 @@ n4_status_t launch_grid_path(n4_context *ctx, const n4_params_t *p, const Params
 }
 
 template <int NT>
-n4_status_t launch_cluster_kernel(const ClusterArgs &a, int K, int nclusters, int smem, cudaStream_t st) {
+n4_status_t launch_cluster_kernel(n4_context *ctx, const ClusterArgs &a, int K, int nclusters, int smem,
+                                  cudaStream_t st) {
   auto kern = k_n4_cluster<NT>;
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  int &granted = ctx->attr_smem[NT == 1024 ? 1 : 0];
+  if (smem > granted) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    granted = smem;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(K * nclusters);
   cfg.blockDim = dim3(NT);
@@ -611,8 +637,8 @@ n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector
     a.queue = u.dp<int>(o_q);
     a.use_tma = 1;
     const int ncl = std::min<int>(cap, (int)in_cluster.size());
-    if (ch.nt == 1024) TRY(launch_cluster_kernel<1024>(a, ch.K, ncl, smem, st));
-    else TRY(launch_cluster_kernel<512>(a, ch.K, ncl, smem, st));
+    if (ch.nt == 1024) TRY(launch_cluster_kernel<1024>(ctx, a, ch.K, ncl, smem, st));
+    else TRY(launch_cluster_kernel<512>(ctx, a, ch.K, ncl, smem, st));
     for (int i : in_cluster) { slot.path[i] = 1; slot.csize[i] = ch.K; }
     ++launches;
   }
@@ -960,11 +986,13 @@ n4_status_t n4_sharpen_image(n4_context_t *ctx, const float *d_before, const flo
   k_minmax<<<nb, 256, 0, st>>>(d_before, d_mask, n, part);
   k_minmax_final<<<1, 256, 0, st>>>(part, nb, bins, stats);
   CK(cudaMemsetAsync(hist, 0, (size_t)bins * 8, st));
-  k_hist<<<nb, 256, bins * 8, st>>>(d_before, d_mask, n, stats, bins, hist);
+  // one block sees at most (grid-stride trips) x 256 voxels
+  const int shift = hist_shift_for(((long long)n + (long long)nb * 256 - 1) / ((long long)nb * 256) * 256);
+  k_hist<<<nb, 256, bins * 4, st>>>(d_before, d_mask, n, stats, bins, shift, hist);
   const int npad = npad_of(bins), hoff = (int)(0.5 * (npad - bins));
   const int smem = npad * (16 * 3 + 8) + bins * 16;
   CK(cudaFuncSetAttribute(k_sharpen, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_sharpen<<<1, 512, smem, st>>>(hist, stats, bins, npad, hoff, decimal_of(wiener), decimal_of(fwhm), E);
+  k_sharpen<<<1, 512, smem, st>>>(hist, stats, bins, shift, npad, hoff, decimal_of(wiener), decimal_of(fwhm), E);
   k_remap<<<nb, 256, 0, st>>>(d_before, d_mask, n, stats, E, bins, d_after);
   CK(cudaGetLastError());
   double hs[4];

@@ -19,9 +19,8 @@ namespace n4 {
 
 constexpr int kMaxThreads = 1024;
 constexpr unsigned kFull = 0xffffffffu;
-constexpr float kHistScale = 16777216.0f;        // 2^24 fixed-point histogram weight
-constexpr double kHistInvScale = 1.0 / 16777216.0;
-constexpr int kHistCopies = 4;                   // shared histogram copies per CTA
+constexpr int kHistCopies = 8;                   // shared histogram copies per CTA
+constexpr int kHistMaxShift = 24;                // fixed-point weight 2^shift, shift <= 24
 constexpr unsigned long long kSpinLimit = 1ull << 25;   // bounded waits (~2-4 s)
 
 // ---------------------------------------------------------------- tables
@@ -35,6 +34,8 @@ struct Axis {
   float4 *w;    // [n]   cubic weights B0..B3
   float *p;     // [4][n] fit numerator weights  w_j^3 / sum_k w_k^2
   float *q;     // [4][n] fit denominator weights w_j^2
+  float4 *p4;   // [n]   the same numerator weights, packed per voxel
+  float4 *q4;   // [n]   the same denominator weights, packed per voxel
   int *lo, *hi; // [nsp] voxel range of each span
 };
 
@@ -44,6 +45,7 @@ __host__ __device__ inline size_t axis_bytes(int n, int nsp) {
   b += ((size_t)n * 4 + 15) / 16 * 16;          // s
   b += (size_t)n * 16;                           // w
   b += (size_t)n * 16 * 2;                       // p, q
+  b += (size_t)n * 16 * 2;                       // p4, q4
   b += ((size_t)nsp * 8 + 15) / 16 * 16;         // lo, hi
   return b;
 }
@@ -56,6 +58,8 @@ __host__ __device__ inline Axis axis_at(char *base, int n, int nc) {
   a.w = (float4 *)p; p += (size_t)n * 16;
   a.p = (float *)p;  p += (size_t)n * 16;
   a.q = (float *)p;  p += (size_t)n * 16;
+  a.p4 = (float4 *)p; p += (size_t)n * 16;
+  a.q4 = (float4 *)p; p += (size_t)n * 16;
   a.lo = (int *)p;   a.hi = a.lo + a.nsp;
   return a;
 }
@@ -91,6 +95,8 @@ __device__ void build_axis(const Axis &a) {
     a.q[1 * a.n + i] = (float)(w1 * w1);
     a.q[2 * a.n + i] = (float)(w2 * w2);
     a.q[3 * a.n + i] = (float)(w3 * w3);
+    a.p4[i] = make_float4(a.p[i], a.p[a.n + i], a.p[2 * a.n + i], a.p[3 * a.n + i]);
+    a.q4[i] = make_float4(a.q[i], a.q[a.n + i], a.q[2 * a.n + i], a.q[3 * a.n + i]);
   }
   // voxel range of every span by binary search on the monotone span index
   for (int sp = threadIdx.x; sp < a.nsp; sp += blockDim.x) {
@@ -233,8 +239,7 @@ __device__ double2 *fft_forward(double2 *a, double2 *b, int N, const double2 *tw
   int Ns = 1;
   int rem = N;
   while (rem > 1) {
-    if (rem % 8 == 0 && rem != 16 && rem != 32) { stockham_pass<8>(a, b, N, Ns, tw); Ns *= 8; rem /= 8; }
-    else if (rem % 4 == 0) { stockham_pass<4>(a, b, N, Ns, tw); Ns *= 4; rem /= 4; }
+    if (rem % 4 == 0) { stockham_pass<4>(a, b, N, Ns, tw); Ns *= 4; rem /= 4; }
     else { stockham_pass<2>(a, b, N, Ns, tw); Ns *= 2; rem /= 2; }
     __syncthreads();
     double2 *t = a; a = b; b = t;
@@ -321,33 +326,41 @@ struct BinMap {
 };
 
 // Fractional histogram contribution of one value (N4.py:21-29) from its
-// FP64 bin coordinate, as 2^24 fixed-point weights.  Returns the bin or -1
-// when the value adds nothing.
-__device__ __forceinline__ int hist_bin(double c, int bins, unsigned &qlo, unsigned &qhi) {
+// FP64 bin coordinate, as fixed-point weights of 2^shift per voxel (the two
+// parts of a split add up to exactly one voxel).  Returns the bin or -1 when
+// the value adds nothing.
+__device__ __forceinline__ int hist_bin(double c, int bins, double scale, unsigned &qlo, unsigned &qhi) {
   if (!(c >= 0.0) || !(c < (double)bins)) return -1;   // NaN / out of range (defensive)
   const double fc = floor(c);
   const double off = c - fc;
   const int idx = (int)fc;
-  if (off == 0.0) { qlo = 16777216u; qhi = 0u; return idx; }
+  const unsigned one = (unsigned)scale;
+  if (off == 0.0) { qlo = one; qhi = 0u; return idx; }
   if (idx < bins - 1) {
-    qhi = (unsigned)__double2uint_rn(off * 16777216.0);
-    qlo = 16777216u - qhi;
+    qhi = (unsigned)__double2uint_rn(off * scale);
+    qlo = one - qhi;
     return idx;
   }
   return -1;                                             // the reference drops it
 }
 
-// Warp-aggregated add of one value into a shared u64 histogram.  All 32
+// Largest shift <= 24 for which `n` voxels cannot overflow a 32-bit bin.
+__host__ __device__ inline int hist_shift_for(long long n) {
+  int s = kHistMaxShift;
+  while (s > 0 && (unsigned long long)n << s > 0xffffffffull) --s;
+  return s;
+}
+
+// Warp-aggregated add of one value into a shared 32-bit histogram.  All 32
 // lanes must call it (lanes without a value pass key < 0).
-__device__ __forceinline__ void hist_add_warp(unsigned long long *h, int bins, int key,
-                                              unsigned qlo, unsigned qhi) {
-  unsigned grp = __match_any_sync(kFull, key);
+__device__ __forceinline__ void hist_add_warp(unsigned *h, int bins, int key, unsigned qlo, unsigned qhi) {
+  const unsigned grp = __match_any_sync(kFull, key);
   if (key >= 0) {
-    unsigned slo = __reduce_add_sync(grp, qlo);
-    unsigned shi = __reduce_add_sync(grp, qhi);
+    const unsigned slo = __reduce_add_sync(grp, qlo);
+    const unsigned shi = __reduce_add_sync(grp, qhi);
     if ((threadIdx.x & 31) == (unsigned)(__ffs(grp) - 1)) {
-      atomicAdd(&h[key], (unsigned long long)slo);
-      if (shi && key + 1 < bins) atomicAdd(&h[key + 1], (unsigned long long)shi);
+      atomicAdd(&h[key], slo);
+      if (shi && key + 1 < bins) atomicAdd(&h[key + 1], shi);
     }
   }
 }

@@ -34,13 +34,13 @@ struct Plan {
   // limits
   int levels, nc0x, nc0y, nc0z, NCX, NCY, NCZ, NLAT;
   int Xmax, Ymax, Zmax, slab_floats, rows_max, nvxl;
-  int bins, npad, hoff;
+  int bins, npad, hoff, hist_shift;
   // shared
-  int o_ax, o_ay, o_az, o_L, o_D, o_den, o_tmp, o_aux, o_hist, o_H, o_E;
+  int o_ax, o_ay, o_az, o_L, o_D, o_den, o_tmp, o_aux, o_hist, o_H64, o_H, o_E;
   int o_fa, o_fb, o_tw, o_ff, o_red, o_misc;
   int sm_bytes;
   // big
-  int b_imlog, b_logu, b_G, b_Gd, b_T2, b_slotA, b_slotB, b_slotC, big_bytes;
+  int b_imlog, b_logu, b_G, b_Gd, b_T2, b_slotA, b_slotB, b_slotC, b_slice, big_bytes;
 };
 
 struct Params {
@@ -90,9 +90,31 @@ struct GridGroup {
   static constexpr bool kGrid = true;
 };
 
+// ------------------------------------------------------------------ phase timers
+// Compile with -DN4_PHASE_TIMERS to print, per volume, the cycles thread 0
+// of the first CTA spends between phase marks (measurement builds only).
+#ifdef N4_PHASE_TIMERS
+#define N4_MARK(k)                                                     \
+  do {                                                                 \
+    if (threadIdx.x == 0) {                                            \
+      const long long t_ = clock64();                                  \
+      ph_acc[k] += t_ - ph_last;                                       \
+      ph_last = t_;                                                    \
+    }                                                                  \
+  } while (0)
+#else
+#define N4_MARK(k) do { } while (0)
+#endif
+enum { PH_SETUP, PH_A, PH_B, PH_SHARP, PH_C, PH_FIT, PH_UPDATE, PH_A_LOOP, PH_A_RED, PH_B_ZERO, PH_B_LOOP, PH_B_MERGE,
+       PH_B_RED, PH_F_T1, PH_F_T2, PH_F_P, PH_F_RED, PH_N };
+
 // ------------------------------------------------------------------ engine
 template <class Group>
 struct Engine {
+#ifdef N4_PHASE_TIMERS
+  long long ph_acc[PH_N] = {};
+  long long ph_last = 0;
+#endif
   Group g;
   const Plan &pl;
   const Params &pr;
@@ -100,7 +122,10 @@ struct Engine {
   char *big;
   float *red_global;   // grid path: [NLAT] / [bins] slice-reduction buffer
   // volume
-  int X, Y, Z, r0, r1, nrow, rank, K;
+  int X, Y, Z, nrow, rank, K;
+  // rows of this CTA: grid path, contiguous rows r0 + rl; cluster path,
+  // whole x-planes vx = rank + m * K (m = rl / Y), interleaved over the group
+  int r0, nplane;
   FastDiv divZ;
   const float *imlog;
   float *logu;
@@ -110,7 +135,8 @@ struct Engine {
   // smem views
   float *L, *D, *den, *tmp, *aux;
   double *H, *E, *Ff;
-  unsigned long long *hist;
+  unsigned *hist;
+  unsigned long long *H64;
   double2 *fa, *fb, *tw;
   double *red;
   float *G, *Gd, *T2, *slotC;
@@ -121,7 +147,8 @@ struct Engine {
       : g(g_), pl(p), pr(r), sm(sm_), big(big_), red_global(rg) {
     L = (float *)(sm + pl.o_L); D = (float *)(sm + pl.o_D); den = (float *)(sm + pl.o_den);
     tmp = (float *)(sm + pl.o_tmp); aux = (float *)(sm + pl.o_aux);
-    hist = (unsigned long long *)(sm + pl.o_hist); H = (double *)(sm + pl.o_H); E = (double *)(sm + pl.o_E);
+    hist = (unsigned *)(sm + pl.o_hist); H64 = (unsigned long long *)(sm + pl.o_H64);
+    H = (double *)(sm + pl.o_H); E = (double *)(sm + pl.o_E);
     fa = (double2 *)(sm + pl.o_fa); fb = (double2 *)(sm + pl.o_fb); tw = (double2 *)(sm + pl.o_tw);
     Ff = (double *)(sm + pl.o_ff); red = (double *)(sm + pl.o_red);
     G = (float *)(big + pl.b_G); Gd = (float *)(big + pl.b_Gd); T2 = (float *)(big + pl.b_T2);
@@ -144,13 +171,25 @@ struct Engine {
     __syncthreads();
   }
 
+  __device__ __forceinline__ void row_xy(int rl, int &vx, int &vy) const {
+    if (Group::kGrid) {
+      const int row = r0 + rl;
+      vx = row / Y;
+      vy = row - vx * Y;
+    } else {
+      const int m = rl / Y;
+      vx = rank + m * K;
+      vy = rl - m * Y;
+    }
+  }
+
   // ---- rows(lat) -> Gt: x/y contraction of the lattice for every local row
   __device__ void rowtab(const float *lat, float *Gt) {
     const int ntask = nrow * ncz;
     for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
       const int rl = t / ncz, cz = t - rl * ncz;
-      const int row = r0 + rl;
-      const int vx = row / Y, vy = row - vx * Y;
+      int vx, vy;
+      row_xy(rl, vx, vy);
       const int sx = ax.s[vx], sy = ay.s[vy];
       const float4 wx = ax.w[vx], wy = ay.w[vy];
       const float wxa[4] = {wx.x, wx.y, wx.z, wx.w};
@@ -196,89 +235,147 @@ struct Engine {
     return true;
   }
 
-  // Sum of every CTA's `mine[0..n)` into `out` (shared), identical in all CTAs.
+  // Sum of every CTA's `mine[0..n)` into `out` (shared), identical in all
+  // CTAs: each CTA reduces one slice over all peers (fixed order), then every
+  // CTA gathers the slices.  Slices live in a buffer of their own, so a CTA
+  // may modify `out` while slower peers are still gathering.
   template <class T>
   __device__ bool allreduce(const T *mine, T *out, int n) {
     if (!g.sync()) return false;
-    if (!Group::kGrid) {
-      for (int c = threadIdx.x; c < n; c += blockDim.x) {
-        T acc = 0;
-        for (int k = 0; k < K; ++k) acc += g.load(g.peer(mine, k) + c);
-        out[c] = acc;
-      }
-      __syncthreads();
-      return true;
-    }
-    // grid: each CTA reduces a slice into global memory, then all copy it
-    T *rg = (T *)red_global;
     const int per = (n + K - 1) / K;
     const int c0 = rank * per, c1 = min(n, c0 + per);
+    T *slice = Group::kGrid ? (T *)red_global : (T *)(big + pl.b_slice);
     for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
       T acc = 0;
+#pragma unroll 4
       for (int k = 0; k < K; ++k) acc += g.load(g.peer(mine, k) + c);
-      rg[c] = acc;
+      slice[Group::kGrid ? c : c - c0] = acc;
     }
     if (!g.sync()) return false;
-    for (int c = threadIdx.x; c < n; c += blockDim.x) out[c] = __ldcg(rg + c);
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+      if (Group::kGrid) {
+        out[c] = __ldcg(slice + c);
+      } else {
+        const int owner = c / per;
+        out[c] = *(g.peer(slice, owner) + (c - owner * per));
+      }
+    }
     __syncthreads();
     return true;
   }
 
   // ---- separable fit contraction of the local rows into slotC (full lattice)
-  // num: values R (logu) with weights p; den: mask with weights q.
-  __device__ void contract(bool num_mode) {
+  // num: residuals R = logU - remap(logU) (computed here, fused with pass C)
+  // with weights w^3/sum w^2; den: the mask with weights w^2 (N4.py:224-236).
+  //   T1[row][cz]   z contraction: one thread per (row, z-span) accumulates
+  //                 the span's 4 targets in registers; spans s = phi mod 4
+  //                 never share a target, so 4 phases add without atomics in
+  //                 a fixed order
+  //   T2[vx][cy][cz] y contraction over the CTA's rows of each x-plane
+  //   slotC[c]       x contraction (the CTA's partial lattice)
+  __device__ void contract(bool num_mode, const BinMap &bm, bool degenerate) {
     float *T1 = Gd;   // Gd is dead between pass A and the next update
-    const float *P = num_mode ? az.p : az.q;
     const int nt1 = nrow * ncz;
-    for (int t = threadIdx.x; t < nt1; t += blockDim.x) {
-      const int rl = t / ncz, cz = t - rl * ncz;
-      float acc = 0.0f;
-      for (int j = 0; j < 4; ++j) {
-        const int sp = cz - j;
-        if (sp < 0 || sp >= az.nsp) continue;
-        const float *wz = P + j * Z;
+    for (int t = threadIdx.x; t < nt1; t += blockDim.x) T1[t] = 0.0f;
+    __syncthreads();
+    const float4 *W4 = num_mode ? az.p4 : az.q4;
+    for (int phase = 0; phase < 4; ++phase) {
+      const int nsp = phase < az.nsp ? (az.nsp - phase + 3) / 4 : 0;   // spans phase, phase+4, ...
+      const int ntask = nrow * nsp;
+      for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
+        const int rl = t / nsp, sp = phase + 4 * (t - rl * nsp);
         const int lo = az.lo[sp], hi = az.hi[sp];
+        float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
         if (num_mode) {
-          const float *rv = logu + (size_t)rl * Z;
-          for (int vz = lo; vz < hi; ++vz) acc = __fmaf_rn(wz[vz], rv[vz], acc);
+          const float *lu = logu + (size_t)rl * Z;
+          if (!degenerate) {
+            for (int vz = lo; vz < hi; ++vz) {
+              const float x = lu[vz];
+              if (isnan(x)) continue;
+              const float r = (float)((double)x - sharpened_value(bm.coord(x), E, pr.bins));
+              const float4 w = W4[vz];
+              a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
+              a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
+            }
+          }
         } else {
           const float *iv = imlog + (size_t)rl * Z;
-          for (int vz = lo; vz < hi; ++vz) acc += isnan(iv[vz]) ? 0.0f : wz[vz];
+          for (int vz = lo; vz < hi; ++vz) {
+            if (isnan(iv[vz])) continue;
+            const float4 w = W4[vz];
+            a0 += w.x; a1 += w.y; a2 += w.z; a3 += w.w;
+          }
         }
+        float *t1 = T1 + rl * ncz + sp;
+        t1[0] += a0; t1[1] += a1; t1[2] += a2; t1[3] += a3;
       }
-      T1[t] = acc;
+      __syncthreads();
     }
-    __syncthreads();
+    N4_MARK(PH_F_T1);
     const float *PY = num_mode ? ay.p : ay.q;
     const float *PX = num_mode ? ax.p : ax.q;
-    const int vx0 = r0 / Y, vx1 = (r1 - 1) / Y;
-    const int nvx = vx1 - vx0 + 1;
-    const int nt2 = nvx * ncy * ncz;
+    if (Group::kGrid) {
+      // contiguous rows: planes vx0..vx1, partially covered at both ends
+      const int vx0 = r0 / Y, vx1 = (r0 + nrow - 1) / Y;
+      const int nt2 = (vx1 - vx0 + 1) * ncy * ncz;
+      for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
+        const int cz = t % ncz, cy = (t / ncz) % ncy, xl = t / (ncz * ncy);
+        const int rb = (vx0 + xl) * Y - r0;   // local row of (vx, 0)
+        float acc = 0.0f;
+        for (int j = 0; j < 4; ++j) {
+          const int sp = cy - j;
+          if (sp < 0 || sp >= ay.nsp) continue;
+          const int lo = max(ay.lo[sp], -rb), hi = min(ay.hi[sp], nrow - rb);
+          const float *wy = PY + j * Y;
+          for (int vy = lo; vy < hi; ++vy) acc = __fmaf_rn(wy[vy], T1[(rb + vy) * ncz + cz], acc);
+        }
+        T2[t] = acc;
+      }
+      __syncthreads();
+      N4_MARK(PH_F_T2);
+      for (int c = threadIdx.x; c < nlat; c += blockDim.x) {
+        const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
+        float acc = 0.0f;
+        for (int j = 0; j < 4; ++j) {
+          const int sp = cx - j;
+          if (sp < 0 || sp >= ax.nsp) continue;
+          const int lo = max(ax.lo[sp], vx0), hi = min(ax.hi[sp], vx1 + 1);
+          const float *wx = PX + j * X;
+          for (int vx = lo; vx < hi; ++vx)
+            acc = __fmaf_rn(wx[vx], T2[((vx - vx0) * ncy + cy) * ncz + cz], acc);
+        }
+        slotC[c] = acc;
+      }
+      return;
+    }
+    // whole planes vx = rank + m*K: y contraction per local plane
+    const int nt2 = nplane * ncy * ncz;
     for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
-      const int cz = t % ncz, cy = (t / ncz) % ncy, xl = t / (ncz * ncy);
-      const int vx = vx0 + xl;
-      const int rbase = vx * Y - r0;        // local row of (vx, 0)
+      const int cz = t % ncz, cy = (t / ncz) % ncy, m = t / (ncz * ncy);
+      const float *t1 = T1 + (size_t)m * Y * ncz + cz;
       float acc = 0.0f;
       for (int j = 0; j < 4; ++j) {
         const int sp = cy - j;
         if (sp < 0 || sp >= ay.nsp) continue;
-        const int lo = max(ay.lo[sp], -rbase), hi = min(ay.hi[sp], nrow - rbase);
         const float *wy = PY + j * Y;
-        for (int vy = lo; vy < hi; ++vy) acc = __fmaf_rn(wy[vy], T1[(rbase + vy) * ncz + cz], acc);
+        for (int vy = ay.lo[sp]; vy < ay.hi[sp]; ++vy) acc = __fmaf_rn(wy[vy], t1[vy * ncz], acc);
       }
       T2[t] = acc;
     }
     __syncthreads();
+    N4_MARK(PH_F_T2);
     for (int c = threadIdx.x; c < nlat; c += blockDim.x) {
       const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
       float acc = 0.0f;
       for (int j = 0; j < 4; ++j) {
         const int sp = cx - j;
         if (sp < 0 || sp >= ax.nsp) continue;
-        const int lo = max(ax.lo[sp], vx0), hi = min(ax.hi[sp], vx1 + 1);
         const float *wx = PX + j * X;
-        for (int vx = lo; vx < hi; ++vx)
-          acc = __fmaf_rn(wx[vx], T2[((vx - vx0) * ncy + cy) * ncz + cz], acc);
+        // local planes inside [lo, hi): vx = rank + m*K
+        const int lo = ax.lo[sp], hi = ax.hi[sp];
+        int m = lo <= rank ? 0 : (lo - rank + K - 1) / K;
+        for (int vx = rank + m * K; vx < hi; vx += K, ++m)
+          acc = __fmaf_rn(wx[vx], T2[(m * ncy + cy) * ncz + cz], acc);
       }
       slotC[c] = acc;
     }
@@ -309,15 +406,20 @@ struct Engine {
     __syncthreads();
     for (int i = 0; i < 4; ++i) loc[i] = red[4 + i];
     __syncthreads();
-    return reduce_stats(loc, st);
+    N4_MARK(PH_A_LOOP);
+    const bool ok = reduce_stats(loc, st);
+    N4_MARK(PH_A_RED);
+    return ok;
   }
 
   // ---- pass B + sharpening: histogram of logU over the group, then E
   __device__ bool pass_b(const BinMap &bm) {
-    const int bins = pr.bins;
-    for (int i = threadIdx.x; i < kHistCopies * bins; i += blockDim.x) hist[i] = 0ull;
+    const int bins = pr.bins, shift = pl.hist_shift;
+    const double scale = ldexp(1.0, shift);
+    for (int i = threadIdx.x; i < kHistCopies * bins; i += blockDim.x) hist[i] = 0u;
     __syncthreads();
-    unsigned long long *hc = hist + ((threadIdx.x >> 5) % kHistCopies) * bins;
+    N4_MARK(PH_B_ZERO);
+    unsigned *hc = hist + ((threadIdx.x >> 5) % kHistCopies) * bins;
     const int n = nrow * Z;
     for (int base = 0; base < n; base += blockDim.x) {
       const int i = base + threadIdx.x;
@@ -325,36 +427,32 @@ struct Engine {
       unsigned qlo = 0, qhi = 0;
       if (i < n) {
         const float lu = logu[i];
-        if (!isnan(lu)) key = hist_bin(bm.coord(lu), bins, qlo, qhi);
+        if (!isnan(lu)) key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
       }
-      hist_add_warp(hc, bins, key, qlo, qhi);
+      if (key >= 0) {
+        atomicAdd(&hc[key], qlo);
+        if (qhi) atomicAdd(&hc[key + 1], qhi);
+      }
     }
     __syncthreads();
+    N4_MARK(PH_B_LOOP);
     for (int b = threadIdx.x; b < bins; b += blockDim.x) {
       unsigned long long s = 0;
       for (int c = 0; c < kHistCopies; ++c) s += hist[c * bins + b];
       slotB[b] = s;
     }
-    unsigned long long *Hs = hist;   // reuse copy 0 for the group sum
-    if (!allreduce(slotB, Hs, bins)) return false;
-    for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (double)Hs[b] * kHistInvScale;
     __syncthreads();
+    N4_MARK(PH_B_MERGE);
+    if (!allreduce(slotB, H64, bins)) return false;
+    N4_MARK(PH_B_RED);
+    const double inv = ldexp(1.0, -shift);
+    for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (double)H64[b] * inv;
+    __syncthreads();
+    N4_MARK(PH_B);
     SharpenBufs sb{fa, fb, tw, Ff};
     sharpen_map(H, bins, pl.npad, pl.hoff, bm.binMin, bm.slope, pr.wiener, pr.fwhm, sb, E);
+    N4_MARK(PH_SHARP);
     return true;
-  }
-
-  // ---- pass C: residual in place of logU (0 outside the mask)
-  __device__ void pass_c(const BinMap &bm, bool degenerate) {
-    const int n = nrow * Z;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const float lu = logu[i];
-      float r = 0.0f;
-      if (!isnan(lu) && !degenerate)
-        r = (float)((double)lu - sharpened_value(bm.coord(lu), E, pr.bins));
-      logu[i] = r;
-    }
-    __syncthreads();
   }
 
   // ---- one sharpen + fit step from the current G; leaves the update in D
@@ -365,9 +463,12 @@ struct Engine {
     const bool degenerate = !(slope > 0.0) || !isfinite(slope);
     const BinMap bm(bmin, degenerate ? 1.0 : slope, pr.bins);
     if (!degenerate) { if (!pass_b(bm)) return false; }
-    pass_c(bm, degenerate);
-    contract(true);
+    N4_MARK(PH_C);
+    contract(true, bm, degenerate);
+    __syncthreads();
+    N4_MARK(PH_F_P);
     if (!allreduce(slotC, D, nlat)) return false;
+    N4_MARK(PH_F_RED);
     for (int c = threadIdx.x; c < nlat; c += blockDim.x) {
       const float nu = D[c], de = den[c];
       D[c] = pr.zero_den ? (de != 0.0f ? nu / de : 0.0f) : nu / (de + pr.eps);
@@ -388,15 +489,24 @@ struct Engine {
     X = job.X; Y = job.Y; Z = job.Z;
     rank = g.rank(); K = g.size();
     const int rows = X * Y;
-    r0 = (int)((long long)rows * rank / K);
-    r1 = (int)((long long)rows * (rank + 1) / K);
-    nrow = r1 - r0;
+    if (Group::kGrid) {            // contiguous rows: the volume lives in global memory
+      r0 = (int)((long long)rows * rank / K);
+      nrow = (int)((long long)rows * (rank + 1) / K) - r0;
+      nplane = 0;
+    } else {                       // interleaved planes: every CTA samples the whole volume
+      r0 = 0;
+      nplane = X > rank ? (X - rank + K - 1) / K : 0;
+      nrow = nplane * Y;
+    }
     divZ = FastDiv((unsigned)Z);
     imlog = imlog_in;
     logu = logu_in;
     const bool lead = (rank == 0 && threadIdx.x == 0);
     n4_report_t *rep = job.report;
 
+#ifdef N4_PHASE_TIMERS
+    if (threadIdx.x == 0) ph_last = clock64();
+#endif
     fft_twiddles(tw, pl.npad);
     // foreground count of the group
     float cnt = 0.0f;
@@ -435,7 +545,7 @@ struct Engine {
         __syncthreads();
       }
       // constant denominator of the fit at this level
-      contract(false);
+      contract(false, BinMap(0.0, 1.0, pr.bins), true);
       if (!allreduce(slotC, den, nlat)) goto timeout;
       rowtab(L, G);
       __syncthreads();
@@ -483,8 +593,10 @@ struct Engine {
           rep->first_cv_plain = cvs[1];
         }
       }
+      N4_MARK(PH_SETUP);
       for (;;) {
         if (!pass_a(it > 0, st)) goto timeout;
+        N4_MARK(PH_A);
         if (it > 0) cv = cv_from(st, nfg);
         if (!((double)cv > pr.thr) || it >= maxIt) break;
         if (!fit_step(st)) goto timeout;
@@ -493,6 +605,7 @@ struct Engine {
         rowtab(D, Gd);
         rowtab(L, G);
         __syncthreads();
+        N4_MARK(PH_UPDATE);
         ++it;
       }
       if (lead) { rep->iterations[level] = it; rep->final_cv[level] = cv; rep->levels = level + 1; }
@@ -501,6 +614,15 @@ struct Engine {
       for (int c = threadIdx.x; c < nlat; c += blockDim.x) job.lattice_out[c] = L[c];
       if (threadIdx.x == 0) rep->status = N4_OK;
     }
+#ifdef N4_PHASE_TIMERS
+    if (lead)
+      printf("N4PHASE K=%d nt=%d setup=%lld A=%lld Aloop=%lld Ared=%lld Bzero=%lld Bloop=%lld Bmerge=%lld Bred=%lld "
+             "Bconv=%lld sharp=%lld C=%lld T1=%lld T2=%lld P=%lld Fred=%lld update=%lld\n",
+             K, (int)blockDim.x, ph_acc[PH_SETUP], ph_acc[PH_A], ph_acc[PH_A_LOOP], ph_acc[PH_A_RED],
+             ph_acc[PH_B_ZERO], ph_acc[PH_B_LOOP], ph_acc[PH_B_MERGE], ph_acc[PH_B_RED], ph_acc[PH_B],
+             ph_acc[PH_SHARP], ph_acc[PH_C], ph_acc[PH_F_T1], ph_acc[PH_F_T2], ph_acc[PH_F_P], ph_acc[PH_F_RED],
+             ph_acc[PH_UPDATE]);
+#endif
     return;
   timeout:
     if (lead) rep->status = N4_ERR_TIMEOUT;

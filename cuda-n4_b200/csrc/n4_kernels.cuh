@@ -102,39 +102,42 @@ __device__ unsigned mbar_wait(unsigned long long *mbar, unsigned phase) {
   return done;
 }
 
-// Copy `nfl` floats from global `src` into shared memory with 1-D bulk
-// (TMA) copies; returns the shared pointer at which src[0] landed.  The
-// global buffer must be readable up to 16 bytes past its end.  Every wait is
-// bounded; returns nullptr on timeout.
-__device__ float *stage_slab(const float *src, int nfl, float *dst_base, unsigned long long *mbar,
-                             unsigned &phase, bool use_tma) {
-  if (!use_tma) {
-    for (int i = threadIdx.x; i < nfl; i += blockDim.x) dst_base[i] = src[i];
+// Stage rows rank, rank + K, ... of a [rows][Z] volume into consecutive
+// shared-memory rows.  Rows whose size is a multiple of 16 bytes go by 1-D
+// bulk (TMA) copies completing on an mbarrier; others by plain loads.  Every
+// wait is bounded; returns false on timeout.
+__device__ bool stage_rows(const float *src, int rank, int K, int nrow, int Z, float *dst,
+                           unsigned long long *mbar, unsigned &phase, bool use_tma) {
+  const bool bulk = use_tma && (Z % 4 == 0) && (((uintptr_t)src & 15u) == 0) && nrow > 0;
+  if (!bulk) {
+    for (int i = threadIdx.x; i < nrow * Z; i += blockDim.x) {
+      const int rl = i / Z, z = i - rl * Z;
+      dst[i] = src[(size_t)(rank + rl * K) * Z + z];
+    }
     __syncthreads();
-    return dst_base;
+    return true;
   }
-  const uintptr_t sa = (uintptr_t)src;
-  const int mis = (int)((sa & 15u) >> 2);
-  const char *src_al = (const char *)(sa & ~(uintptr_t)15);
-  const unsigned bytes = (unsigned)(((mis + nfl) * 4 + 15) & ~15);
+  const unsigned row_bytes = (unsigned)Z * 4u;
   if (threadIdx.x == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)),
+                 "r"(row_bytes * (unsigned)nrow)
                  : "memory");
-    const unsigned chunk = 32768;
-    for (unsigned off = 0; off < bytes; off += chunk) {
-      const unsigned sz = bytes - off < chunk ? bytes - off : chunk;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    for (int rl = threadIdx.x; rl < nrow; rl += 32) {
       asm volatile(
           "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-              smem_u32((char *)dst_base + off)),
-          "l"(src_al + off), "r"(sz), "r"(smem_u32(mbar))
+              smem_u32(dst + (size_t)rl * Z)),
+          "l"(src + (size_t)(rank + rl * K) * Z), "r"(row_bytes), "r"(smem_u32(mbar))
           : "memory");
     }
   }
   const unsigned done = mbar_wait(mbar, phase);
   phase ^= 1u;
   __syncthreads();
-  return done ? dst_base + mis : nullptr;
+  return done != 0;
 }
 
 struct ClusterArgs {
@@ -172,11 +175,11 @@ __global__ void __launch_bounds__(NT, 1) k_n4_cluster(const __grid_constant__ Cl
     g.sync();
     if (j >= a.njobs) break;
     const VolJob &job = a.jobs[a.order[j]];
-    int r0, r1;
-    row_range(job.X * job.Y, g.rank(), g.size(), r0, r1);
-    float *slab = stage_slab(job.imlog + (size_t)r0 * job.Z, (r1 - r0) * job.Z,
-                             (float *)(big + s_pl.b_imlog), &s_mbar, phase, a.use_tma != 0);
-    int ok = slab != nullptr;
+    const int rank = g.rank(), K = g.size();
+    const int nplane = job.X > rank ? (job.X - rank + K - 1) / K : 0;
+    float *slab = (float *)(big + s_pl.b_imlog);
+    // planes rank, rank + K, ... (each Y*Z contiguous floats)
+    int ok = stage_rows(job.imlog, rank, K, nplane, job.Y * job.Z, slab, &s_mbar, phase, a.use_tma != 0) ? 1 : 0;
     if (!ok && threadIdx.x == 0) job.report->status = N4_ERR_TIMEOUT;
     // all CTAs of the cluster must agree before starting the volume
     __shared__ int s_ok;
@@ -423,10 +426,10 @@ __global__ void k_minmax_final(const float *part, int nb, int bins, double *stat
   }
 }
 
-__global__ void k_hist(const float *x, const float *mask, long long n, const double *stats, int bins,
+__global__ void k_hist(const float *x, const float *mask, long long n, const double *stats, int bins, int shift,
                        unsigned long long *hist) {
-  extern __shared__ unsigned long long hs[];
-  for (int i = threadIdx.x; i < bins; i += blockDim.x) hs[i] = 0ull;
+  extern __shared__ unsigned hs[];
+  for (int i = threadIdx.x; i < bins; i += blockDim.x) hs[i] = 0u;
   __syncthreads();
   const double inv = stats[3];
   const BinMap bm(stats[0], inv > 0.0 ? stats[2] : 1.0, bins);
@@ -435,23 +438,23 @@ __global__ void k_hist(const float *x, const float *mask, long long n, const dou
     const long long i = base + threadIdx.x;
     int key = -1;
     unsigned qlo = 0, qhi = 0;
-    if (i < n && inv > 0.0 && (!mask || mask[i] != 0.0f)) key = hist_bin(bm.coord(x[i]), bins, qlo, qhi);
+    if (i < n && inv > 0.0 && (!mask || mask[i] != 0.0f)) key = hist_bin(bm.coord(x[i]), bins, ldexp(1.0, shift), qlo, qhi);
     hist_add_warp(hs, bins, key, qlo, qhi);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < bins; i += blockDim.x)
-    if (hs[i]) atomicAdd(&hist[i], hs[i]);
+    if (hs[i]) atomicAdd(&hist[i], (unsigned long long)hs[i]);
 }
 
-__global__ void k_sharpen(const unsigned long long *hist, const double *stats, int bins, int npad, int hoff,
-                          double wiener, double fwhm, double *E_out) {
+__global__ void k_sharpen(const unsigned long long *hist, const double *stats, int bins, int shift, int npad,
+                          int hoff, double wiener, double fwhm, double *E_out) {
   extern __shared__ __align__(16) char sm[];
   double2 *fa = (double2 *)sm, *fb = fa + npad, *tw = fb + npad;
   double *Ff = (double *)(tw + npad);
   double *H = Ff + npad;
   double *E = H + bins;
   fft_twiddles(tw, npad);
-  for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (double)hist[b] * kHistInvScale;
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (double)hist[b] * ldexp(1.0, -shift);
   __syncthreads();
   if (stats[3] > 0.0) {
     SharpenBufs sb{fa, fb, tw, Ff};

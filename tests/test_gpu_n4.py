@@ -87,6 +87,7 @@ def test_c2_shape_shrink4(cuda):
     ph = make_phantom((256, 256, 176), seed=2, sigma=0.02, grid=6, coeff_std=0.25)
     im, mk = cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")
     res = n4b200.N4(im, mk, param(4, [8] * 4, 0.0, ShrinkFactor=4), return_bias=True)
+    assert res.report["path"] == "cluster" and res.report["cluster_size"] == 16
     out, lat, lb = O.N4Shrink(ph.im, ph.mask, 4, low_value=0, maximumNumberOfLevels=4,
                               maximumNumberOfIterations=[8] * 4, ConvergenceThreshold=0.0,
                               return_log_bias=True)
