@@ -265,15 +265,15 @@ struct Engine {
   }
 
   // ---- separable fit contraction of the local rows into slotC (full lattice)
-  // num: residuals R = logU - remap(logU) (computed here, fused with pass C)
-  // with weights w^3/sum w^2; den: the mask with weights w^2 (N4.py:224-236).
+  // num: the residuals left by pass C with weights w^3/sum w^2; den: the mask
+  // with weights w^2 (N4.py:224-236).
   //   T1[row][cz]   z contraction: one thread per (row, z-span) accumulates
   //                 the span's 4 targets in registers; spans s = phi mod 4
   //                 never share a target, so 4 phases add without atomics in
   //                 a fixed order
   //   T2[vx][cy][cz] y contraction over the CTA's rows of each x-plane
   //   slotC[c]       x contraction (the CTA's partial lattice)
-  __device__ void contract(bool num_mode, const BinMap &bm, bool degenerate) {
+  __device__ void contract(bool num_mode) {
     float *T1 = Gd;   // Gd is dead between pass A and the next update
     const int nt1 = nrow * ncz;
     for (int t = threadIdx.x; t < nt1; t += blockDim.x) T1[t] = 0.0f;
@@ -287,16 +287,13 @@ struct Engine {
         const int lo = az.lo[sp], hi = az.hi[sp];
         float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
         if (num_mode) {
-          const float *lu = logu + (size_t)rl * Z;
-          if (!degenerate) {
-            for (int vz = lo; vz < hi; ++vz) {
-              const float x = lu[vz];
-              if (isnan(x)) continue;
-              const float r = (float)((double)x - sharpened_value(bm.coord(x), E, pr.bins));
-              const float4 w = W4[vz];
-              a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
-              a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
-            }
+          const float *rv = logu + (size_t)rl * Z;   // residuals (NaN outside the mask)
+          for (int vz = lo; vz < hi; ++vz) {
+            const float r = rv[vz];
+            if (isnan(r)) continue;
+            const float4 w = W4[vz];
+            a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
+            a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
           }
         } else {
           const float *iv = imlog + (size_t)rl * Z;
@@ -388,7 +385,7 @@ struct Engine {
     const int n = nrow * Z;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const float v = imlog[i];
-      if (isnan(v)) { logu[i] = v; continue; }
+      if (isnan(v)) continue;   // logu keeps NaN there (set when the volume starts)
       const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
       const float lu = __fsub_rn(v, eval(G, rl, vz));
       logu[i] = lu;
@@ -455,6 +452,18 @@ struct Engine {
     return true;
   }
 
+  // ---- pass C: residual R = logU - remap(logU) in place (masked voxels only;
+  // the others stay NaN)
+  __device__ void pass_c(const BinMap &bm, bool degenerate) {
+    const int n = nrow * Z;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float lu = logu[i];
+      if (isnan(lu)) continue;
+      logu[i] = degenerate ? 0.0f : (float)((double)lu - sharpened_value(bm.coord(lu), E, pr.bins));
+    }
+    __syncthreads();
+  }
+
   // ---- one sharpen + fit step from the current G; leaves the update in D
   __device__ bool fit_step(const double st[4]) {
     // bin range of the masked logU (N4.py:14-15); st holds FP32 values
@@ -463,8 +472,9 @@ struct Engine {
     const bool degenerate = !(slope > 0.0) || !isfinite(slope);
     const BinMap bm(bmin, degenerate ? 1.0 : slope, pr.bins);
     if (!degenerate) { if (!pass_b(bm)) return false; }
+    pass_c(bm, degenerate);
     N4_MARK(PH_C);
-    contract(true, bm, degenerate);
+    contract(true);
     __syncthreads();
     N4_MARK(PH_F_P);
     if (!allreduce(slotC, D, nlat)) return false;
@@ -508,6 +518,7 @@ struct Engine {
     if (threadIdx.x == 0) ph_last = clock64();
 #endif
     fft_twiddles(tw, pl.npad);
+    for (int i = threadIdx.x; i < nrow * Z; i += blockDim.x) logu[i] = imlog[i];
     // foreground count of the group
     float cnt = 0.0f;
     double cntd = 0.0;
@@ -545,7 +556,7 @@ struct Engine {
         __syncthreads();
       }
       // constant denominator of the fit at this level
-      contract(false, BinMap(0.0, 1.0, pr.bins), true);
+      contract(false);
       if (!allreduce(slotC, den, nlat)) goto timeout;
       rowtab(L, G);
       __syncthreads();
