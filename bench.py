@@ -61,7 +61,7 @@ def peaks():
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """Samples SM clocks and throttle reasons every 100 ms (NVML)."""
+    """Samples SM clocks and throttle reasons every 20 ms (NVML)."""
 
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
                0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
@@ -92,7 +92,7 @@ class ClockSampler:
                             self.reasons.add(name)
                 except Exception:
                     pass
-                self._stop.wait(0.1)
+                self._stop.wait(0.02)
 
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
@@ -230,8 +230,10 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    h0 = time.perf_counter()
     for _ in range(args.steps):
         step_batched()
+    host_ms = 1000 * (time.perf_counter() - h0) / args.steps
     e1.record(stream)
     barrier()
     clk = clocks.stop()
@@ -264,31 +266,70 @@ def run_ours(args, rank, world, local_rank):
     ms_plain = max_over_ranks(e0.elapsed_time(e1))
     plain = world * B * args.steps / (ms_plain / 1000.0)
 
-    # ---- end to end: pinned host inputs -> device -> batched N4 -> host outputs
+    # ---- end to end: pinned host inputs -> device -> batched N4 -> host outputs,
+    # pipelined in sub-batches over 3 streams (one context each) so that the
+    # host<->device copies of one sub-batch overlap the kernels of another
+    nsub = 4 if B % 4 == 0 else 1
+    per = B // nsub
+    streams = [torch.cuda.Stream(dev) for _ in range(3)]
+    ctxs = [n4b200.Context(local_rank) for _ in range(3)]
     dev_in = [(torch.empty_like(a, device=dev), torch.empty_like(b, device=dev)) for a, b in vols_host]
     out_h = [torch.empty_like(a).pin_memory() for a, _ in vols_host]
     lat_h = [torch.empty(n4b200.lattice_dims(p), dtype=torch.float32).pin_memory() for _ in vols_host]
 
     def step_e2e():
-        for (ih, mh), (idv, mdv) in zip(vols_host, dev_in):
-            idv.copy_(ih, non_blocking=True)
-            mdv.copy_(mh, non_blocking=True)
-        rs = n4b200.N4Batch(dev_in, p, ctx=ctx, synchronous=False)
-        for r, o, l in zip(rs, out_h, lat_h):
-            o.copy_(r.im_normalized, non_blocking=True)
-            l.copy_(r.lattice, non_blocking=True)
+        for k in range(nsub):
+            st = streams[k % 3]
+            sl = slice(k * per, (k + 1) * per)
+            with torch.cuda.stream(st):
+                for (ih, mh), (idv, mdv) in zip(vols_host[sl], dev_in[sl]):
+                    idv.copy_(ih, non_blocking=True)
+                    mdv.copy_(mh, non_blocking=True)
+                rs = n4b200.N4Batch(dev_in[sl], p, ctx=ctxs[k % 3], synchronous=False)
+                for r, o, l in zip(rs, out_h[sl], lat_h[sl]):
+                    o.copy_(r.im_normalized, non_blocking=True)
+                    l.copy_(r.lattice, non_blocking=True)
 
     for _ in range(min(args.warmup, 2)):
         step_e2e()
     barrier()
     e0.record(stream)
+    for s2 in streams:
+        s2.wait_event(e0)
     for _ in range(args.steps):
         step_e2e()
+    for s2 in streams:
+        ev = torch.cuda.Event()
+        ev.record(s2)
+        stream.wait_event(ev)
     e1.record(stream)
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1))
     h2d = sum(a.numel() * 4 + b.numel() * 4 for a, b in vols_host)
     d2h = sum(o.numel() * 4 for o in out_h) + sum(l.numel() * 4 for l in lat_h)
+
+    # ---- standalone HBM-bound kernels at the 512x512x320 scale: the fit on
+    # its 256x256x160 fitting grid (reads field 4 B + float mask 4 B per voxel)
+    # and the dense evaluation at full resolution (writes 4 B per voxel)
+    def timed(fn, reps=10):
+        fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / reps
+    gen = torch.Generator(device=dev).manual_seed(5)
+    fit_shape, full_shape = (256, 256, 160), (512, 512, 320)
+    field = torch.randn(fit_shape, device=dev, generator=gen)
+    fmask = (torch.rand(fit_shape, device=dev, generator=gen) > 0.4).float()
+    lat11 = torch.randn((11, 11, 11), device=dev, generator=gen) * 0.1
+    ms_fit = timed(lambda: n4b200.FitBspline3D(field, fmask, (11, 11, 11), ctx=ctx))
+    ms_eval = timed(lambda: n4b200.EvaluateBspline3D(lat11, (11, 11, 11), full_shape, ctx=ctx))
+    nfit, nfull = field.numel(), int(np.prod(full_shape))
+    del field, fmask
 
     line = {
         "metric": METRIC, "value": value, "unit": "volumes/s", "n_gpus": world, "steps": args.steps,
@@ -310,7 +351,14 @@ def run_ours(args, rank, world, local_rank):
         "plain": {"value": plain, "unit": "volumes/s", "ms_per_volume": ms_plain / (args.steps * B)},
         "stages_ms_per_batch": {k: t[k] for k in ("prologue_ms", "n4_ms", "tables_ms", "correct_ms")},
         "stage_gbs": {"correct": corr_gbs, "prologue": pro_gbs},
+        "fit_gbs": {"value": 8 * nfit / (ms_fit / 1000) / 1e9, "frac": 8 * nfit / (ms_fit / 1000) / 1e9 / hbm_peak,
+                    "ms": ms_fit, "workload": "FitBspline3D 256x256x160 field + float mask, 11^3 lattice "
+                                              "(8 B per voxel read)"},
+        "upsample_gbs": {"value": 4 * nfull / (ms_eval / 1000) / 1e9,
+                         "frac": 4 * nfull / (ms_eval / 1000) / 1e9 / hbm_peak, "ms": ms_eval,
+                         "workload": "EvaluateBspline3D 11^3 lattice -> 512x512x320 (4 B per voxel written)"},
         "iterations_per_volume": total_iters / B,
+        "host_enqueue_ms_per_step": host_ms,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_single()
@@ -325,7 +373,7 @@ def run_ours(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")

@@ -28,6 +28,13 @@ n4_status_t fail(n4_status_t s, const std::string &msg) {
   return s;
 }
 
+}  // namespace
+
+// shared with the encoder translation unit
+n4_status_t n4_record_error(n4_status_t s, const char *msg) { return fail(s, msg); }
+
+namespace {
+
 #define CK(call)                                                                         \
   do {                                                                                   \
     cudaError_t e_ = (call);                                                             \
@@ -142,7 +149,7 @@ int npad_of(int bins) {
 // float4 I/O is used only when rows are whole float4s and every pointer is 16-byte aligned.
 int vec4_ok(int fz, const void *a, const void *b, const void *c) {
   auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
-  return (fz % 4 == 0) && al(a) && al(b) && al(c) ? 1 : 0;
+  return (fz % 4 == 0) && fz <= 1024 && al(a) && al(b) && al(c) ? 1 : 0;
 }
 
 int final_nc(unsigned nc0, unsigned levels) { return (int)(((nc0 - 3) << (levels - 1)) + 3); }
@@ -925,7 +932,9 @@ n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const floa
   TRY(ctx->s2.ensure(t2 * 8, "fit planes"));
   float *t1n = ctx->s1.as<float>(), *t1d = t1n + t1, *t2n = ctx->s2.as<float>(), *t2d = t2n + t2;
   const int gb = ctx->nsm * 8;
-  k_fit_rows<<<(int)std::min<size_t>((t1 + 255) / 256, gb), 256, 0, st>>>(d_field, d_mask, fx, fy, fz, az, t1n, t1d);
+  const long long rows = (long long)fx * fy;
+  k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(d_field, d_mask, rows, fz, az,
+                                                                                 t1n, t1d);
   k_fit_planes<<<(int)std::min<size_t>((t2 + 255) / 256, gb), 256, 0, st>>>(t1n, t1d, fx, fy, ay, ncpt_z, t2n, t2d);
   const int nlat = ncpt_x * ncpt_y * ncpt_z;
   k_fit_final<<<(nlat + 255) / 256, 256, 0, st>>>(t2n, t2d, fx, ax, ncpt_y, ncpt_z, eps, zero_den, d_lattice);

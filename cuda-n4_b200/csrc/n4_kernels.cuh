@@ -285,23 +285,34 @@ __global__ void __launch_bounds__(256) k_correct(const CorrectVol *vols, const l
   const int FZ = C.FZ;
   const long long base = row0 * FZ;
   if (C.vec4) {
+    // each thread owns 4 consecutive z (weights in registers) and walks rows;
+    // exp/divide use the fast intrinsics (a few ulp)
     const int nz4 = FZ >> 2;
-    for (int t = threadIdx.x; t < nr * nz4; t += blockDim.x) {
-      const int r = t / nz4, z4 = (t - r * nz4) * 4;
-      const long long off = base + (long long)r * FZ + z4;
-      float bz[4];
+    const int rpp = blockDim.x / nz4;            // rows per pass (nz4 <= 256)
+    if ((int)threadIdx.x < rpp * nz4) {
+      const int z = (threadIdx.x % nz4) * 4;
+      const int r_first = threadIdx.x / nz4;
+      int sz[4];
+      float4 wz[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) bz[k] = dot4(az.w[z4 + k], Gs + r * ncz + az.s[z4 + k]);
-      if (C.im) {
-        const float4 x = __ldcs((const float4 *)(C.im + off));
-        const float xa[4] = {x.x, x.y, x.z, x.w};
-        float o[4], e[4];
+      for (int k = 0; k < 4; ++k) { sz[k] = az.s[z + k]; wz[k] = az.w[z + k]; }
+      for (int r = r_first; r < nr; r += rpp) {
+        const float *g = Gs + r * ncz;
+        float bz[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) { e[k] = expf(bz[k]); o[k] = xa[k] > low ? xa[k] / e[k] : 0.0f; }
-        __stcs((float4 *)(C.out + off), make_float4(o[0], o[1], o[2], o[3]));
-        if (C.bias) __stcs((float4 *)(C.bias + off), make_float4(e[0], e[1], e[2], e[3]));
-      } else {
-        __stcs((float4 *)(C.out + off), make_float4(bz[0], bz[1], bz[2], bz[3]));
+        for (int k = 0; k < 4; ++k) bz[k] = dot4(wz[k], g + sz[k]);
+        const long long off = base + (long long)r * FZ + z;
+        if (C.im) {
+          const float4 x = __ldcs((const float4 *)(C.im + off));
+          const float xa[4] = {x.x, x.y, x.z, x.w};
+          float o[4], e[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) { e[k] = __expf(bz[k]); o[k] = xa[k] > low ? __fdividef(xa[k], e[k]) : 0.0f; }
+          __stcs((float4 *)(C.out + off), make_float4(o[0], o[1], o[2], o[3]));
+          if (C.bias) __stcs((float4 *)(C.bias + off), make_float4(e[0], e[1], e[2], e[3]));
+        } else {
+          __stcs((float4 *)(C.out + off), make_float4(bz[0], bz[1], bz[2], bz[3]));
+        }
       }
     }
   } else {
@@ -311,8 +322,8 @@ __global__ void __launch_bounds__(256) k_correct(const CorrectVol *vols, const l
       const float b = dot4(az.w[z], Gs + r * ncz + az.s[z]);
       if (C.im) {
         const float x = C.im[off];
-        const float e = expf(b);
-        C.out[off] = x > low ? x / e : 0.0f;
+        const float e = __expf(b);
+        C.out[off] = x > low ? __fdividef(x, e) : 0.0f;
         if (C.bias) C.bias[off] = e;
       } else {
         C.out[off] = b;
@@ -322,29 +333,64 @@ __global__ void __launch_bounds__(256) k_correct(const CorrectVol *vols, const l
 }
 
 // ------------------------------------------------------------------ standalone fit
-// T1[row][cz] (numerator and denominator) for every row of the field.
-__global__ void k_fit_rows(const float *field, const float *mask, int X, int Y, int Z, Axis az,
-                           float *t1n, float *t1d) {
+constexpr int kFitRows = 128;   // rows per block (one thread each)
+constexpr int kFitChunk = 32;   // z voxels staged per step
+
+// T1[row][cz] (numerator and denominator) for every row of the field.  One
+// thread per row walks z once with the 4 open targets of its current span in
+// registers (a span's voxels feed targets s..s+3; target s is final when the
+// walk leaves span s), so every voxel is read once and every target written
+// once.  Rows are staged through shared memory in coalesced [rows][32] tiles.
+__global__ void __launch_bounds__(kFitRows) k_fit_rows(const float *field, const float *mask, long long rows, int Z,
+                                                       Axis az, float *t1n, float *t1d) {
+  __shared__ float fs[kFitRows][kFitChunk + 1];
+  __shared__ float ms[kFitRows][kFitChunk + 1];
+  const long long row0 = (long long)blockIdx.x * kFitRows;
+  const int nr = (int)min((long long)kFitRows, rows - row0);
   const int ncz = az.nc;
-  const long long ntask = (long long)X * Y * ncz;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntask;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long row = t / ncz;
-    const int cz = (int)(t - row * ncz);
-    const float *f = field + row * Z;
-    const float *m = mask ? mask + row * Z : nullptr;
-    float an = 0.0f, ad = 0.0f;
-    for (int j = 0; j < 4; ++j) {
-      const int sp = cz - j;
-      if (sp < 0 || sp >= az.nsp) continue;
-      for (int vz = az.lo[sp]; vz < az.hi[sp]; ++vz) {
-        if (m && m[vz] == 0.0f) continue;
-        an = __fmaf_rn(az.p[j * Z + vz], f[vz], an);
-        ad += az.q[j * Z + vz];
+  const long long my = row0 + threadIdx.x;
+  float n0 = 0.f, n1 = 0.f, n2 = 0.f, n3 = 0.f, d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
+  int cur = 0;                                   // span of the open window
+  for (int z0 = 0; z0 < Z; z0 += kFitChunk) {
+    const int nz = min(kFitChunk, Z - z0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nr * kFitChunk; i += blockDim.x) {
+      const int r = i / kFitChunk, z = i - r * kFitChunk;
+      if (z < nz) {
+        const long long g = (row0 + r) * Z + z0 + z;
+        fs[r][z] = field[g];
+        ms[r][z] = mask ? mask[g] : 1.0f;
       }
     }
-    t1n[t] = an;
-    t1d[t] = ad;
+    __syncthreads();
+    if ((int)threadIdx.x < nr) {
+      for (int z = 0; z < nz; ++z) {
+        const int vz = z0 + z;
+        const int sp = az.s[vz];
+        while (cur < sp) {                       // close target `cur`
+          t1n[my * ncz + cur] = n0;
+          t1d[my * ncz + cur] = d0;
+          n0 = n1; n1 = n2; n2 = n3; n3 = 0.f;
+          d0 = d1; d1 = d2; d2 = d3; d3 = 0.f;
+          ++cur;
+        }
+        if (ms[threadIdx.x][z] == 0.0f) continue;
+        const float f = fs[threadIdx.x][z];
+        const float4 p = az.p4[vz], q = az.q4[vz];
+        n0 = __fmaf_rn(p.x, f, n0); n1 = __fmaf_rn(p.y, f, n1);
+        n2 = __fmaf_rn(p.z, f, n2); n3 = __fmaf_rn(p.w, f, n3);
+        d0 += q.x; d1 += q.y; d2 += q.z; d3 += q.w;
+      }
+    }
+  }
+  if ((int)threadIdx.x < nr) {
+    // flush the open window and any targets after it
+    const float nn[4] = {n0, n1, n2, n3}, dd[4] = {d0, d1, d2, d3};
+    for (int c = cur; c < ncz; ++c) {
+      const int k = c - cur;
+      t1n[my * ncz + c] = k < 4 ? nn[k] : 0.0f;
+      t1d[my * ncz + c] = k < 4 ? dd[k] : 0.0f;
+    }
   }
 }
 

@@ -103,6 +103,14 @@ SIGNATURES = [
     ("n4_sharpen_image", C.c_int, [_P, _P, _P, _U, _U, C.c_float, C.c_float, _P,
                                    C.POINTER(C.c_float), C.POINTER(C.c_float), _P]),
     ("n4_convergence", C.c_int, [_P, _P, _P, _P, _U, C.c_int, C.POINTER(C.c_double)]),
+    ("n4_encoder_num_params", C.c_size_t, []),
+    ("n4_encoder_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int]),
+    ("n4_encoder_destroy", C.c_int, [_P]),
+    ("n4_encoder_set_params", C.c_int, [_P, _P, C.c_size_t]),
+    ("n4_encoder_get_params", C.c_int, [_P, _P, _P, C.c_size_t]),
+    ("n4_encoder_predict", C.c_int, [_P, _P, C.c_int, _P, _P]),
+    ("n4_encoder_train_step", C.c_int, [_P, _P, _P, C.c_int, C.c_float, C.POINTER(C.c_float), _P]),
+    ("n4_encoder_pool_input", C.c_int, [_P, _P, _U, _U, _U, C.c_float, _P, _P]),
 ]
 
 _lib = None

@@ -47,7 +47,8 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", LIB + ".tmp", os.path.join(CSRC, "n4_api.cu")]
+    units = [os.path.join(CSRC, f) for f in ("n4_api.cu", "n4_encoder.cu")]
+    cmd = [nvcc(), *NVCC_FLAGS, "-o", LIB + ".tmp", *units]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

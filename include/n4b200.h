@@ -185,6 +185,34 @@ n4_status_t n4_sharpen_image(n4_context_t *ctx, const float *d_before, const flo
 n4_status_t n4_convergence(n4_context_t *ctx, const float *d_field1, const float *d_field2,
                            const float *d_mask, unsigned int n, int ddof, double *cv);
 
+/* ---- learned warm start (no counterpart in the reference) ----
+ * A small 3-D convolutional encoder (4 conv 3x3x3 stride 2 layers of
+ * 16/32/64/64 channels with ReLU, then a linear layer to 64 outputs) that
+ * predicts the first-level 4x4x4 log-bias lattice from the masked log volume
+ * average-pooled to 32x32x24.  BF16 weights and activations, FP32
+ * accumulation on the tensor cores; FP32 master weights and Adam moments.
+ * Inputs are device arrays of batch x 32 x 32 x 24 BF16 values
+ * (n4_encoder_pool_input writes one); outputs batch x 64 floats, which are
+ * first-level lattices to pass as `warm_lattice`. */
+typedef struct n4_encoder n4_encoder_t;
+
+size_t n4_encoder_num_params(void);
+n4_status_t n4_encoder_create(n4_encoder_t **enc, int device, int max_batch);
+n4_status_t n4_encoder_destroy(n4_encoder_t *enc);
+/* Host FP32 parameter vector (n4_encoder_num_params entries); resets Adam. */
+n4_status_t n4_encoder_set_params(n4_encoder_t *enc, const float *h_params, size_t n);
+/* Parameters and the gradients of the last train step (either may be NULL). */
+n4_status_t n4_encoder_get_params(n4_encoder_t *enc, float *h_params, float *h_grads, size_t n);
+n4_status_t n4_encoder_predict(n4_encoder_t *enc, const void *d_x, int batch, float *d_out, void *stream);
+/* Forward, MSE against d_target (batch x 64), backward; an Adam step when
+ * lr > 0.  h_loss (may be NULL) receives the batch loss (synchronises). */
+n4_status_t n4_encoder_train_step(n4_encoder_t *enc, const void *d_x, const float *d_target, int batch,
+                                  float lr, float *h_loss, void *stream);
+/* Network input of one volume: mean of log(im) over masked voxels above
+ * low_value in each of 32x32x24 adaptive pooling cells, as BF16. */
+n4_status_t n4_encoder_pool_input(const float *d_im, const float *d_mask, unsigned int fx, unsigned int fy,
+                                  unsigned int fz, float low_value, void *d_x, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
