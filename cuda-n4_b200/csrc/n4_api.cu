@@ -133,6 +133,8 @@ struct n4_context {
   bool prof_valid = false;
 };
 
+struct n4_batch_graph;
+
 namespace {
 
 // ------------------------------------------------------------------ params
@@ -400,6 +402,18 @@ struct RunVol {
   Dims d;
 };
 
+// Workspaces of the whole-GPU path for one volume (sized before any capture).
+n4_status_t ensure_grid_workspace(n4_context *ctx, const n4_params_t *p, const Dims &d) {
+  std::vector<Dims> one{d};
+  Plan pl = make_plan(p, ctx->nsm, one, true);
+  const size_t nfit = (size_t)d.X * d.Y * d.Z;
+  TRY(ctx->logu.ensure(nfit * 4 + 64, "logU"));
+  TRY(ctx->big.ensure((size_t)pl.big_bytes * ctx->nsm, "grid workspace"));
+  TRY(ctx->red.ensure(std::max((size_t)pl.bins * 8, (size_t)pl.NLAT * 4) + 64, "grid reduction"));
+  TRY(ctx->bar.ensure(64, "grid barrier"));
+  return N4_OK;
+}
+
 n4_status_t launch_grid_path(n4_context *ctx, const n4_params_t *p, const Params &pr, const RunVol &rv,
                              const VolJob &job0, int nt, cudaStream_t st) {
   std::vector<Dims> one{rv.d};
@@ -502,178 +516,234 @@ n4_status_t choose_path(n4_context *ctx, const n4_params_t *p, const std::vector
 }
 
 // Core of n4_run / n4_run_batched: every pointer is a device pointer.
-n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector<RunVol> &rvs, cudaStream_t st,
-                        const Choice *forced) {
-  const int n = (int)rvs.size();
-  const Params pr = make_dev_params(p);
+// A run's plan: the execution path of every volume and the layout of its
+// descriptor buffer (volume descriptors, reports, flags, work-queue counter).
+struct Prepared {
+  int n = 0;
+  Params pr{};
+  Choice ch{};
+  std::vector<int> in_cluster, in_grid, path, csize;
   std::vector<Dims> dims;
-  for (const RunVol &r : rvs) dims.push_back(r.d);
-  // volumes that fit a cluster run together; the others use the whole GPU
+  std::vector<RunVol> rvs;
+  std::vector<size_t> imlog_off, tab_off;
+  int NCX = 0, NCY = 0, NCZ = 0;
+  size_t o_pro = 0, o_pst = 0, o_job = 0, o_ord = 0, o_tab = 0, o_cor = 0, o_tst = 0, o_rep = 0, o_flg = 0,
+         o_q = 0, bytes = 0;
+  long long fit_total = 0, tiles = 0;
+};
+
+// Descriptor buffer: pinned host staging and its device copy.
+struct DescBuf {
+  char *h = nullptr;
+  char *d = nullptr;
+  template <class T> T *hp(size_t o) const { return (T *)(h + o); }
+  template <class T> T *dp(size_t o) const { return (T *)(d + o); }
+};
+
+// Choose paths, size the workspaces and lay out the descriptors.
+n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<RunVol> &rvs, const Choice *forced,
+                     Prepared &P) {
+  const int n = (int)rvs.size();
+  P.n = n;
+  P.rvs = rvs;
+  P.pr = make_dev_params(p);
+  for (const RunVol &r : rvs) P.dims.push_back(r.d);
+  const std::vector<Dims> &dims = P.dims;
   Choice ch{};
   if (forced) ch = *forced;
   else TRY(choose_path(ctx, p, dims, n > 1, ch));
-  std::vector<int> in_cluster, in_grid;
   if (!ch.grid) {
-    for (int i = 0; i < n; ++i) in_cluster.push_back(i);
+    for (int i = 0; i < n; ++i) P.in_cluster.push_back(i);
   } else if (n == 1) {
-    in_grid.push_back(0);
+    P.in_grid.push_back(0);
   } else {
     // batch with volumes too large for a cluster: split by fit
     for (int i = 0; i < n; ++i) {
       std::vector<Dims> one{dims[i]};
       int K = 0;
       TRY(choose_cluster(ctx, p, one, 1024, &K));
-      (K ? in_cluster : in_grid).push_back(i);
+      (K ? P.in_cluster : P.in_grid).push_back(i);
     }
-    if (!in_cluster.empty()) {
+    if (!P.in_cluster.empty()) {
       std::vector<Dims> sub;
-      for (int i : in_cluster) sub.push_back(dims[i]);
+      for (int i : P.in_cluster) sub.push_back(dims[i]);
       ch.grid = false;
       ch.nt = 1024;
       TRY(choose_cluster(ctx, p, sub, 1024, &ch.K));
     }
   }
-  // ---- workspaces
-  const int NCX = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
-  const int NCY = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);
-  const int NCZ = final_nc(p->NumberOfControlPoints_z, p->NumberOfFittingLevels);
-  std::vector<size_t> imlog_off(n), tab_off(n);
+  P.ch = ch;
+  for (int i : P.in_grid) TRY(ensure_grid_workspace(ctx, p, dims[i]));
+  P.path.assign(n, 0);
+  P.csize.assign(n, 0);
+  for (int i : P.in_cluster) { P.path[i] = 1; P.csize[i] = ch.K; }
+  for (int i : P.in_grid) { P.path[i] = 2; P.csize[i] = ctx->nsm; }
+  // workspaces
+  P.NCX = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
+  P.NCY = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);
+  P.NCZ = final_nc(p->NumberOfControlPoints_z, p->NumberOfFittingLevels);
+  P.imlog_off.resize(n);
+  P.tab_off.resize(n);
   size_t imlog_bytes = 0, tab_bytes = 0;
   for (int i = 0; i < n; ++i) {
-    imlog_off[i] = imlog_bytes;
+    P.imlog_off[i] = imlog_bytes;
     imlog_bytes = align_up(imlog_bytes + (size_t)dims[i].X * dims[i].Y * dims[i].Z * 4 + 64, 256);
-    tab_off[i] = tab_bytes;
-    tab_bytes += align_up(axis_bytes(dims[i].FX, NCX - 3), 256) + align_up(axis_bytes(dims[i].FY, NCY - 3), 256) +
-                 align_up(axis_bytes(dims[i].FZ, NCZ - 3), 256);
+    P.tab_off[i] = tab_bytes;
+    tab_bytes += align_up(axis_bytes(dims[i].FX, P.NCX - 3), 256) + align_up(axis_bytes(dims[i].FY, P.NCY - 3), 256) +
+                 align_up(axis_bytes(dims[i].FZ, P.NCZ - 3), 256);
   }
   TRY(ctx->imlog.ensure(imlog_bytes, "fitting grid"));
   TRY(ctx->tables.ensure(tab_bytes, "axis tables"));
-  // ---- descriptors
-  Upload u;
   size_t o = 0;
   auto take = [&](size_t b) { size_t r = o; o = align_up(o + b, 16); return r; };
-  const size_t o_pro = take(sizeof(PrologueVol) * n), o_pst = take(8 * n), o_job = take(sizeof(VolJob) * n),
-               o_ord = take(4 * n), o_tab = take(sizeof(TableJob) * 3 * n), o_cor = take(sizeof(CorrectVol) * n),
-               o_tst = take(8 * n), o_rep = take(sizeof(n4_report_t) * n), o_flg = take(4 * n),
-               o_q = take(16);
-  TRY(acquire_slot(ctx, o, u));
-  PrologueVol *pv = u.hp<PrologueVol>(o_pro);
-  long long *pst = u.hp<long long>(o_pst);
-  VolJob *jb = u.hp<VolJob>(o_job);
-  int *ord = u.hp<int>(o_ord);
-  TableJob *tj = u.hp<TableJob>(o_tab);
-  CorrectVol *cv = u.hp<CorrectVol>(o_cor);
-  long long *tst = u.hp<long long>(o_tst);
-  n4_report_t *rep = u.hp<n4_report_t>(o_rep);
+  P.o_pro = take(sizeof(PrologueVol) * n);
+  P.o_pst = take(8 * n);
+  P.o_job = take(sizeof(VolJob) * n);
+  P.o_ord = take(4 * n);
+  P.o_tab = take(sizeof(TableJob) * 3 * n);
+  P.o_cor = take(sizeof(CorrectVol) * n);
+  P.o_tst = take(8 * n);
+  P.o_rep = take(sizeof(n4_report_t) * n);
+  P.o_flg = take(4 * n);
+  P.o_q = take(16);
+  P.bytes = o;
+  return N4_OK;
+}
+
+// Fill the descriptors (host side of `B`, which must hold P.bytes zeroed bytes).
+void fill_descriptors(n4_context *ctx, const n4_params_t *p, Prepared &P, const DescBuf &B) {
+  const int n = P.n;
+  PrologueVol *pv = B.hp<PrologueVol>(P.o_pro);
+  long long *pst = B.hp<long long>(P.o_pst);
+  VolJob *jb = B.hp<VolJob>(P.o_job);
+  int *ord = B.hp<int>(P.o_ord);
+  TableJob *tj = B.hp<TableJob>(P.o_tab);
+  CorrectVol *cv = B.hp<CorrectVol>(P.o_cor);
+  long long *tst = B.hp<long long>(P.o_tst);
+  n4_report_t *rep = B.hp<n4_report_t>(P.o_rep);
   long long fit_total = 0, tiles = 0;
   char *tabs = ctx->tables.as<char>();
   for (int i = 0; i < n; ++i) {
-    const RunVol &r = rvs[i];
-    const Dims &d = dims[i];
-    float *il = (float *)(ctx->imlog.as<char>() + imlog_off[i]);
+    const RunVol &r = P.rvs[i];
+    const Dims &d = P.dims[i];
+    float *il = (float *)(ctx->imlog.as<char>() + P.imlog_off[i]);
     pv[i] = PrologueVol{r.im, r.mask, r.im_w, r.mask_w, d.FX, d.FY, d.FZ, (int)p->ShrinkFactor,
                         d.X, d.Y, d.Z, il, fit_total};
     pst[i] = fit_total;
     fit_total += (long long)d.X * d.Y * d.Z;
-    jb[i] = VolJob{d.X, d.Y, d.Z, il, nullptr, r.warm, r.lat, u.dp<n4_report_t>(o_rep) + i};
-    char *tx = tabs + tab_off[i];
-    char *ty = tx + align_up(axis_bytes(d.FX, NCX - 3), 256);
-    char *tz = ty + align_up(axis_bytes(d.FY, NCY - 3), 256);
-    tj[3 * i] = TableJob{tx, d.FX, NCX};
-    tj[3 * i + 1] = TableJob{ty, d.FY, NCY};
-    tj[3 * i + 2] = TableJob{tz, d.FZ, NCZ};
-    cv[i] = CorrectVol{r.im, r.out, r.bias, r.lat, tx, ty, tz, d.FX, d.FY, d.FZ, NCX, NCY, NCZ, tiles,
+    jb[i] = VolJob{d.X, d.Y, d.Z, il, nullptr, r.warm, r.lat, B.dp<n4_report_t>(P.o_rep) + i};
+    char *tx = tabs + P.tab_off[i];
+    char *ty = tx + align_up(axis_bytes(d.FX, P.NCX - 3), 256);
+    char *tz = ty + align_up(axis_bytes(d.FY, P.NCY - 3), 256);
+    tj[3 * i] = TableJob{tx, d.FX, P.NCX};
+    tj[3 * i + 1] = TableJob{ty, d.FY, P.NCY};
+    tj[3 * i + 2] = TableJob{tz, d.FZ, P.NCZ};
+    cv[i] = CorrectVol{r.im, r.out, r.bias, r.lat, tx, ty, tz, d.FX, d.FY, d.FZ, P.NCX, P.NCY, P.NCZ, tiles,
                        vec4_ok(d.FZ, r.im, r.out, r.bias)};
     tst[i] = tiles;
     tiles += ((long long)d.FX * d.FY + kRowsPerTile - 1) / kRowsPerTile;
     std::memset(&rep[i], 0, sizeof(n4_report_t));
     rep[i].status = -1;
   }
+  P.fit_total = fit_total;
+  P.tiles = tiles;
   // longest-first order of the cluster queue
-  std::vector<int> order = in_cluster;
+  std::vector<int> order = P.in_cluster;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-    return (long long)dims[a].X * dims[a].Y * dims[a].Z > (long long)dims[b].X * dims[b].Y * dims[b].Z;
+    const Dims &x = P.dims[a], &y = P.dims[b];
+    return (long long)x.X * x.Y * x.Z > (long long)y.X * y.Y * y.Z;
   });
   for (size_t k = 0; k < order.size(); ++k) ord[k] = order[k];
-  TRY(begin_run(ctx, st));
-  CK(cudaMemcpyAsync(u.slot->d.p, u.slot->h, o, cudaMemcpyHostToDevice, st));
-  int *flags = u.dp<int>(o_flg);
+}
+
+// The launches of a run (descriptors already on the device); capturable.
+n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P, const DescBuf &B, cudaStream_t st,
+                        bool profile) {
+  const int n = P.n;
   int launches = 0;
-  TRY(prof_mark(ctx, 0, st));
-  // ---- prologue
+  if (profile) TRY(prof_mark(ctx, 0, st));
   {
     ++launches;
-    const int blocks = (int)std::min<long long>((fit_total + 255) / 256, (long long)ctx->nsm * 16);
-    k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(u.dp<PrologueVol>(o_pro), u.dp<long long>(o_pst), n, fit_total,
-                                                     p->low_value, flags);
+    const int blocks = (int)std::min<long long>((P.fit_total + 255) / 256, (long long)ctx->nsm * 16);
+    k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(B.dp<PrologueVol>(P.o_pro), B.dp<long long>(P.o_pst), n,
+                                                     P.fit_total, p->low_value, B.dp<int>(P.o_flg));
     CK(cudaGetLastError());
     if (p->ShrinkFactor > 1 && (p->flags & N4_FLAG_INPLACE_THRESH)) {
       for (int i = 0; i < n; ++i) {
-        const long long nf = (long long)dims[i].FX * dims[i].FY * dims[i].FZ;
-        if (rvs[i].im_w) {
+        const long long nf = (long long)P.dims[i].FX * P.dims[i].FY * P.dims[i].FZ;
+        if (P.rvs[i].im_w) {
           k_threshold_inplace<<<(int)std::min<long long>((nf + 255) / 256, ctx->nsm * 16LL), 256, 0, st>>>(
-              rvs[i].im_w, rvs[i].mask_w, nf, p->low_value);
+              P.rvs[i].im_w, P.rvs[i].mask_w, nf, p->low_value);
           ++launches;
           CK(cudaGetLastError());
         }
       }
     }
   }
-  TRY(prof_mark(ctx, 1, st));
-  // ---- N4
-  Slot &slot = *u.slot;
-  slot.nrep = n;
-  slot.off_rep = o_rep;
-  slot.off_flags = o_flg;
-  slot.path.assign(n, 0);
-  slot.csize.assign(n, 0);
-  if (!in_cluster.empty()) {
+  if (profile) TRY(prof_mark(ctx, 1, st));
+  if (!P.in_cluster.empty()) {
     std::vector<Dims> sub;
-    for (int i : in_cluster) sub.push_back(dims[i]);
-    Plan pl = make_plan(p, ch.K, sub, false);
+    for (int i : P.in_cluster) sub.push_back(P.dims[i]);
+    Plan pl = make_plan(p, P.ch.K, sub, false);
     const int smem = pl.sm_bytes + pl.big_bytes;
     int cap = 0;
-    TRY(capacity(ctx, ch.nt, ch.K, smem, &cap));
+    TRY(capacity(ctx, P.ch.nt, P.ch.K, smem, &cap));
     if (cap < 1) return fail(N4_ERR_TOO_LARGE, "no cluster of this size fits on the device");
     ClusterArgs a{};
     a.pl = pl;
-    a.pr = pr;
-    a.jobs = u.dp<VolJob>(o_job);
-    a.order = u.dp<int>(o_ord);
-    a.njobs = (int)in_cluster.size();
-    a.queue = u.dp<int>(o_q);
+    a.pr = P.pr;
+    a.jobs = B.dp<VolJob>(P.o_job);
+    a.order = B.dp<int>(P.o_ord);
+    a.njobs = (int)P.in_cluster.size();
+    a.queue = B.dp<int>(P.o_q);
     a.use_tma = 1;
-    const int ncl = std::min<int>(cap, (int)in_cluster.size());
-    if (ch.nt == 1024) TRY(launch_cluster_kernel<1024>(ctx, a, ch.K, ncl, smem, st));
-    else TRY(launch_cluster_kernel<512>(ctx, a, ch.K, ncl, smem, st));
-    for (int i : in_cluster) { slot.path[i] = 1; slot.csize[i] = ch.K; }
+    const int ncl = std::min<int>(cap, (int)P.in_cluster.size());
+    if (P.ch.nt == 1024) TRY(launch_cluster_kernel<1024>(ctx, a, P.ch.K, ncl, smem, st));
+    else TRY(launch_cluster_kernel<512>(ctx, a, P.ch.K, ncl, smem, st));
     ++launches;
   }
-  for (int i : in_grid) {
-    VolJob j = jb[i];
-    j.report = u.dp<n4_report_t>(o_rep) + i;
-    TRY(launch_grid_path(ctx, p, pr, rvs[i], j, ch.nt ? ch.nt : 1024, st));
-    slot.path[i] = 2;
-    slot.csize[i] = ctx->nsm;
+  for (int i : P.in_grid) {
+    VolJob j = B.hp<VolJob>(P.o_job)[i];
+    TRY(launch_grid_path(ctx, p, P.pr, P.rvs[i], j, P.ch.nt ? P.ch.nt : 1024, st));
     ++launches;
   }
-  TRY(prof_mark(ctx, 2, st));
-  // ---- final correction at full resolution
-  k_axis_tables<<<3 * n, 256, 0, st>>>(u.dp<TableJob>(o_tab));
+  if (profile) TRY(prof_mark(ctx, 2, st));
+  k_axis_tables<<<3 * n, 256, 0, st>>>(B.dp<TableJob>(P.o_tab));
   CK(cudaGetLastError());
-  TRY(prof_mark(ctx, 3, st));
-  k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(o_cor), u.dp<long long>(o_tst), n, p->low_value);
+  if (profile) TRY(prof_mark(ctx, 3, st));
+  k_correct<<<(unsigned)P.tiles, 256, 0, st>>>(B.dp<CorrectVol>(P.o_cor), B.dp<long long>(P.o_tst), n, p->low_value);
   CK(cudaGetLastError());
-  TRY(prof_mark(ctx, 4, st));
+  if (profile) TRY(prof_mark(ctx, 4, st));
   launches += 2;
   ctx->prof_launches = launches;
-  ctx->prof_fit = fit_total;
+  ctx->prof_fit = P.fit_total;
   ctx->prof_full = 0;
-  for (const Dims &d : dims) ctx->prof_full += (long long)d.FX * d.FY * d.FZ;
+  for (const Dims &d : P.dims) ctx->prof_full += (long long)d.FX * d.FY * d.FZ;
+  return N4_OK;
+}
+
+// Core of n4_run / n4_run_batched: every pointer is a device pointer.
+n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector<RunVol> &rvs, cudaStream_t st,
+                        const Choice *forced) {
+  Prepared P;
+  TRY(plan_run(ctx, p, rvs, forced, P));
+  Upload u;
+  TRY(acquire_slot(ctx, P.bytes, u));
+  DescBuf B{u.slot->h, (char *)u.slot->d.p};
+  fill_descriptors(ctx, p, P, B);
+  TRY(begin_run(ctx, st));
+  CK(cudaMemcpyAsync(B.d, B.h, P.bytes, cudaMemcpyHostToDevice, st));
+  TRY(enqueue_run(ctx, p, P, B, st, ctx->profiling != 0));
   ctx->prof_valid = ctx->profiling != 0;
+  Slot &slot = *u.slot;
+  slot.nrep = P.n;
+  slot.off_rep = P.o_rep;
+  slot.off_flags = P.o_flg;
+  slot.path = P.path;
+  slot.csize = P.csize;
   // reports back to the slot's pinned buffer
-  CK(cudaMemcpyAsync(u.slot->h + o_rep, u.dp<char>(o_rep), sizeof(n4_report_t) * n + 0, cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(u.slot->h + o_flg, u.dp<char>(o_flg), 4 * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(B.h + P.o_rep, B.d + P.o_rep, sizeof(n4_report_t) * P.n, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(B.h + P.o_flg, B.d + P.o_flg, 4 * P.n, cudaMemcpyDeviceToHost, st));
   return end_run(ctx, st, u);
 }
 
@@ -893,6 +963,128 @@ n4_status_t n4_run_host(n4_context_t *ctx, const n4_params_t *p, const float *h_
   if (h_bias_field) CK(cudaMemcpyAsync(h_bias_field, ctx->h_bias.p, nv * 4, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return s;
+}
+
+}  // extern "C"
+
+struct n4_batch_graph {
+  n4_context *ctx = nullptr;
+  Prepared P;
+  n4_params_t params{};
+  char *h_desc = nullptr, *d_desc = nullptr, *h_rep = nullptr;
+  size_t rep_bytes = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t done = nullptr;
+  bool launched = false;
+};
+
+static void graph_free(n4_batch_graph *g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->done) cudaEventDestroy(g->done);
+  if (g->h_desc) cudaFreeHost(g->h_desc);
+  if (g->h_rep) cudaFreeHost(g->h_rep);
+  if (g->d_desc) cudaFree(g->d_desc);
+  delete g;
+}
+
+extern "C" {
+
+n4_status_t n4_batch_graph_create(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols,
+                                  n4_batch_graph_t **out) {
+  if (!ctx || !vols || n < 1 || !out) return fail(N4_ERR_INVALID_ARG, "bad arguments");
+  *out = nullptr;
+  TRY(check_params(p));
+  CK(cudaSetDevice(ctx->device));
+  std::vector<RunVol> v(n);
+  for (int i = 0; i < n; ++i) {
+    const n4_volume_t &q = vols[i];
+    if (!q.im || !q.im_normalized || !q.lattice) return fail(N4_ERR_INVALID_ARG, "NULL pointer in batch");
+    TRY(make_dims(p, q.fx, q.fy, q.fz, v[i].d));
+    v[i].im = q.im; v[i].mask = q.mask; v[i].out = q.im_normalized; v[i].lat = q.lattice;
+    v[i].bias = q.bias_field; v[i].warm = q.warm_lattice;
+  }
+  n4_batch_graph *g = new n4_batch_graph();
+  g->ctx = ctx;
+  g->params = *p;
+  n4_status_t s = plan_run(ctx, p, v, nullptr, g->P);
+  if (s != N4_OK) { graph_free(g); return s; }
+  const Prepared &P = g->P;
+  g->rep_bytes = P.o_flg + 4 * (size_t)P.n - P.o_rep;
+  cudaError_t e;
+  if ((e = cudaMallocHost((void **)&g->h_desc, P.bytes)) || (e = cudaMallocHost((void **)&g->h_rep, g->rep_bytes)) ||
+      (e = cudaMalloc((void **)&g->d_desc, P.bytes)) || (e = cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming))) {
+    graph_free(g);
+    return fail(N4_ERR_OOM, cudaGetErrorString(e));
+  }
+  std::memset(g->h_desc, 0, P.bytes);
+  std::memset(g->h_rep, 0, g->rep_bytes);
+  DescBuf B{g->h_desc, g->d_desc};
+  fill_descriptors(ctx, p, g->P, B);
+  cudaStream_t cs;
+  CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  s = N4_OK;
+  if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed)) != cudaSuccess) {
+    s = fail(N4_ERR_CUDA, cudaGetErrorString(e));
+  } else {
+    // every replay starts from the pristine descriptors (reports, queue counter)
+    if ((e = cudaMemcpyAsync(B.d, B.h, P.bytes, cudaMemcpyHostToDevice, cs)) != cudaSuccess)
+      s = fail(N4_ERR_CUDA, cudaGetErrorString(e));
+    if (s == N4_OK) s = enqueue_run(ctx, p, P, B, cs, false);
+    if (s == N4_OK &&
+        (e = cudaMemcpyAsync(g->h_rep, B.d + P.o_rep, g->rep_bytes, cudaMemcpyDeviceToHost, cs)) != cudaSuccess)
+      s = fail(N4_ERR_CUDA, cudaGetErrorString(e));
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(cs, &graph);
+    if (s == N4_OK && e != cudaSuccess) s = fail(N4_ERR_CUDA, cudaGetErrorString(e));
+    g->graph = graph;
+    if (s == N4_OK && (e = cudaGraphInstantiate(&g->exec, graph, 0)) != cudaSuccess)
+      s = fail(N4_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaStreamDestroy(cs);
+  cudaGetLastError();
+  if (s != N4_OK) { graph_free(g); return s; }
+  *out = g;
+  return N4_OK;
+}
+
+n4_status_t n4_batch_graph_launch(n4_batch_graph_t *g, void *stream) {
+  if (!g) return fail(N4_ERR_INVALID_ARG, "graph is NULL");
+  CK(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  CK(cudaEventRecord(g->done, (cudaStream_t)stream));
+  g->launched = true;
+  return N4_OK;
+}
+
+n4_status_t n4_batch_graph_sync(n4_batch_graph_t *g, n4_report_t *reports, int n) {
+  if (!g) return fail(N4_ERR_INVALID_ARG, "graph is NULL");
+  if (!g->launched) return fail(N4_ERR_INVALID_ARG, "graph not launched");
+  CK(cudaEventSynchronize(g->done));
+  const Prepared &P = g->P;
+  const n4_report_t *rep = (const n4_report_t *)g->h_rep;
+  const int *flg = (const int *)(g->h_rep + (P.o_flg - P.o_rep));
+  n4_status_t worst = N4_OK;
+  for (int i = 0; i < P.n; ++i) {
+    n4_report_t r = rep[i];
+    if (r.status == -1) r.status = N4_ERR_CUDA;
+    if (r.status == N4_OK && flg[i]) r.status = N4_ERR_NONFINITE;
+    r.path = P.path[i];
+    r.cluster_size = P.csize[i];
+    if (reports && i < n) reports[i] = r;
+    if (r.status != N4_OK && worst == N4_OK) worst = (n4_status_t)r.status;
+  }
+  if (worst != N4_OK) return fail(worst, std::string("volume failed: ") + n4_status_string(worst));
+  return N4_OK;
+}
+
+n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *g) {
+  if (!g) return N4_OK;
+  cudaSetDevice(g->ctx->device);
+  if (g->launched) cudaEventSynchronize(g->done);
+  graph_free(g);
+  return N4_OK;
 }
 
 // ---------------------------------------------------------------- components

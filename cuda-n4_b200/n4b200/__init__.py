@@ -36,7 +36,7 @@ from . import _lib
 from ._lib import N4Error, check, n4_params_t, n4_report_t, n4_volume_t
 
 __all__ = [
-    "N4Param", "N4", "N4Batch", "N4Result", "Context", "FitBspline3D",
+    "N4Param", "N4", "N4Batch", "N4BatchGraph", "N4Result", "Context", "FitBspline3D",
     "EvaluateBspline3D", "UpsampleLattice3D", "upsampleLattice3D", "sharpenImage",
     "CalculateConvergenceMeasurement", "calculateConvergenceMeasurement", "N4Error",
     "lattice_dims", "library",
@@ -295,6 +295,63 @@ def N4Batch(volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=No
         for r, rep in zip(results, reps):
             r.report = _report_dict(rep)
     return results
+
+
+class N4BatchGraph:
+    """A batched run recorded once as a CUDA graph and replayed with
+    ``launch()`` (``n4_batch_graph_*``).  Inputs are read from the given
+    CUDA tensors at every launch (refill them in place to correct new data);
+    outputs are written to ``results[i].im_normalized`` etc."""
+
+    def __init__(self, volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=None,
+                 return_bias=False, ctx: Optional[Context] = None):
+        torch = _torch()
+        param = param or N4Param()
+        self._cpar = param.to_c()
+        dims = lattice_dims(param)
+        n = len(volumes)
+        arr = (n4_volume_t * n)()
+        self._keep, self.results = [], []
+        dev = None
+        for i, (im, mask) in enumerate(volumes):
+            imt = _dev_f32(im)
+            dev = imt.device
+            mk = None if mask is None else _dev_f32(mask, dev)
+            wl = None if warm_lattices is None or warm_lattices[i] is None else _dev_f32(warm_lattices[i], dev)
+            out = torch.empty_like(imt)
+            lat = torch.empty(dims, dtype=torch.float32, device=dev)
+            bias = torch.empty_like(imt) if return_bias else None
+            self._keep += [imt, mk, wl]
+            fx, fy, fz = (int(d) for d in imt.shape)
+            arr[i] = n4_volume_t(_ptr(imt), _ptr(mk), fx, fy, fz, _ptr(out), _ptr(lat), _ptr(bias), _ptr(wl))
+            self.results.append(N4Result(out, lat, bias, {}))
+        self.inputs = [(self._keep[3 * i], self._keep[3 * i + 1]) for i in range(n)]
+        self.ctx = ctx or Context.default(dev.index or 0)
+        self.device = dev
+        self._h = C.c_void_p()
+        check(_lib.load().n4_batch_graph_create(self.ctx.handle, C.byref(self._cpar), n, arr, C.byref(self._h)))
+
+    def launch(self):
+        check(_lib.load().n4_batch_graph_launch(self._h, _stream(self.device)))
+
+    def sync(self):
+        n = len(self.results)
+        reps = (n4_report_t * n)()
+        check(_lib.load().n4_batch_graph_sync(self._h, reps, n))
+        for r, rep in zip(self.results, reps):
+            r.report = _report_dict(rep)
+        return self.results
+
+    def close(self):
+        if self._h:
+            _lib.load().n4_batch_graph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------- components

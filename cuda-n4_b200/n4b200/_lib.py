@@ -95,6 +95,11 @@ SIGNATURES = [
     ("n4_run_batched", C.c_int, [_P, C.POINTER(n4_params_t), C.c_int, C.POINTER(n4_volume_t), _P,
                                  C.POINTER(n4_report_t)]),
     ("n4_sync", C.c_int, [_P, C.POINTER(n4_report_t), C.c_int]),
+    ("n4_batch_graph_create", C.c_int, [_P, C.POINTER(n4_params_t), C.c_int, C.POINTER(n4_volume_t),
+                                        C.POINTER(C.c_void_p)]),
+    ("n4_batch_graph_launch", C.c_int, [_P, _P]),
+    ("n4_batch_graph_sync", C.c_int, [_P, C.POINTER(n4_report_t), C.c_int]),
+    ("n4_batch_graph_destroy", C.c_int, [_P]),
     ("n4_set_profiling", C.c_int, [_P, C.c_int]),
     ("n4_last_timings", C.c_int, [_P, C.POINTER(n4_timings_t)]),
     ("n4_fit_bspline3d", C.c_int, [_P, _P, _P, _U, _U, _U, _U, _U, _U, C.c_float, C.c_int, _P, _P]),

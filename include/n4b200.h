@@ -134,6 +134,19 @@ n4_status_t n4_run_batched(n4_context_t *ctx, const n4_params_t *p, int n,
 /* Wait for the context's last asynchronous run and fill its reports. */
 n4_status_t n4_sync(n4_context_t *ctx, n4_report_t *reports, int n);
 
+/* A batched run recorded once as a CUDA graph (no counterpart in the
+ * reference).  Every launch repeats the run on the same buffers (the
+ * caller may refill the inputs in between) without host-side planning.
+ * The graph uses the context's workspaces: do not run other work on the
+ * context while a launch is in flight. */
+typedef struct n4_batch_graph n4_batch_graph_t;
+n4_status_t n4_batch_graph_create(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols,
+                                  n4_batch_graph_t **graph);
+n4_status_t n4_batch_graph_launch(n4_batch_graph_t *graph, void *stream);
+/* Wait for the last launch and fill its reports (n entries, may be NULL). */
+n4_status_t n4_batch_graph_sync(n4_batch_graph_t *graph, n4_report_t *reports, int n);
+n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *graph);
+
 /* ---- measurement (no counterpart in the reference) ----
  * With profiling enabled, every run records CUDA events around its kernels
  * on the run's stream; n4_last_timings waits for the last run and returns

@@ -249,3 +249,31 @@ def test_nonfinite_input_is_reported(cuda):
     im[8, 8, 8] = np.inf
     with pytest.raises(n4b200.N4Error, match="NONFINITE"):
         n4b200.N4(cuda.tensor(im, device="cuda"), cuda.tensor(ph.mask, device="cuda"), param(1, [2], 0.0))
+
+
+def test_batch_graph_replays(cuda):
+    """The graph-recorded batch equals N4Batch, and a launch after refilling
+    an input in place corrects the new data."""
+    import n4b200
+    shapes = [(40, 48, 32), (64, 56, 40), (24, 32, 48)]
+    vols = []
+    for i, sh in enumerate(shapes):
+        ph = make_phantom(sh, seed=200 + i)
+        vols.append((cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")))
+    p = param(3, [20] * 3, 0.001)
+    g = n4b200.N4BatchGraph(vols, p)
+    for _ in range(2):
+        g.launch()
+    res = g.sync()
+    ref = n4b200.N4Batch(vols, p)
+    for r, q in zip(res, ref):
+        assert r.report["status"] == "N4_OK" and r.report["iterations"] == q.report["iterations"]
+        assert cuda.equal(r.lattice, q.lattice) and cuda.equal(r.im_normalized, q.im_normalized)
+    ph = make_phantom(shapes[0], seed=999)
+    g.inputs[0][0].copy_(cuda.tensor(ph.im, device="cuda"))
+    g.inputs[0][1].copy_(cuda.tensor(ph.mask, device="cuda"))
+    g.launch()
+    res = g.sync()
+    single = n4b200.N4(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"), p)
+    assert cuda.equal(res[0].lattice, single.lattice)
+    g.close()
