@@ -912,12 +912,7 @@ n4_status_t n4_last_timings(n4_context_t *ctx, n4_timings_t *t) {
   if (!ctx || !t) return fail(N4_ERR_INVALID_ARG, "NULL argument");
   if (!ctx->prof_valid) return fail(N4_ERR_INVALID_ARG, "no profiled run");
   CK(cudaEventSynchronize(ctx->ev[4]));
-  float ms[4];
-  for (int k = 0; k < 4; ++k) CK(cudaEventElapsedTime(&ms[k], ctx->ev[k], ctx->ev[k + 1]));
-  t->prologue_ms = ms[0];
-  t->n4_ms = ms[1];
-  t->tables_ms = ms[2];
-  t->correct_ms = ms[3];
+  for (int k = 0; k < 4; ++k) CK(cudaEventElapsedTime(&t->stage_ms[k], ctx->ev[k], ctx->ev[k + 1]));
   t->launches = ctx->prof_launches;
   t->fit_voxels = ctx->prof_fit;
   t->full_voxels = ctx->prof_full;
@@ -1125,12 +1120,21 @@ n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const floa
   float *t1n = ctx->s1.as<float>(), *t1d = t1n + t1, *t2n = ctx->s2.as<float>(), *t2d = t2n + t2;
   const int gb = ctx->nsm * 8;
   const long long rows = (long long)fx * fy;
+  const bool prof = ctx->profiling != 0;
+  if (prof) TRY(prof_mark(ctx, 0, st));
   k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(d_field, d_mask, rows, fz, az,
                                                                                  t1n, t1d);
+  if (prof) TRY(prof_mark(ctx, 1, st));
   k_fit_planes<<<(int)std::min<size_t>((t2 + 255) / 256, gb), 256, 0, st>>>(t1n, t1d, fx, fy, ay, ncpt_z, t2n, t2d);
+  if (prof) TRY(prof_mark(ctx, 2, st));
   const int nlat = ncpt_x * ncpt_y * ncpt_z;
   k_fit_final<<<(nlat + 255) / 256, 256, 0, st>>>(t2n, t2d, fx, ax, ncpt_y, ncpt_z, eps, zero_den, d_lattice);
+  if (prof) { TRY(prof_mark(ctx, 3, st)); TRY(prof_mark(ctx, 4, st)); }
   CK(cudaGetLastError());
+  ctx->prof_launches = 4;
+  ctx->prof_fit = (long long)fx * fy * fz;
+  ctx->prof_full = 0;
+  ctx->prof_valid = prof;
   return N4_OK;
 }
 
@@ -1142,6 +1146,7 @@ n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice, uns
   if (ncpt_z > (unsigned)kMaxNcz) return fail(N4_ERR_TOO_LARGE, "at most 64 control points along z");
   cudaStream_t st = (cudaStream_t)stream;
   Axis ax, ay, az;
+  if (ctx->profiling) TRY(prof_mark(ctx, 0, st));
   TRY(component_tables(ctx, fx, fy, fz, ncpt_x, ncpt_y, ncpt_z, st, ax, ay, az));
   CorrectVol cv{nullptr, d_fitted, nullptr, d_lattice, (char *)ax.s, (char *)ay.s, (char *)az.s,
                 (int)fx, (int)fy, (int)fz, (int)ncpt_x, (int)ncpt_y, (int)ncpt_z, 0,
@@ -1153,8 +1158,15 @@ n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice, uns
   TRY(begin_run(ctx, st));
   CK(cudaMemcpyAsync(u.slot->d.p, u.slot->h, sizeof(cv) + 16, cudaMemcpyHostToDevice, st));
   const size_t so = align_up(sizeof(cv), 16);
+  const bool prof = ctx->profiling != 0;
+  if (prof) TRY(prof_mark(ctx, 1, st));
   k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0.0f);
   CK(cudaGetLastError());
+  if (prof) { TRY(prof_mark(ctx, 2, st)); TRY(prof_mark(ctx, 3, st)); TRY(prof_mark(ctx, 4, st)); }
+  ctx->prof_launches = 2;
+  ctx->prof_fit = 0;
+  ctx->prof_full = (long long)fx * fy * fz;
+  ctx->prof_valid = prof;
   u.slot->nrep = 0;
   return end_run(ctx, st, u);
 }

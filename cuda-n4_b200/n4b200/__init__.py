@@ -154,7 +154,8 @@ class Context:
     def last_timings(self) -> dict:
         t = _lib.n4_timings_t()
         check(_lib.load().n4_last_timings(self._h, C.byref(t)))
-        return {k: getattr(t, k) for k, _ in t._fields_}
+        return dict(stage_ms=list(t.stage_ms), launches=t.launches, fit_voxels=t.fit_voxels,
+                    full_voxels=t.full_voxels)
 
     @classmethod
     def default(cls, device: int = 0) -> "Context":

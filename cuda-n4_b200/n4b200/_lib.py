@@ -69,8 +69,7 @@ class n4_volume_t(C.Structure):
 
 class n4_timings_t(C.Structure):
     _fields_ = [
-        ("prologue_ms", C.c_float), ("n4_ms", C.c_float), ("tables_ms", C.c_float),
-        ("correct_ms", C.c_float), ("launches", C.c_int), ("fit_voxels", C.c_longlong),
+        ("stage_ms", C.c_float * 4), ("launches", C.c_int), ("fit_voxels", C.c_longlong),
         ("full_voxels", C.c_longlong),
     ]
 

@@ -148,17 +148,19 @@ n4_status_t n4_batch_graph_sync(n4_batch_graph_t *graph, n4_report_t *reports, i
 n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *graph);
 
 /* ---- measurement (no counterpart in the reference) ----
- * With profiling enabled, every run records CUDA events around its kernels
- * on the run's stream; n4_last_timings waits for the last run and returns
- * the device time of each stage and how many kernels it launched. */
+ * With profiling enabled, every call records CUDA events around its kernels
+ * on its stream; n4_last_timings waits for the last profiled call and
+ * returns the device time of its stages:
+ *   n4_run / n4_run_batched: [0] threshold/shrink/log, [1] all levels and
+ *     iterations, [2] full-resolution tables, [3] evaluation + im / exp(b);
+ *   n4_fit_bspline3d: [0] z contraction (one pass over field and mask),
+ *     [1] y contraction, [2] x contraction and division, [3] 0;
+ *   n4_evaluate_bspline3d: [0] tables, [1] dense evaluation, [2], [3] 0. */
 typedef struct {
-  float prologue_ms;   /* threshold / shrink / log                        */
-  float n4_ms;         /* all levels and iterations (cluster or grid)     */
-  float tables_ms;     /* full-resolution B-spline tables                 */
-  float correct_ms;    /* fused evaluation + im / exp(b) at full size     */
-  int launches;        /* kernels launched by the run                     */
-  long long fit_voxels;    /* fitting-grid voxels of the run              */
-  long long full_voxels;   /* full-resolution voxels of the run           */
+  float stage_ms[4];
+  int launches;            /* kernels launched by the call                */
+  long long fit_voxels;    /* fitting-grid voxels of the call             */
+  long long full_voxels;   /* full-resolution voxels of the call          */
 } n4_timings_t;
 
 n4_status_t n4_set_profiling(n4_context_t *ctx, int enable);

@@ -275,5 +275,7 @@ def test_batch_graph_replays(cuda):
     g.launch()
     res = g.sync()
     single = n4b200.N4(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"), p)
-    assert cuda.equal(res[0].lattice, single.lattice)
+    # the histogram's fixed-point scale follows the batch's largest volume, so
+    # a volume in a batch matches its single run to round-off, not bitwise
+    assert nrel(res[0].lattice, single.lattice.cpu().numpy().astype(np.float64)) < 1e-6
     g.close()
