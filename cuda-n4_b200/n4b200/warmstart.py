@@ -1,4 +1,4 @@
-"""Training data and end-to-end use of the learned warm start.
+"""Training data, training and evaluation of the learned warm start.
 
 * ``phantoms_gpu`` — seeded phantoms generated on the GPU (same model as
   ``phantom.make_phantom``: nested jittered ellipsoids, exp of a cubic
@@ -8,16 +8,29 @@
   first-level 4x4x4 lattice of the plain GPU N4 run to convergence with one
   fitting level at the run's shrink factor.
 * ``train_encoder`` — Adam on MSE with the tensor-core encoder.
+* ``evaluate`` — held-out phantoms corrected batched with and without the
+  predicted warm lattices: iterations, volumes/s, warm starts kept, and the
+  largest log-bias difference between the two runs.
 * ``WarmBatch`` — pool + predict + batched N4 with the predictions as warm
   lattices (the batch itself recorded as a CUDA graph).
+
+Command line (GPU)::
+
+    python -m n4b200.warmstart train --out weights.npy      # 4096 x 128x128x96, 20 epochs
+    python -m n4b200.warmstart eval --weights weights.npy   # 256 x 256x256x176
 """
 from __future__ import annotations
 
 import numpy as np
 
-from . import N4Batch, N4BatchGraph, N4Param
+import os
+
+from . import EvaluateBspline3D, N4Batch, N4BatchGraph, N4Param
 from .encoder import Encoder, pool_input, train
 from .phantom import _axis_weights
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "warmstart_encoder.npy")
+TRAIN_GEN = dict(sigma=0.03, grid=6, coeff_std=0.3)
 
 
 def phantoms_gpu(n, shape, seed, sigma=0.03, grid=6, coeff_std=0.3, device="cuda"):
@@ -54,6 +67,23 @@ def label_param(shrink):
                    low_value=0.0, ShrinkFactor=shrink)
 
 
+def eval_param(shrink=4, levels=4):
+    """The 256x256x176 workload's parameters: 4 levels, <= 50 iterations,
+    convergence 0.001, 200 bins, FWHM 0.15, Wiener 0.01."""
+    return N4Param(NumberOfFittingLevels=levels, MaximumNumberOfIterations=50, ConvergenceThreshold=0.001,
+                   low_value=0.0, ShrinkFactor=shrink)
+
+
+def predict_warm(enc: Encoder, volumes, low_value=0.0):
+    """First-level lattices [n, 4, 4, 4] predicted for (im, mask) pairs."""
+    import torch
+    n = len(volumes)
+    x = torch.empty((n, 32, 32, 24), dtype=torch.bfloat16, device=volumes[0][0].device)
+    for i, (im, mask) in enumerate(volumes):
+        pool_input(im, mask, low_value, out=x[i])
+    return enc.predict(x)
+
+
 def make_dataset(n, shape, seed, shrink=4, chunk=256, **gen):
     """(x [n,32,32,24] bf16, y [n,4,4,4] float) on the GPU."""
     import torch
@@ -75,9 +105,12 @@ def train_encoder(n_train=4096, n_val=256, shape=(128, 128, 96), epochs=20, batc
                   shrink=4, **gen):
     """Generate data with the plain GPU N4 and train; returns (encoder, report dict)."""
     import time
+    import torch
+    gen = {**TRAIN_GEN, **gen}
     t0 = time.time()
     x, y = make_dataset(n_train, shape, seed, shrink, **gen)
     xv, yv = make_dataset(n_val, shape, seed + 1_000_000, shrink, **gen)
+    torch.cuda.synchronize()
     t_data = time.time() - t0
     enc = Encoder(max_batch=batch, seed=seed)
     rep = train(enc, x, y.reshape(-1, 64), epochs=epochs, batch=batch, lr=lr, seed=seed,
@@ -86,6 +119,72 @@ def train_encoder(n_train=4096, n_val=256, shape=(128, 128, 96), epochs=20, batc
     return enc, dict(n_train=n_train, n_val=n_val, epochs=epochs, data_seconds=t_data, train_seconds=rep.seconds,
                      loss_first_epoch=rep.losses[0], loss_last_epoch=rep.losses[-1], val_mse=rep.val_loss,
                      val_mse_of_mean_predictor=base)
+
+
+def evaluate(enc: Encoder, n_eval=256, shape=(256, 256, 176), seed=5_000_000, chunk=32, param=None, **gen):
+    """Held-out phantoms corrected batched from zero and from the predicted
+    lattices.  Returns mean iterations of both runs, device-timed volumes/s
+    of both batched runs (pooling and prediction included in the warm one),
+    the share of warm starts kept, and the log-bias difference d between the
+    two runs at full resolution: max |d| over the mask, max |d - mean_mask(d)|
+    over the mask (a constant log bias is a global intensity scale, which the
+    convergence measure std/mean of exp(change) does not see, so two runs
+    stopping at CV < threshold may differ by one), and max |d| over the whole
+    field of view (outside the mask the lattice is extrapolated)."""
+    import torch
+    gen = {**TRAIN_GEN, **gen}
+    param = param or eval_param()
+    dims = param.lattice_dims()
+    it_plain, it_warm, lvl1_plain, lvl1_warm, kept, dmask, dcent, dfov = [], [], [], [], [], [], [], []
+    ms_plain = ms_warm = 0.0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for c0 in range(0, n_eval, chunk):
+        m = min(chunk, n_eval - c0)
+        im, mask = phantoms_gpu(m, shape, seed + c0, **gen)
+        vols = [(im[i], mask[i]) for i in range(m)]
+        N4Batch(vols, param)                       # warm the context's workspaces
+        torch.cuda.synchronize()
+        ev[0].record()
+        plain = N4Batch(vols, param, synchronous=False)
+        ev[1].record()
+        ev[2].record()
+        warm_lat = predict_warm(enc, vols)
+        warm = N4Batch(vols, param, warm_lattices=[warm_lat[i] for i in range(m)], synchronous=False)
+        ev[3].record()
+        torch.cuda.synchronize()
+        ms_plain += ev[0].elapsed_time(ev[1])
+        ms_warm += ev[2].elapsed_time(ev[3])
+        # reports (synchronous reruns are bitwise identical: the engine is deterministic)
+        plain = N4Batch(vols, param)
+        warm = N4Batch(vols, param, warm_lattices=[warm_lat[i] for i in range(m)])
+        for i, (a, b) in enumerate(zip(plain, warm)):
+            it_plain.append(sum(a.report["iterations"][:a.report["levels"]]))
+            it_warm.append(sum(b.report["iterations"][:b.report["levels"]]))
+            lvl1_plain.append(a.report["iterations"][0])
+            lvl1_warm.append(b.report["iterations"][0])
+            kept.append(b.report["warm_start_used"])
+            d = EvaluateBspline3D(b.lattice - a.lattice, dims, tuple(shape))
+            inside = d[mask[i] != 0]
+            dmask.append(float(inside.abs().max()))
+            dcent.append(float((inside - inside.double().mean().float()).abs().max()))
+            dfov.append(float(d.abs().max()))
+        del im, mask, vols, plain, warm
+    n = len(it_plain)
+    return dict(n_eval=n, shape=list(shape),
+                iterations_plain=float(np.mean(it_plain)), iterations_warm=float(np.mean(it_warm)),
+                level1_iterations_plain=float(np.mean(lvl1_plain)),
+                level1_iterations_warm=float(np.mean(lvl1_warm)),
+                warm_kept=float(np.mean(kept)),
+                volumes_per_s_plain_batched=n / (ms_plain / 1000.0),
+                volumes_per_s_warm_batched=n / (ms_warm / 1000.0),
+                max_abs_log_bias_diff_mask=float(np.max(dmask)),
+                max_abs_log_bias_diff_mask_mean_removed=float(np.max(dcent)),
+                median_abs_log_bias_diff_mask_mean_removed=float(np.median(dcent)),
+                max_abs_log_bias_diff_fov=float(np.max(dfov)))
+
+
+def load_encoder(path=WEIGHTS, max_batch=64) -> Encoder:
+    return Encoder(max_batch=max_batch, params=np.load(path))
 
 
 class WarmBatch:
@@ -112,3 +211,34 @@ class WarmBatch:
 
     def sync(self):
         return self.graph.sync()
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(prog="python -m n4b200.warmstart")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--out", default=WEIGHTS)
+    t.add_argument("--n-train", type=int, default=4096)
+    t.add_argument("--n-val", type=int, default=256)
+    t.add_argument("--epochs", type=int, default=20)
+    t.add_argument("--seed", type=int, default=0)
+    e = sub.add_parser("eval")
+    e.add_argument("--weights", default=WEIGHTS)
+    e.add_argument("--n-eval", type=int, default=256)
+    e.add_argument("--untrained", action="store_true", help="random-init encoder (the method without training)")
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        enc, rep = train_encoder(n_train=a.n_train, n_val=a.n_val, epochs=a.epochs, seed=a.seed)
+        os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+        np.save(a.out, enc.params())
+        rep["weights"] = a.out
+        print(json.dumps(rep))
+    else:
+        enc = Encoder(max_batch=64, seed=0) if a.untrained else load_encoder(a.weights)
+        print(json.dumps(evaluate(enc, n_eval=a.n_eval)))
+
+
+if __name__ == "__main__":
+    main()
