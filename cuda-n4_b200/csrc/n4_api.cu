@@ -7,6 +7,7 @@
 // and iterations on the device), per-axis tables, and the fused full-
 // resolution correction.  Workspaces are owned by the context and only grow.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1237,6 +1238,75 @@ n4_status_t n4_convergence(n4_context_t *ctx, const float *d_field1, const float
   double var = s1 / c - m * m;
   if (ddof) var = c > 1.0 ? var * c / (c - 1.0) : 0.0;
   *cv = std::sqrt(var > 0 ? var : 0.0) / (1.0 + m);
+  return N4_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- no-allocation fit
+// Fixed device scratch for n4_fit_bspline3d_noalloc: the three axis tables,
+// T1 (numerator/denominator per field row and z control point) and T2 (per
+// x voxel and (y, z) control point).  Every entry the fit reads is written
+// earlier in the same call, so nothing in it has to start at zero.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 8u << 20;   // 8 MiB per device
+static __device__ __align__(256) unsigned char g_fit_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::atomic<void *> g_fit_scratch_ptr[kMaxDevices];
+
+// The three tables of one call, passed by value (no descriptor upload).
+__global__ void k_axis_tables_by_value(TableJob jx, TableJob jy, TableJob jz) {
+  const TableJob t = blockIdx.x == 0 ? jx : (blockIdx.x == 1 ? jy : jz);
+  build_axis(axis_at(t.base, t.n, t.nc));
+}
+
+}  // namespace
+
+extern "C" {
+
+n4_status_t n4_fit_bspline3d_noalloc(const float *d_field, const float *d_mask, unsigned int ncpt_x,
+                                     unsigned int ncpt_y, unsigned int ncpt_z, unsigned int fx, unsigned int fy,
+                                     unsigned int fz, float eps, int zero_den, float *d_lattice, void *stream) {
+  if (!d_field || !d_lattice) return fail(N4_ERR_INVALID_ARG, "NULL pointer");
+  if (ncpt_x < 4 || ncpt_y < 4 || ncpt_z < 4 || !fx || !fy || !fz) return fail(N4_ERR_INVALID_ARG, "bad sizes");
+  const size_t bx = align_up(axis_bytes(fx, ncpt_x - 3), 256), by = align_up(axis_bytes(fy, ncpt_y - 3), 256),
+               bz = align_up(axis_bytes(fz, ncpt_z - 3), 256);
+  const size_t t1 = (size_t)fx * fy * ncpt_z, t2 = (size_t)fx * ncpt_y * ncpt_z;
+  const size_t need = bx + by + bz + align_up(t1 * 8, 256) + align_up(t2 * 8, 256);
+  if (need > kNoAllocScratchBytes) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg),
+                  "n4_fit_bspline3d_noalloc needs %zu bytes of scratch; its fixed scratch holds %zu "
+                  "(use n4_fit_bspline3d)", need, kNoAllocScratchBytes);
+    return fail(N4_ERR_TOO_LARGE, msg);
+  }
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(N4_ERR_INVALID_ARG, "device ordinal out of range");
+  char *base = (char *)g_fit_scratch_ptr[dev].load(std::memory_order_acquire);
+  if (!base) {   // once per device: the scratch's device address
+    void *p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_fit_scratch));
+    g_fit_scratch_ptr[dev].store(p, std::memory_order_release);
+    base = (char *)p;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const TableJob jx{base, (int)fx, (int)ncpt_x}, jy{base + bx, (int)fy, (int)ncpt_y},
+      jz{base + bx + by, (int)fz, (int)ncpt_z};
+  k_axis_tables_by_value<<<3, 256, 0, st>>>(jx, jy, jz);
+  const Axis ax = axis_at(jx.base, fx, ncpt_x), ay = axis_at(jy.base, fy, ncpt_y), az = axis_at(jz.base, fz, ncpt_z);
+  float *t1n = (float *)(base + bx + by + bz), *t1d = t1n + t1;
+  float *t2n = (float *)(base + bx + by + bz + align_up(t1 * 8, 256)), *t2d = t2n + t2;
+  const long long rows = (long long)fx * fy;
+  k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(d_field, d_mask, rows, fz, az,
+                                                                                 t1n, t1d);
+  k_fit_planes<<<(int)std::min<size_t>((t2 + 255) / 256, 148 * 8), 256, 0, st>>>(t1n, t1d, fx, fy, ay, ncpt_z, t2n,
+                                                                                   t2d);
+  const int nlat = ncpt_x * ncpt_y * ncpt_z;
+  k_fit_final<<<(nlat + 255) / 256, 256, 0, st>>>(t2n, t2d, fx, ax, ncpt_y, ncpt_z, eps, zero_den, d_lattice);
+  CK(cudaGetLastError());
   return N4_OK;
 }
 

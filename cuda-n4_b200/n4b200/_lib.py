@@ -102,6 +102,7 @@ SIGNATURES = [
     ("n4_set_profiling", C.c_int, [_P, C.c_int]),
     ("n4_last_timings", C.c_int, [_P, C.POINTER(n4_timings_t)]),
     ("n4_fit_bspline3d", C.c_int, [_P, _P, _P, _U, _U, _U, _U, _U, _U, C.c_float, C.c_int, _P, _P]),
+    ("n4_fit_bspline3d_noalloc", C.c_int, [_P, _P, _U, _U, _U, _U, _U, _U, C.c_float, C.c_int, _P, _P]),
     ("n4_evaluate_bspline3d", C.c_int, [_P, _P, _U, _U, _U, _U, _U, _U, _P, _P]),
     ("n4_upsample_lattice3d", C.c_int, [_P, _P, _U, _U, _U, _P, _P]),
     ("n4_sharpen_image", C.c_int, [_P, _P, _P, _U, _U, C.c_float, C.c_float, _P,

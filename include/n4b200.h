@@ -176,6 +176,25 @@ n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const floa
                              unsigned int fx, unsigned int fy, unsigned int fz,
                              float eps, int zero_den, float *d_lattice, void *stream);
 
+/* No counterpart in the reference (its FitBspline3D cudaMallocs and frees
+ * three buffers per call, cudaN4.cu:1275-1365).  The same fit as
+ * n4_fit_bspline3d for callers that must not allocate device memory during
+ * the call, e.g. code running under a fixed memory budget or a caching
+ * allocator that owns the whole device: it takes no context and makes no
+ * cudaMalloc/cudaFree or allocating library call.  Its scratch is one fixed
+ * 8 MiB device array per device, which holds the axis tables plus
+ * fx*fy*ncpt_z*8 + fx*ncpt_y*ncpt_z*8 bytes (e.g. 256x256 rows with up to
+ * 15 control points along z); larger fits return N4_ERR_TOO_LARGE and need
+ * n4_fit_bspline3d.  The first call on a device looks up the array's address
+ * (make it before any stream capture).  Calls on one device share the
+ * scratch: two calls that may overlap in time (different streams or host
+ * threads) race and must be ordered by the caller.  Runs on the current
+ * device, asynchronously on `stream`. */
+n4_status_t n4_fit_bspline3d_noalloc(const float *d_field, const float *d_mask,
+                                     unsigned int ncpt_x, unsigned int ncpt_y, unsigned int ncpt_z,
+                                     unsigned int fx, unsigned int fy, unsigned int fz,
+                                     float eps, int zero_den, float *d_lattice, void *stream);
+
 /* Replaces EvaluateBspline3D (cudaN4.h:288-298). */
 n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice,
                                   unsigned int ncpt_x, unsigned int ncpt_y, unsigned int ncpt_z,
