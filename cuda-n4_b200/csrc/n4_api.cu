@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -33,6 +34,10 @@ n4_status_t fail(n4_status_t s, const std::string &msg) {
 
 // shared with the encoder translation unit
 n4_status_t n4_record_error(n4_status_t s, const char *msg) { return fail(s, msg); }
+// defined in the encoder translation unit
+int n4_encoder_capacity(const n4_encoder_t *enc);
+// kernels one n4_encoder_predict call launches (4 convolutions + the head)
+constexpr int kEncoderLaunches = 5;
 
 namespace {
 
@@ -92,13 +97,9 @@ struct Slot {
   std::vector<int> path, csize;
 };
 
-struct TuneKey {
-  int X, Y, Z, nx, ny, nz, levels, bins, batch;
-  bool operator<(const TuneKey &o) const {
-    return std::tie(X, Y, Z, nx, ny, nz, levels, bins, batch) <
-           std::tie(o.X, o.Y, o.Z, o.nx, o.ny, o.nz, o.levels, o.bins, o.batch);
-  }
-};
+// Autotuner key: lattice, levels, bins and the fitting-grid size of every
+// volume of the run, in order.
+using TuneKey = std::vector<int>;
 struct TuneVal {
   int grid;   // 1 = whole-GPU path
   int K;      // CTAs per cluster
@@ -116,6 +117,7 @@ struct n4_context {
   int max_smem = 0;
   DevBuf imlog, tables, logu, big, red, bar;
   DevBuf s1, s2, s3, s4, s5;   // component scratch
+  DevBuf warm_x, warm_lat;     // learned warm start: network inputs, predicted lattices
   DevBuf h_im, h_mask, h_out, h_lat, h_bias, h_warm;   // host-run staging
   Slot slots[kSlots];
   int next_slot = 0;
@@ -125,7 +127,6 @@ struct n4_context {
   std::map<TuneKey, TuneVal> tune;
   // max co-resident clusters per (threads, cluster size, shared bytes)
   std::map<std::tuple<int, int, int>, int> cluster_cap;
-  int attr_smem[2] = {0, 0};   // dynamic shared memory already granted (512, 1024 threads)
   // profiling
   int profiling = 0;
   cudaEvent_t ev[5] = {};
@@ -177,6 +178,7 @@ n4_status_t check_params(const n4_params_t *p) {
   if (!(p->FitEpsilon >= 0.0f)) return fail(N4_ERR_INVALID_ARG, "FitEpsilon must be >= 0");
   for (unsigned l = 0; l < p->NumberOfFittingLevels; ++l)
     if (p->MaximumNumberOfIterations[l] > 1000000u) return fail(N4_ERR_INVALID_ARG, "too many iterations");
+  if (((p->flags >> 8) & 31u) > 16u) return fail(N4_ERR_INVALID_ARG, "cluster size must be in [1, 16]");
   return N4_OK;
 }
 
@@ -289,15 +291,30 @@ bool cluster_fits(const n4_context *ctx, const Plan &pl) {
   return (long long)pl.sm_bytes + pl.big_bytes + kStaticSmemReserve <= ctx->max_smem;
 }
 
+// Dynamic shared memory granted to k_n4_cluster<NT> per device.  The
+// attribute belongs to the function (process-wide), not to a context, so the
+// record is process-wide too and the grant only ever grows.
+constexpr int kMaxDev = 64;
+std::mutex g_attr_mu;
+int g_attr_smem[kMaxDev][2];
+
+template <int NT>
+n4_status_t grant_cluster_smem(n4_context *ctx, int smem) {
+  if (ctx->device < 0 || ctx->device >= kMaxDev) return fail(N4_ERR_INVALID_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  int &granted = g_attr_smem[ctx->device][NT == 1024 ? 1 : 0];
+  if (smem > granted) {
+    CK(cudaFuncSetAttribute(k_n4_cluster<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CK(cudaFuncSetAttribute(k_n4_cluster<NT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    granted = smem;
+  }
+  return N4_OK;
+}
+
 template <int NT>
 n4_status_t cluster_capacity(n4_context *ctx, int K, int smem, int *nclusters) {
   auto kern = k_n4_cluster<NT>;
-  int &granted = ctx->attr_smem[NT == 1024 ? 1 : 0];
-  if (smem > granted) {
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    granted = smem;
-  }
+  TRY(grant_cluster_smem<NT>(ctx, smem));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(K);
   cfg.blockDim = dim3(NT);
@@ -464,12 +481,7 @@ template <int NT>
 n4_status_t launch_cluster_kernel(n4_context *ctx, const ClusterArgs &a, int K, int nclusters, int smem,
                                   cudaStream_t st) {
   auto kern = k_n4_cluster<NT>;
-  int &granted = ctx->attr_smem[NT == 1024 ? 1 : 0];
-  if (smem > granted) {
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    granted = smem;
-  }
+  TRY(grant_cluster_smem<NT>(ctx, smem));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(K * nclusters);
   cfg.blockDim = dim3(NT);
@@ -491,17 +503,34 @@ struct Choice {
   int K, nt;
 };
 
+TuneKey tune_key(const n4_params_t *p, const std::vector<Dims> &vols) {
+  TuneKey k{(int)p->NumberOfControlPoints_x, (int)p->NumberOfControlPoints_y, (int)p->NumberOfControlPoints_z,
+            (int)p->NumberOfFittingLevels, (int)p->NumberOfHistogramBins, (int)vols.size()};
+  for (const Dims &d : vols) { k.push_back(d.X); k.push_back(d.Y); k.push_back(d.Z); }
+  return k;
+}
+
 n4_status_t choose_path(n4_context *ctx, const n4_params_t *p, const std::vector<Dims> &vols, bool batch,
                         Choice &c) {
   const Dims &d0 = vols[0];
   c.nt = 1024;
   c.grid = false;
   c.K = 0;
-  if (!batch && vols.size() == 1) {
-    TuneKey key{d0.X, d0.Y, d0.Z, (int)p->NumberOfControlPoints_x, (int)p->NumberOfControlPoints_y,
-                (int)p->NumberOfControlPoints_z, (int)p->NumberOfFittingLevels, (int)p->NumberOfHistogramBins, 0};
-    auto it = ctx->tune.find(key);
-    if (it != ctx->tune.end() && !(p->flags & (N4_FLAG_FORCE_GRID | N4_FLAG_FORCE_CLUSTER))) {
+  (void)d0;
+  (void)batch;
+  const int forced_k = (int)((p->flags >> 8) & 31u);
+  if (forced_k) {
+    if (p->flags & N4_FLAG_FORCE_GRID) return fail(N4_ERR_INVALID_ARG, "cluster size given with FORCE_GRID");
+    Plan pl = make_plan(p, forced_k, vols, false);
+    int cap = 0;
+    if (cluster_fits(ctx, pl)) TRY(capacity(ctx, c.nt, forced_k, pl.sm_bytes + pl.big_bytes, &cap));
+    if (cap < 1) return fail(N4_ERR_TOO_LARGE, "a volume does not fit a cluster of the requested size");
+    c.K = forced_k;
+    return N4_OK;
+  }
+  if (!(p->flags & (N4_FLAG_FORCE_GRID | N4_FLAG_FORCE_CLUSTER))) {
+    auto it = ctx->tune.find(tune_key(p, vols));
+    if (it != ctx->tune.end()) {
       c.grid = it->second.grid != 0;
       c.K = it->second.K;
       c.nt = it->second.nt;
@@ -529,7 +558,9 @@ struct Prepared {
   std::vector<size_t> imlog_off, tab_off;
   int NCX = 0, NCY = 0, NCZ = 0;
   size_t o_pro = 0, o_pst = 0, o_job = 0, o_ord = 0, o_tab = 0, o_cor = 0, o_tst = 0, o_rep = 0, o_flg = 0,
-         o_q = 0, bytes = 0;
+         o_q = 0, o_pool = 0, bytes = 0;
+  n4_encoder_t *enc = nullptr;   // learned warm start run inside the batch
+  int enc_batch = 0;             // predictions per encoder call
   long long fit_total = 0, tiles = 0;
 };
 
@@ -543,10 +574,22 @@ struct DescBuf {
 
 // Choose paths, size the workspaces and lay out the descriptors.
 n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<RunVol> &rvs, const Choice *forced,
-                     Prepared &P) {
+                     Prepared &P, n4_encoder_t *enc = nullptr) {
   const int n = (int)rvs.size();
   P.n = n;
   P.rvs = rvs;
+  if (enc) {
+    if (p->NumberOfControlPoints_x != 4 || p->NumberOfControlPoints_y != 4 || p->NumberOfControlPoints_z != 4)
+      return fail(N4_ERR_INVALID_ARG, "the warm-start encoder predicts 4x4x4 first-level lattices");
+    for (const RunVol &r : rvs)
+      if (r.warm) return fail(N4_ERR_INVALID_ARG, "warm lattices are predicted by the encoder: pass none");
+    TRY(ctx->warm_x.ensure((size_t)n * kPoolCells * 2, "warm-start inputs"));
+    TRY(ctx->warm_lat.ensure((size_t)n * 64 * 4, "warm-start lattices"));
+    for (int i = 0; i < n; ++i) P.rvs[i].warm = ctx->warm_lat.as<float>() + 64 * i;
+    P.enc = enc;
+    P.enc_batch = n4_encoder_capacity(enc);
+    if (P.enc_batch < 1) return fail(N4_ERR_INVALID_ARG, "encoder has no batch capacity");
+  }
   P.pr = make_dev_params(p);
   for (const RunVol &r : rvs) P.dims.push_back(r.d);
   const std::vector<Dims> &dims = P.dims;
@@ -607,6 +650,7 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
   P.o_rep = take(sizeof(n4_report_t) * n);
   P.o_flg = take(4 * n);
   P.o_q = take(16);
+  P.o_pool = take(sizeof(PoolJob) * n);
   P.bytes = o;
   return N4_OK;
 }
@@ -633,6 +677,7 @@ void fill_descriptors(n4_context *ctx, const n4_params_t *p, Prepared &P, const 
     pst[i] = fit_total;
     fit_total += (long long)d.X * d.Y * d.Z;
     jb[i] = VolJob{d.X, d.Y, d.Z, il, nullptr, r.warm, r.lat, B.dp<n4_report_t>(P.o_rep) + i};
+    B.hp<PoolJob>(P.o_pool)[i] = PoolJob{il, d.X, d.Y, d.Z};
     char *tx = tabs + P.tab_off[i];
     char *ty = tx + align_up(axis_bytes(d.FX, P.NCX - 3), 256);
     char *tz = ty + align_up(axis_bytes(d.FY, P.NCY - 3), 256);
@@ -657,6 +702,15 @@ void fill_descriptors(n4_context *ctx, const n4_params_t *p, Prepared &P, const 
   for (size_t k = 0; k < order.size(); ++k) ord[k] = order[k];
 }
 
+// Network inputs of the warm start from the prologue's fitting grids.
+n4_status_t enqueue_pool(n4_context *ctx, const Prepared &P, const DescBuf &B, __nv_bfloat16 *d_x, cudaStream_t st) {
+  const long long cells = (long long)P.n * kPoolCells;
+  const int blocks = (int)std::min<long long>((cells + 255) / 256, (long long)ctx->nsm * 16);
+  k_pool_fitgrid<<<blocks, 256, 0, st>>>(B.dp<PoolJob>(P.o_pool), P.n, d_x);
+  CK(cudaGetLastError());
+  return N4_OK;
+}
+
 // The launches of a run (descriptors already on the device); capturable.
 n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P, const DescBuf &B, cudaStream_t st,
                         bool profile) {
@@ -679,6 +733,17 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
           CK(cudaGetLastError());
         }
       }
+    }
+  }
+  if (P.enc) {
+    // learned warm start: pooled fitting grids -> encoder -> first-level lattices
+    TRY(enqueue_pool(ctx, P, B, (__nv_bfloat16 *)ctx->warm_x.p, st));
+    ++launches;
+    for (int c0 = 0; c0 < n; c0 += P.enc_batch) {
+      const int nb = std::min(P.enc_batch, n - c0);
+      TRY(n4_encoder_predict(P.enc, (const __nv_bfloat16 *)ctx->warm_x.p + (size_t)c0 * kPoolCells, nb,
+                             ctx->warm_lat.as<float>() + 64 * c0, st));
+      launches += kEncoderLaunches;
     }
   }
   if (profile) TRY(prof_mark(ctx, 1, st));
@@ -725,9 +790,9 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
 
 // Core of n4_run / n4_run_batched: every pointer is a device pointer.
 n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector<RunVol> &rvs, cudaStream_t st,
-                        const Choice *forced) {
+                        const Choice *forced, n4_encoder_t *enc = nullptr) {
   Prepared P;
-  TRY(plan_run(ctx, p, rvs, forced, P));
+  TRY(plan_run(ctx, p, rvs, forced, P, enc));
   Upload u;
   TRY(acquire_slot(ctx, P.bytes, u));
   DescBuf B{u.slot->h, (char *)u.slot->d.p};
@@ -846,7 +911,8 @@ n4_status_t n4_destroy(n4_context_t *c) {
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
   for (DevBuf *b : {&c->imlog, &c->tables, &c->logu, &c->big, &c->red, &c->bar, &c->s1, &c->s2, &c->s3, &c->s4,
-                    &c->s5, &c->h_im, &c->h_mask, &c->h_out, &c->h_lat, &c->h_bias, &c->h_warm})
+                    &c->s5, &c->h_im, &c->h_mask, &c->h_out, &c->h_lat, &c->h_bias, &c->h_warm, &c->warm_x,
+                    &c->warm_lat})
     b->release();
   for (Slot &s : c->slots) {
     if (s.h) cudaFreeHost(s.h);
@@ -899,6 +965,165 @@ n4_status_t n4_run_batched(n4_context_t *ctx, const n4_params_t *p, int n, const
   }
   TRY(run_volumes(ctx, p, v, (cudaStream_t)stream, nullptr));
   if (reports) return collect(ctx, reports, n);
+  return N4_OK;
+}
+
+n4_status_t n4_run_batched_warm(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols,
+                                n4_encoder_t *enc, void *stream, n4_report_t *reports) {
+  if (!ctx || !vols || n < 1 || !enc) return fail(N4_ERR_INVALID_ARG, "bad batch");
+  TRY(check_params(p));
+  std::vector<RunVol> v(n);
+  for (int i = 0; i < n; ++i) {
+    const n4_volume_t &q = vols[i];
+    if (!q.im || !q.im_normalized || !q.lattice) return fail(N4_ERR_INVALID_ARG, "NULL pointer in batch");
+    TRY(make_dims(p, q.fx, q.fy, q.fz, v[i].d));
+    v[i].im = q.im;
+    v[i].mask = q.mask;
+    v[i].out = q.im_normalized;
+    v[i].lat = q.lattice;
+    v[i].bias = q.bias_field;
+    v[i].warm = q.warm_lattice;
+  }
+  TRY(run_volumes(ctx, p, v, (cudaStream_t)stream, nullptr, enc));
+  if (reports) return collect(ctx, reports, n);
+  return N4_OK;
+}
+
+n4_status_t n4_warm_inputs(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols, void *d_x,
+                           void *stream) {
+  if (!ctx || !vols || n < 1 || !d_x) return fail(N4_ERR_INVALID_ARG, "bad arguments");
+  TRY(check_params(p));
+  std::vector<RunVol> v(n);
+  for (int i = 0; i < n; ++i) {
+    const n4_volume_t &q = vols[i];
+    if (!q.im) return fail(N4_ERR_INVALID_ARG, "NULL image in batch");
+    TRY(make_dims(p, q.fx, q.fy, q.fz, v[i].d));
+    v[i].im = q.im;
+    v[i].mask = q.mask;
+  }
+  // the prologue and the pooling of a run, without the run
+  Prepared P;
+  const Choice grid_only{true, 0, 1024};
+  P.n = n;
+  P.rvs = v;
+  P.ch = grid_only;
+  for (const RunVol &r : v) P.dims.push_back(r.d);
+  P.NCX = P.NCY = P.NCZ = 4;
+  P.imlog_off.resize(n);
+  P.tab_off.assign(n, 0);
+  size_t imlog_bytes = 0;
+  for (int i = 0; i < n; ++i) {
+    P.imlog_off[i] = imlog_bytes;
+    imlog_bytes = align_up(imlog_bytes + (size_t)v[i].d.X * v[i].d.Y * v[i].d.Z * 4 + 64, 256);
+  }
+  TRY(ctx->imlog.ensure(imlog_bytes, "fitting grid"));
+  size_t o = 0;
+  auto take = [&](size_t b) { size_t r = o; o = align_up(o + b, 16); return r; };
+  P.o_pro = take(sizeof(PrologueVol) * n);
+  P.o_pst = take(8 * n);
+  P.o_flg = take(4 * n);
+  P.o_pool = take(sizeof(PoolJob) * n);
+  P.bytes = o;
+  Upload u;
+  TRY(acquire_slot(ctx, P.bytes, u));
+  DescBuf B{u.slot->h, (char *)u.slot->d.p};
+  long long fit_total = 0;
+  for (int i = 0; i < n; ++i) {
+    const Dims &d = v[i].d;
+    float *il = (float *)(ctx->imlog.as<char>() + P.imlog_off[i]);
+    B.hp<PrologueVol>(P.o_pro)[i] = PrologueVol{v[i].im, v[i].mask, nullptr, nullptr, d.FX, d.FY, d.FZ,
+                                                (int)p->ShrinkFactor, d.X, d.Y, d.Z, il, fit_total};
+    B.hp<long long>(P.o_pst)[i] = fit_total;
+    B.hp<PoolJob>(P.o_pool)[i] = PoolJob{il, d.X, d.Y, d.Z};
+    fit_total += (long long)d.X * d.Y * d.Z;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  TRY(begin_run(ctx, st));
+  CK(cudaMemcpyAsync(B.d, B.h, P.bytes, cudaMemcpyHostToDevice, st));
+  const int blocks = (int)std::min<long long>((fit_total + 255) / 256, (long long)ctx->nsm * 16);
+  k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(B.dp<PrologueVol>(P.o_pro), B.dp<long long>(P.o_pst), n,
+                                                   fit_total, p->low_value, B.dp<int>(P.o_flg));
+  CK(cudaGetLastError());
+  TRY(enqueue_pool(ctx, P, B, (__nv_bfloat16 *)d_x, st));
+  u.slot->nrep = 0;
+  return end_run(ctx, st, u);
+}
+
+n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols, void *stream,
+                        n4_tune_report_t *report) {
+  if (!ctx || !vols || n < 1) return fail(N4_ERR_INVALID_ARG, "bad batch");
+  TRY(check_params(p));
+  if (p->flags & (N4_FLAG_FORCE_GRID | N4_FLAG_FORCE_CLUSTER | N4_FLAG_CLUSTER_SIZE(31)))
+    return fail(N4_ERR_INVALID_ARG, "autotuning chooses the path itself: clear the FORCE and cluster-size flags");
+  std::vector<RunVol> v(n);
+  std::vector<Dims> dims(n);
+  for (int i = 0; i < n; ++i) {
+    const n4_volume_t &q = vols[i];
+    if (!q.im || !q.im_normalized || !q.lattice) return fail(N4_ERR_INVALID_ARG, "NULL pointer in batch");
+    TRY(make_dims(p, q.fx, q.fy, q.fz, v[i].d));
+    v[i].im = q.im;
+    v[i].mask = q.mask;
+    v[i].out = q.im_normalized;
+    v[i].lat = q.lattice;
+    v[i].bias = q.bias_field;
+    v[i].warm = q.warm_lattice;
+    dims[i] = v[i].d;
+  }
+  CK(cudaSetDevice(ctx->device));
+  // candidates: every cluster size whose per-CTA share of every volume fits,
+  // and the whole-GPU path for a single volume
+  std::vector<Choice> cand;
+  for (int K : {16, 12, 8, 6, 4, 2}) {
+    Plan pl = make_plan(p, K, dims, false);
+    if (!cluster_fits(ctx, pl)) continue;
+    int cap = 0;
+    TRY(capacity(ctx, 1024, K, pl.sm_bytes + pl.big_bytes, &cap));
+    if (cap > 0) cand.push_back(Choice{false, K, 1024});
+  }
+  if (n == 1) cand.push_back(Choice{true, 0, 1024});
+  if ((int)cand.size() > N4_TUNE_MAX) cand.resize(N4_TUNE_MAX);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int saved_prof = ctx->profiling;
+  ctx->profiling = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  n4_status_t status = N4_OK;
+  n4_tune_report_t rep{};
+  int best = -1;
+  float best_ms = 0.0f;
+  std::vector<n4_report_t> reps(n);
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    status = fail(N4_ERR_CUDA, "cudaEventCreate failed");
+  }
+  for (size_t c = 0; c < cand.size() && status == N4_OK; ++c) {
+    const Choice &ch = cand[c];
+    constexpr int kReps = 2;
+    n4_status_t s = run_volumes(ctx, p, v, st, &ch);   // untimed first run
+    if (s == N4_OK) s = collect(ctx, reps.data(), n);
+    if (s == N4_ERR_TOO_LARGE) continue;                // e.g. a grid the device cannot hold
+    if (s != N4_OK) { status = s; break; }
+    if (cudaEventRecord(e0, st) != cudaSuccess) { status = fail(N4_ERR_CUDA, "cudaEventRecord failed"); break; }
+    for (int r = 0; r < kReps && s == N4_OK; ++r) s = run_volumes(ctx, p, v, st, &ch);
+    if (s == N4_OK && cudaEventRecord(e1, st) != cudaSuccess) s = fail(N4_ERR_CUDA, "cudaEventRecord failed");
+    if (s == N4_OK) s = collect(ctx, reps.data(), n);
+    if (s != N4_OK) { status = s; break; }
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) { status = fail(N4_ERR_CUDA, "event timing failed"); break; }
+    ms /= kReps;
+    const int k = rep.candidates++;
+    rep.cluster_size[k] = ch.grid ? 0 : ch.K;
+    rep.ms[k] = ms;
+    if (best < 0 || ms < best_ms) { best = k; best_ms = ms; }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  ctx->profiling = saved_prof;
+  if (status != N4_OK) return status;
+  if (best < 0) return fail(N4_ERR_TOO_LARGE, "no execution path fits these volumes");
+  rep.chosen = best;
+  const int K = rep.cluster_size[best];
+  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, 1024};
+  if (report) *report = rep;
   return N4_OK;
 }
 
@@ -988,8 +1213,8 @@ static void graph_free(n4_batch_graph *g) {
 
 extern "C" {
 
-n4_status_t n4_batch_graph_create(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols,
-                                  n4_batch_graph_t **out) {
+static n4_status_t graph_create(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols,
+                                n4_encoder_t *enc, n4_batch_graph_t **out) {
   if (!ctx || !vols || n < 1 || !out) return fail(N4_ERR_INVALID_ARG, "bad arguments");
   *out = nullptr;
   TRY(check_params(p));
@@ -1005,7 +1230,7 @@ n4_status_t n4_batch_graph_create(n4_context_t *ctx, const n4_params_t *p, int n
   n4_batch_graph *g = new n4_batch_graph();
   g->ctx = ctx;
   g->params = *p;
-  n4_status_t s = plan_run(ctx, p, v, nullptr, g->P);
+  n4_status_t s = plan_run(ctx, p, v, nullptr, g->P, enc);
   if (s != N4_OK) { graph_free(g); return s; }
   const Prepared &P = g->P;
   g->rep_bytes = P.o_flg + 4 * (size_t)P.n - P.o_rep;
@@ -1046,6 +1271,17 @@ n4_status_t n4_batch_graph_create(n4_context_t *ctx, const n4_params_t *p, int n
   return N4_OK;
 }
 
+n4_status_t n4_batch_graph_create(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols,
+                                  n4_batch_graph_t **out) {
+  return graph_create(ctx, p, n, vols, nullptr, out);
+}
+
+n4_status_t n4_batch_graph_create_warm(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols,
+                                       n4_encoder_t *enc, n4_batch_graph_t **out) {
+  if (!enc) return fail(N4_ERR_INVALID_ARG, "encoder is NULL");
+  return graph_create(ctx, p, n, vols, enc, out);
+}
+
 n4_status_t n4_batch_graph_launch(n4_batch_graph_t *g, void *stream) {
   if (!g) return fail(N4_ERR_INVALID_ARG, "graph is NULL");
   CK(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
@@ -1084,6 +1320,19 @@ n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *g) {
 }
 
 // ---------------------------------------------------------------- components
+// z contraction of a standalone fit: the vectorised kernel when every row
+// starts on a 16-byte boundary, the scalar one otherwise (same arithmetic).
+static void launch_fit_rows(const float *field, const float *mask, long long rows, int Z, const Axis &az,
+                            float *t1n, float *t1d, cudaStream_t st) {
+  const bool v4 = Z % 4 == 0 && ((uintptr_t)field & 15u) == 0 && ((uintptr_t)mask & 15u) == 0;
+  if (v4)
+    k_fit_rows_v4<<<(unsigned)((rows + kFitRowsV - 1) / kFitRowsV), kFitRowsV, 0, st>>>(field, mask, rows, Z, az,
+                                                                                         t1n, t1d);
+  else
+    k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(field, mask, rows, Z, az, t1n,
+                                                                                   t1d);
+}
+
 static n4_status_t component_tables(n4_context_t *ctx, unsigned fx, unsigned fy, unsigned fz, unsigned nx, unsigned ny,
                                     unsigned nz, cudaStream_t st, Axis &ax, Axis &ay, Axis &az) {
   const size_t bx = align_up(axis_bytes(fx, nx - 3), 256), by = align_up(axis_bytes(fy, ny - 3), 256),
@@ -1123,8 +1372,7 @@ n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const floa
   const long long rows = (long long)fx * fy;
   const bool prof = ctx->profiling != 0;
   if (prof) TRY(prof_mark(ctx, 0, st));
-  k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(d_field, d_mask, rows, fz, az,
-                                                                                 t1n, t1d);
+  launch_fit_rows(d_field, d_mask, rows, fz, az, t1n, t1d, st);
   if (prof) TRY(prof_mark(ctx, 1, st));
   k_fit_planes<<<(int)std::min<size_t>((t2 + 255) / 256, gb), 256, 0, st>>>(t1n, t1d, fx, fy, ay, ncpt_z, t2n, t2d);
   if (prof) TRY(prof_mark(ctx, 2, st));
@@ -1300,8 +1548,7 @@ n4_status_t n4_fit_bspline3d_noalloc(const float *d_field, const float *d_mask, 
   float *t1n = (float *)(base + bx + by + bz), *t1d = t1n + t1;
   float *t2n = (float *)(base + bx + by + bz + align_up(t1 * 8, 256)), *t2d = t2n + t2;
   const long long rows = (long long)fx * fy;
-  k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(d_field, d_mask, rows, fz, az,
-                                                                                 t1n, t1d);
+  launch_fit_rows(d_field, d_mask, rows, fz, az, t1n, t1d, st);
   k_fit_planes<<<(int)std::min<size_t>((t2 + 255) / 256, 148 * 8), 256, 0, st>>>(t1n, t1d, fx, fy, ay, ncpt_z, t2n,
                                                                                    t2d);
   const int nlat = ncpt_x * ncpt_y * ncpt_z;

@@ -298,31 +298,6 @@ __global__ void k_to_bf16(const float *a, int n, bf16 *b) {
 // Adaptive average pool of a volume's masked log intensity to 32x32x24:
 // cell (i,j,k) covers [floor(i D/32), ceil((i+1) D/32)) per axis; the value
 // is the mean of log(im) over masked voxels with im > low (0 when none).
-__global__ void k_pool_input(const float *im, const float *mask, int FX, int FY, int FZ, float low, bf16 *out) {
-  const int cell = blockIdx.x;   // 32*32*24 cells
-  const int k = cell % kIn[2], j = (cell / kIn[2]) % kIn[1], i = cell / (kIn[2] * kIn[1]);
-  const int x0 = i * FX / kIn[0], x1 = ((i + 1) * FX + kIn[0] - 1) / kIn[0];
-  const int y0 = j * FY / kIn[1], y1 = ((j + 1) * FY + kIn[1] - 1) / kIn[1];
-  const int z0 = k * FZ / kIn[2], z1 = ((k + 1) * FZ + kIn[2] - 1) / kIn[2];
-  const int nx = x1 - x0, ny = y1 - y0, nz = z1 - z0;
-  float s = 0.0f, c = 0.0f;
-  for (int t = threadIdx.x; t < nx * ny * nz; t += blockDim.x) {
-    const int dz = t % nz, dy = (t / nz) % ny, dx = t / (nz * ny);
-    const size_t g = ((size_t)(x0 + dx) * FY + (y0 + dy)) * FZ + z0 + dz;
-    const float v = im[g];
-    if ((mask == nullptr || mask[g] != 0.0f) && v > low) { s += logf(v); c += 1.0f; }
-  }
-  for (int o = 16; o; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); c += __shfl_xor_sync(0xffffffffu, c, o); }
-  __shared__ float rs[32], rc[32];
-  if ((threadIdx.x & 31) == 0) { rs[threadIdx.x >> 5] = s; rc[threadIdx.x >> 5] = c; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float ts = 0.0f, tc = 0.0f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { ts += rs[w]; tc += rc[w]; }
-    out[cell] = __float2bfloat16(tc > 0.0f ? ts / tc : 0.0f);
-  }
-}
-
 // ------------------------------------------------------------------ host side
 template <class P>
 cudaError_t run_gemm(const P &p, int splits, cudaStream_t st) {
@@ -371,6 +346,9 @@ struct n4_encoder {
 
 // records the message returned by n4_last_error_string (n4_api.cu)
 n4_status_t n4_record_error(n4_status_t s, const char *msg);
+
+// largest batch one n4_encoder_predict call takes (used by n4_api.cu)
+int n4_encoder_capacity(const n4_encoder_t *enc) { return enc ? enc->max_batch : 0; }
 
 namespace {
 n4_status_t efail(n4_status_t s, const std::string &m) { return n4_record_error(s, m.c_str()); }
@@ -542,14 +520,4 @@ n4_status_t n4_encoder_train_step(n4_encoder_t *e, const void *d_x, const float 
 }
 
 // Network input for one volume: [32][32][24] BF16 written to d_x.
-n4_status_t n4_encoder_pool_input(const float *d_im, const float *d_mask, unsigned fx, unsigned fy, unsigned fz,
-                                  float low_value, void *d_x, void *stream) {
-  if (!d_im || !d_x || fx < (unsigned)kIn[0] || fy < (unsigned)kIn[1] || fz < (unsigned)kIn[2])
-    return efail(N4_ERR_INVALID_ARG, "volume smaller than the 32x32x24 network input");
-  k_pool_input<<<kIn[0] * kIn[1] * kIn[2], 128, 0, (cudaStream_t)stream>>>(d_im, d_mask, fx, fy, fz, low_value,
-                                                                             (bf16 *)d_x);
-  ECK(cudaGetLastError());
-  return N4_OK;
-}
-
 }  // extern "C"

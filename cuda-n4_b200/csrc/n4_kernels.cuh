@@ -14,6 +14,8 @@
 //   k_minmax/k_hist/k_sharpen/k_remap   standalone sharpenImage
 //   k_cv              standalone convergence measurement
 #pragma once
+#include <cuda_bf16.h>
+
 #include "n4_engine.cuh"
 
 namespace n4 {
@@ -74,6 +76,42 @@ __global__ void k_threshold_inplace(float *im, float *mask, long long n, float l
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     if (!(im[i] > low)) { im[i] = 0.0f; if (mask) mask[i] = 0.0f; }
+  }
+}
+
+// ------------------------------------------------------------------ warm-start input
+// Input of the learned warm start: each volume's masked log fitting grid
+// (the prologue's output, NaN outside the mask) averaged over 32x32x24
+// adaptive cells [i*X/32, ceil((i+1)*X/32)) per axis, stored as BF16
+// [volume][32][32][24].  A cell without a masked voxel is 0.
+constexpr int kPoolX = 32, kPoolY = 32, kPoolZ = 24;
+constexpr int kPoolCells = kPoolX * kPoolY * kPoolZ;
+
+struct PoolJob {
+  const float *imlog;
+  int X, Y, Z;
+};
+
+__global__ void k_pool_fitgrid(const PoolJob *jobs, int nvol, __nv_bfloat16 *out) {
+  const long long total = (long long)nvol * kPoolCells;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int v = (int)(t / kPoolCells), cell = (int)(t - (long long)v * kPoolCells);
+    const PoolJob J = jobs[v];
+    const int k = cell % kPoolZ, j = (cell / kPoolZ) % kPoolY, i = cell / (kPoolZ * kPoolY);
+    const int x0 = i * J.X / kPoolX, x1 = ((i + 1) * J.X + kPoolX - 1) / kPoolX;
+    const int y0 = j * J.Y / kPoolY, y1 = ((j + 1) * J.Y + kPoolY - 1) / kPoolY;
+    const int z0 = k * J.Z / kPoolZ, z1 = ((k + 1) * J.Z + kPoolZ - 1) / kPoolZ;
+    float s = 0.0f, c = 0.0f;
+    for (int x = x0; x < x1; ++x)
+      for (int y = y0; y < y1; ++y) {
+        const float *row = J.imlog + ((long long)x * J.Y + y) * J.Z;
+        for (int z = z0; z < z1; ++z) {
+          const float val = row[z];
+          if (!isnan(val)) { s += val; c += 1.0f; }
+        }
+      }
+    out[t] = __float2bfloat16(c > 0.0f ? s / c : 0.0f);
   }
 }
 
@@ -253,7 +291,9 @@ constexpr int kMaxNcz = 64;
 // One CTA per tile of kRowsPerTile full-resolution rows: x/y-contract the
 // lattice for its rows into shared memory, then evaluate z per voxel with
 // float4 I/O.  HBM traffic: read im, write out (+ bias).
-__global__ void __launch_bounds__(256) k_correct(const CorrectVol *vols, const long long *tile_starts,
+constexpr int kCorrectPre = 6;   // input float4 loads a thread keeps in flight
+
+__global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, const long long *tile_starts,
                                                  int nvol, float low) {
   __shared__ float Gs[kRowsPerTile * kMaxNcz];
   const int v = find_volume(tile_starts, nvol, blockIdx.x);
@@ -263,6 +303,26 @@ __global__ void __launch_bounds__(256) k_correct(const CorrectVol *vols, const l
   const long long row0 = (blockIdx.x - C.tile0) * (long long)kRowsPerTile;
   const int nr = (int)min((long long)kRowsPerTile, rows - row0);
   const int ncz = C.ncz, ncy = C.ncy;
+  const int FZ = C.FZ;
+  const long long base = row0 * FZ;
+  // float4 path: each thread owns 4 consecutive z (weights in registers) and
+  // rows r_first, r_first + rpp, ...; its first kCorrectPre input float4s
+  // are requested before the lattice contraction, so the HBM latency of the
+  // tile overlaps the contraction's L1/L2 gathers
+  const bool vec = C.vec4 != 0;
+  const int nz4 = vec ? FZ >> 2 : 1;
+  const int rpp = vec ? (int)blockDim.x / nz4 : 0;          // rows per pass (nz4 <= 256)
+  const bool act = vec && (int)threadIdx.x < rpp * nz4;
+  const int z = act ? ((int)threadIdx.x % nz4) * 4 : 0;
+  const int r_first = act ? (int)threadIdx.x / nz4 : 0;
+  float4 xin[kCorrectPre];
+  if (act && C.im) {
+#pragma unroll
+    for (int k = 0; k < kCorrectPre; ++k) {
+      const int r = r_first + k * rpp;
+      xin[k] = r < nr ? __ldcs((const float4 *)(C.im + base + (long long)r * FZ + z)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
   for (int t = threadIdx.x; t < nr * ncz; t += blockDim.x) {
     const int r = t / ncz, cz = t - r * ncz;
     const long long row = row0 + r;
@@ -282,32 +342,36 @@ __global__ void __launch_bounds__(256) k_correct(const CorrectVol *vols, const l
     Gs[t] = acc;
   }
   __syncthreads();
-  const int FZ = C.FZ;
-  const long long base = row0 * FZ;
-  if (C.vec4) {
-    // each thread owns 4 consecutive z (weights in registers) and walks rows;
-    // exp/divide use the fast intrinsics (a few ulp)
-    const int nz4 = FZ >> 2;
-    const int rpp = blockDim.x / nz4;            // rows per pass (nz4 <= 256)
-    if ((int)threadIdx.x < rpp * nz4) {
-      const int z = (threadIdx.x % nz4) * 4;
-      const int r_first = threadIdx.x / nz4;
-      int sz[4];
-      float4 wz[4];
+  if (vec) {
+    if (!act) return;
+    int sz[4];
+    float4 wz[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) { sz[k] = az.s[z + k]; wz[k] = az.w[z + k]; }
-      for (int r = r_first; r < nr; r += rpp) {
+    for (int k = 0; k < 4; ++k) { sz[k] = az.s[z + k]; wz[k] = az.w[z + k]; }
+    for (int rb = r_first; rb < nr; rb += kCorrectPre * rpp) {
+      if (rb != r_first && C.im) {
+#pragma unroll
+        for (int k = 0; k < kCorrectPre; ++k) {
+          const int r = rb + k * rpp;
+          xin[k] = r < nr ? __ldcs((const float4 *)(C.im + base + (long long)r * FZ + z))
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kCorrectPre; ++k) {
+        const int r = rb + k * rpp;
+        if (r >= nr) break;
         const float *g = Gs + r * ncz;
         float bz[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) bz[k] = dot4(wz[k], g + sz[k]);
+        for (int q = 0; q < 4; ++q) bz[q] = dot4(wz[q], g + sz[q]);
         const long long off = base + (long long)r * FZ + z;
         if (C.im) {
-          const float4 x = __ldcs((const float4 *)(C.im + off));
-          const float xa[4] = {x.x, x.y, x.z, x.w};
+          // exp/divide use the fast intrinsics (a few ulp)
+          const float xa[4] = {xin[k].x, xin[k].y, xin[k].z, xin[k].w};
           float o[4], e[4];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) { e[k] = __expf(bz[k]); o[k] = xa[k] > low ? __fdividef(xa[k], e[k]) : 0.0f; }
+          for (int q = 0; q < 4; ++q) { e[q] = __expf(bz[q]); o[q] = xa[q] > low ? __fdividef(xa[q], e[q]) : 0.0f; }
           __stcs((float4 *)(C.out + off), make_float4(o[0], o[1], o[2], o[3]));
           if (C.bias) __stcs((float4 *)(C.bias + off), make_float4(e[0], e[1], e[2], e[3]));
         } else {
@@ -317,9 +381,9 @@ __global__ void __launch_bounds__(256) k_correct(const CorrectVol *vols, const l
     }
   } else {
     for (int t = threadIdx.x; t < nr * FZ; t += blockDim.x) {
-      const int r = t / FZ, z = t - r * FZ;
-      const long long off = base + (long long)r * FZ + z;
-      const float b = dot4(az.w[z], Gs + r * ncz + az.s[z]);
+      const int r = t / FZ, zz = t - r * FZ;
+      const long long off = base + (long long)r * FZ + zz;
+      const float b = dot4(az.w[zz], Gs + r * ncz + az.s[zz]);
       if (C.im) {
         const float x = C.im[off];
         const float e = __expf(b);
@@ -390,6 +454,93 @@ __global__ void __launch_bounds__(kFitRows) k_fit_rows(const float *field, const
       const int k = c - cur;
       t1n[my * ncz + c] = k < 4 ? nn[k] : 0.0f;
       t1d[my * ncz + c] = k < 4 ? dd[k] : 0.0f;
+    }
+  }
+}
+
+// The same contraction for Z % 4 == 0 and 16-byte aligned field and mask,
+// built for HBM bandwidth: 64 rows per CTA (every CTA of a 256x256-row field
+// resident at once), coalesced float4 streaming loads of the next 32-voxel
+// chunk issued into registers before the current chunk is walked from
+// shared memory, and a shared row stride of 36 floats so that the per-row
+// float4 reads of a quarter warp fall in 8 distinct 16-byte bank groups.
+// The per-voxel arithmetic and its order are those of k_fit_rows.
+constexpr int kFitRowsV = 64;
+constexpr int kFitChunkV = 32;
+constexpr int kFitStrideV = kFitChunkV + 4;
+constexpr int kFitLoadsV = kFitChunkV / 4;   // float4 per thread (one row each) per array and chunk
+
+__global__ void __launch_bounds__(kFitRowsV, 8) k_fit_rows_v4(const float *field, const float *mask, long long rows,
+                                                           int Z, Axis az, float *t1n, float *t1d) {
+  __shared__ __align__(16) float fs[kFitRowsV * kFitStrideV];
+  __shared__ __align__(16) float ms[kFitRowsV * kFitStrideV];
+  const long long row0 = (long long)blockIdx.x * kFitRowsV;
+  const int nr = (int)min((long long)kFitRowsV, rows - row0);
+  const int t = threadIdx.x;
+  const int ncz = az.nc;
+  float4 pf[kFitLoadsV], pm[kFitLoadsV];
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f), one4 = make_float4(1.f, 1.f, 1.f, 1.f);
+  auto load = [&](int z0) {
+#pragma unroll
+    for (int k = 0; k < kFitLoadsV; ++k) {
+      const int i = t + k * kFitRowsV;         // float4 index in the [rows][8] chunk
+      const int r = i >> 3, z = z0 + 4 * (i & 7);
+      pf[k] = zero4;
+      pm[k] = zero4;
+      if (r < nr && z < Z) {
+        const long long g = (row0 + r) * Z + z;
+        pf[k] = __ldcs((const float4 *)(field + g));
+        pm[k] = mask ? __ldcs((const float4 *)(mask + g)) : one4;
+      }
+    }
+  };
+  float n0 = 0.f, n1 = 0.f, n2 = 0.f, n3 = 0.f, d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
+  int cur = 0;
+  load(0);
+  for (int z0 = 0; z0 < Z; z0 += kFitChunkV) {
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kFitLoadsV; ++k) {
+      const int i = t + k * kFitRowsV;
+      const int o = (i >> 3) * kFitStrideV + 4 * (i & 7);
+      *(float4 *)(fs + o) = pf[k];
+      *(float4 *)(ms + o) = pm[k];
+    }
+    __syncthreads();
+    if (z0 + kFitChunkV < Z) load(z0 + kFitChunkV);
+    if (t < nr) {
+      const int nq = min(kFitChunkV, Z - z0) >> 2;
+      for (int q = 0; q < nq; ++q) {
+        const float4 f4 = *(const float4 *)(fs + t * kFitStrideV + 4 * q);
+        const float4 m4 = *(const float4 *)(ms + t * kFitStrideV + 4 * q);
+        const float fa[4] = {f4.x, f4.y, f4.z, f4.w}, ma[4] = {m4.x, m4.y, m4.z, m4.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int vz = z0 + 4 * q + k;
+          const int sp = az.s[vz];
+          while (cur < sp) {
+            t1n[(row0 + t) * ncz + cur] = n0;
+            t1d[(row0 + t) * ncz + cur] = d0;
+            n0 = n1; n1 = n2; n2 = n3; n3 = 0.f;
+            d0 = d1; d1 = d2; d2 = d3; d3 = 0.f;
+            ++cur;
+          }
+          if (ma[k] == 0.0f) continue;
+          const float f = fa[k];
+          const float4 p = az.p4[vz], w = az.q4[vz];
+          n0 = __fmaf_rn(p.x, f, n0); n1 = __fmaf_rn(p.y, f, n1);
+          n2 = __fmaf_rn(p.z, f, n2); n3 = __fmaf_rn(p.w, f, n3);
+          d0 += w.x; d1 += w.y; d2 += w.z; d3 += w.w;
+        }
+      }
+    }
+  }
+  if (t < nr) {
+    const float nn[4] = {n0, n1, n2, n3}, dd[4] = {d0, d1, d2, d3};
+    for (int c = cur; c < ncz; ++c) {
+      const int k = c - cur;
+      t1n[(row0 + t) * ncz + c] = k < 4 ? nn[k] : 0.0f;
+      t1d[(row0 + t) * ncz + c] = k < 4 ? dd[k] : 0.0f;
     }
   }
 }

@@ -39,7 +39,7 @@ __all__ = [
     "N4Param", "N4", "N4Batch", "N4BatchGraph", "N4Result", "Context", "FitBspline3D",
     "EvaluateBspline3D", "UpsampleLattice3D", "upsampleLattice3D", "sharpenImage",
     "CalculateConvergenceMeasurement", "calculateConvergenceMeasurement", "N4Error",
-    "lattice_dims", "library",
+    "lattice_dims", "library", "autotune", "cluster_size_flag", "warm_inputs",
 ]
 
 
@@ -264,10 +264,11 @@ def N4(im, mask=None, param: Optional[N4Param] = None, warm_lattice=None, return
 
 
 def N4Batch(volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=None, return_bias=False,
-            ctx: Optional[Context] = None, synchronous: bool = True):
+            ctx: Optional[Context] = None, synchronous: bool = True, encoder=None):
     """Bias-correct many volumes (CUDA tensors, any sizes) in one persistent
-    launch.  ``volumes``: sequence of ``(im, mask)``.  Returns a list of
-    ``N4Result``."""
+    launch.  ``volumes``: sequence of ``(im, mask)``.  With ``encoder`` (an
+    ``n4b200.encoder.Encoder``) the first-level lattices are predicted inside
+    the run (``n4_run_batched_warm``).  Returns a list of ``N4Result``."""
     torch = _torch()
     param = param or N4Param()
     cpar = param.to_c()
@@ -290,12 +291,75 @@ def N4Batch(volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=No
         results.append(N4Result(out, lat, bias, {}))
     reps = (n4_report_t * n)()
     c = ctx or Context.default(dev.index or 0)
-    st = _lib.load().n4_run_batched(c.handle, C.byref(cpar), n, arr, _stream(dev), reps if synchronous else None)
+    if encoder is not None:
+        st = _lib.load().n4_run_batched_warm(c.handle, C.byref(cpar), n, arr, encoder.h, _stream(dev),
+                                             reps if synchronous else None)
+    else:
+        st = _lib.load().n4_run_batched(c.handle, C.byref(cpar), n, arr, _stream(dev), reps if synchronous else None)
     check(st)
     if synchronous:
         for r, rep in zip(results, reps):
             r.report = _report_dict(rep)
     return results
+
+
+def warm_inputs(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[Context] = None):
+    """Network inputs of the learned warm start (``n4_warm_inputs``): every
+    volume's masked log fitting grid pooled to 32x32x24, CUDA BF16
+    ``[n, 32, 32, 24]``."""
+    torch = _torch()
+    param = param or N4Param()
+    cpar = param.to_c()
+    n = len(volumes)
+    arr = (n4_volume_t * n)()
+    keep = []
+    dev = None
+    for i, (im, mask) in enumerate(volumes):
+        imt = _dev_f32(im)
+        dev = imt.device
+        mk = None if mask is None else _dev_f32(mask, dev)
+        keep += [imt, mk]
+        fx, fy, fz = (int(d) for d in imt.shape)
+        arr[i] = n4_volume_t(_ptr(imt), _ptr(mk), fx, fy, fz, None, None, None, None)
+    x = torch.empty((n, 32, 32, 24), dtype=torch.bfloat16, device=dev)
+    c = ctx or Context.default(dev.index or 0)
+    check(_lib.load().n4_warm_inputs(c.handle, C.byref(cpar), n, arr, x.data_ptr(), _stream(dev)))
+    return x
+
+
+def cluster_size_flag(k: int) -> int:
+    """``N4_FLAG_CLUSTER_SIZE(k)``: run the cluster path with k CTAs per volume."""
+    return (int(k) & 31) << 8
+
+
+def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[Context] = None) -> dict:
+    """Time every execution configuration that fits these volumes
+    (``n4_autotune``) and record the fastest in the context for later runs
+    of volumes of the same sizes with the same lattice, levels and bins.
+    Returns ``{"candidates": [(cluster_size, ms), ...], "chosen": cluster_size}``
+    (cluster size 0 = whole-GPU path)."""
+    torch = _torch()
+    param = param or N4Param()
+    cpar = param.to_c()
+    dims = lattice_dims(param)
+    n = len(volumes)
+    arr = (n4_volume_t * n)()
+    keep = []
+    dev = None
+    for i, (im, mask) in enumerate(volumes):
+        imt = _dev_f32(im)
+        dev = imt.device
+        mk = None if mask is None else _dev_f32(mask, dev)
+        out = torch.empty_like(imt)
+        lat = torch.empty(dims, dtype=torch.float32, device=dev)
+        keep += [imt, mk, out, lat]
+        fx, fy, fz = (int(d) for d in imt.shape)
+        arr[i] = n4_volume_t(_ptr(imt), _ptr(mk), fx, fy, fz, _ptr(out), _ptr(lat), None, None)
+    c = ctx or Context.default(dev.index or 0)
+    rep = _lib.n4_tune_report_t()
+    check(_lib.load().n4_autotune(c.handle, C.byref(cpar), n, arr, _stream(dev), C.byref(rep)))
+    cands = [(int(rep.cluster_size[k]), float(rep.ms[k])) for k in range(rep.candidates)]
+    return {"candidates": cands, "chosen": cands[rep.chosen][0]}
 
 
 class N4BatchGraph:
@@ -305,7 +369,7 @@ class N4BatchGraph:
     outputs are written to ``results[i].im_normalized`` etc."""
 
     def __init__(self, volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=None,
-                 return_bias=False, ctx: Optional[Context] = None):
+                 return_bias=False, ctx: Optional[Context] = None, encoder=None):
         torch = _torch()
         param = param or N4Param()
         self._cpar = param.to_c()
@@ -330,7 +394,13 @@ class N4BatchGraph:
         self.ctx = ctx or Context.default(dev.index or 0)
         self.device = dev
         self._h = C.c_void_p()
-        check(_lib.load().n4_batch_graph_create(self.ctx.handle, C.byref(self._cpar), n, arr, C.byref(self._h)))
+        self.encoder = encoder
+        if encoder is not None:
+            check(_lib.load().n4_batch_graph_create_warm(self.ctx.handle, C.byref(self._cpar), n, arr, encoder.h,
+                                                         C.byref(self._h)))
+        else:
+            check(_lib.load().n4_batch_graph_create(self.ctx.handle, C.byref(self._cpar), n, arr,
+                                                    C.byref(self._h)))
 
     def launch(self):
         check(_lib.load().n4_batch_graph_launch(self._h, _stream(self.device)))

@@ -67,6 +67,16 @@ class n4_volume_t(C.Structure):
     ]
 
 
+N4_TUNE_MAX = 8
+
+
+class n4_tune_report_t(C.Structure):
+    _fields_ = [
+        ("candidates", C.c_int), ("cluster_size", C.c_int * N4_TUNE_MAX), ("ms", C.c_float * N4_TUNE_MAX),
+        ("chosen", C.c_int),
+    ]
+
+
 class n4_timings_t(C.Structure):
     _fields_ = [
         ("stage_ms", C.c_float * 4), ("launches", C.c_int), ("fit_voxels", C.c_longlong),
@@ -101,6 +111,10 @@ SIGNATURES = [
     ("n4_batch_graph_destroy", C.c_int, [_P]),
     ("n4_set_profiling", C.c_int, [_P, C.c_int]),
     ("n4_last_timings", C.c_int, [_P, C.POINTER(n4_timings_t)]),
+    ("n4_autotune", C.c_int, [_P, _P, C.c_int, _P, _P, _P]),
+    ("n4_warm_inputs", C.c_int, [_P, _P, C.c_int, _P, _P, _P]),
+    ("n4_run_batched_warm", C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P]),
+    ("n4_batch_graph_create_warm", C.c_int, [_P, _P, C.c_int, _P, _P, _P]),
     ("n4_fit_bspline3d", C.c_int, [_P, _P, _P, _U, _U, _U, _U, _U, _U, C.c_float, C.c_int, _P, _P]),
     ("n4_fit_bspline3d_noalloc", C.c_int, [_P, _P, _U, _U, _U, _U, _U, _U, C.c_float, C.c_int, _P, _P]),
     ("n4_evaluate_bspline3d", C.c_int, [_P, _P, _U, _U, _U, _U, _U, _U, _P, _P]),
@@ -115,7 +129,6 @@ SIGNATURES = [
     ("n4_encoder_get_params", C.c_int, [_P, _P, _P, C.c_size_t]),
     ("n4_encoder_predict", C.c_int, [_P, _P, C.c_int, _P, _P]),
     ("n4_encoder_train_step", C.c_int, [_P, _P, _P, C.c_int, C.c_float, C.POINTER(C.c_float), _P]),
-    ("n4_encoder_pool_input", C.c_int, [_P, _P, _U, _U, _U, C.c_float, _P, _P]),
 ]
 
 _lib = None

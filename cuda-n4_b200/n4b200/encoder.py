@@ -1,12 +1,13 @@
 """Learned warm start for N4: training data, training loop and inference.
 
 The encoder (``n4_encoder_*`` in ``include/n4b200.h``) maps the masked log
-volume, average-pooled to 32x32x24, to the first-level 4x4x4 log-bias
-lattice.  Training pairs come from the plain GPU N4 itself: for every seeded
+fitting grid, average-pooled to 32x32x24 (``n4b200.warm_inputs``), to the
+first-level 4x4x4 log-bias lattice.  Training pairs come from the plain GPU N4 itself: for every seeded
 phantom the label is the lattice of a one-level N4 run to convergence at the
-run's shrink factor.  Its prediction is passed to ``N4``/``N4Batch`` as the
-warm lattice; N4 still iterates to the same threshold and discards a warm
-start whose first-iteration convergence value exceeds the zero-lattice one.
+run's shrink factor.  ``N4Batch(..., encoder=enc)`` and
+``N4BatchGraph(..., encoder=enc)`` pool, predict and warm-start inside the
+run; N4 still iterates to the same threshold and discards a warm start whose
+first-iteration convergence value exceeds the zero-lattice one.
 
 All network arithmetic runs in ``libn4b200.so`` (BF16 tensor-core kernels);
 this module only orchestrates.
@@ -116,19 +117,6 @@ class Encoder:
                                              C.byref(loss) if want_loss else None,
                                              torch.cuda.current_stream(x.device).cuda_stream))
         return loss.value if want_loss else float("nan")
-
-
-def pool_input(im, mask, low_value: float = 0.0, out=None):
-    """Network input [32, 32, 24] (CUDA bf16) of one CUDA float volume."""
-    import torch
-    lib = _decl()
-    fx, fy, fz = (int(d) for d in im.shape)
-    if out is None:
-        out = torch.empty(IN_SHAPE, dtype=torch.bfloat16, device=im.device)
-    check(lib.n4_encoder_pool_input(im.data_ptr(), None if mask is None else mask.data_ptr(), fx, fy, fz,
-                                    float(low_value), out.data_ptr(),
-                                    torch.cuda.current_stream(im.device).cuda_stream))
-    return out
 
 
 @dataclass

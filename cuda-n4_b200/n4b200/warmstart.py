@@ -4,15 +4,15 @@
   ``phantom.make_phantom``: nested jittered ellipsoids, exp of a cubic
   B-spline bias, Rician noise; torch's generator instead of numpy's, so the
   volumes differ from the numpy ones with the same seed).
-* ``make_dataset`` — network inputs and labels: the label of a phantom is the
+* ``make_dataset`` — network inputs and labels: the input of a phantom is its
+  masked log fitting grid pooled to 32x32x24 (``n4b200.warm_inputs``, the
+  same pooling a warm-started run does internally); its label is the
   first-level 4x4x4 lattice of the plain GPU N4 run to convergence with one
   fitting level at the run's shrink factor.
 * ``train_encoder`` — Adam on MSE with the tensor-core encoder.
 * ``evaluate`` — held-out phantoms corrected batched with and without the
-  predicted warm lattices: iterations, volumes/s, warm starts kept, and the
-  largest log-bias difference between the two runs.
-* ``WarmBatch`` — pool + predict + batched N4 with the predictions as warm
-  lattices (the batch itself recorded as a CUDA graph).
+  learned warm start (``N4Batch(..., encoder=...)``): iterations,
+  volumes/s, warm starts kept, and the log-bias difference between the runs.
 
 Command line (GPU)::
 
@@ -25,8 +25,8 @@ import numpy as np
 
 import os
 
-from . import EvaluateBspline3D, N4Batch, N4BatchGraph, N4Param
-from .encoder import Encoder, pool_input, train
+from . import EvaluateBspline3D, N4Batch, N4Param, warm_inputs
+from .encoder import Encoder, train
 from .phantom import _axis_weights
 
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "warmstart_encoder.npy")
@@ -74,16 +74,6 @@ def eval_param(shrink=4, levels=4):
                    low_value=0.0, ShrinkFactor=shrink)
 
 
-def predict_warm(enc: Encoder, volumes, low_value=0.0):
-    """First-level lattices [n, 4, 4, 4] predicted for (im, mask) pairs."""
-    import torch
-    n = len(volumes)
-    x = torch.empty((n, 32, 32, 24), dtype=torch.bfloat16, device=volumes[0][0].device)
-    for i, (im, mask) in enumerate(volumes):
-        pool_input(im, mask, low_value, out=x[i])
-    return enc.predict(x)
-
-
 def make_dataset(n, shape, seed, shrink=4, chunk=256, **gen):
     """(x [n,32,32,24] bf16, y [n,4,4,4] float) on the GPU."""
     import torch
@@ -91,13 +81,11 @@ def make_dataset(n, shape, seed, shrink=4, chunk=256, **gen):
     for c0 in range(0, n, chunk):
         m = min(chunk, n - c0)
         im, mask = phantoms_gpu(m, shape, seed + c0, **gen)
-        res = N4Batch([(im[i], mask[i]) for i in range(m)], label_param(shrink))
+        vols = [(im[i], mask[i]) for i in range(m)]
+        res = N4Batch(vols, label_param(shrink))
         ys.append(torch.stack([r.lattice for r in res]))
-        x = torch.empty((m, 32, 32, 24), dtype=torch.bfloat16, device=im.device)
-        for i in range(m):
-            pool_input(im[i], mask[i], 0.0, out=x[i])
-        xs.append(x)
-        del im, mask, res
+        xs.append(warm_inputs(vols, label_param(shrink)))
+        del im, mask, res, vols
     return torch.cat(xs), torch.cat(ys)
 
 
@@ -124,7 +112,7 @@ def train_encoder(n_train=4096, n_val=256, shape=(128, 128, 96), epochs=20, batc
 def evaluate(enc: Encoder, n_eval=256, shape=(256, 256, 176), seed=5_000_000, chunk=32, param=None, **gen):
     """Held-out phantoms corrected batched from zero and from the predicted
     lattices.  Returns mean iterations of both runs, device-timed volumes/s
-    of both batched runs (pooling and prediction included in the warm one),
+    of both batched runs (pooling and prediction run inside the warm one),
     the share of warm starts kept, and the log-bias difference d between the
     two runs at full resolution: max |d| over the mask, max |d - mean_mask(d)|
     over the mask (a constant log bias is a global intensity scale, which the
@@ -144,19 +132,20 @@ def evaluate(enc: Encoder, n_eval=256, shape=(256, 256, 176), seed=5_000_000, ch
         vols = [(im[i], mask[i]) for i in range(m)]
         N4Batch(vols, param)                       # warm the context's workspaces
         torch.cuda.synchronize()
+        N4Batch(vols, param, encoder=enc)
+        torch.cuda.synchronize()
         ev[0].record()
         plain = N4Batch(vols, param, synchronous=False)
         ev[1].record()
         ev[2].record()
-        warm_lat = predict_warm(enc, vols)
-        warm = N4Batch(vols, param, warm_lattices=[warm_lat[i] for i in range(m)], synchronous=False)
+        warm = N4Batch(vols, param, encoder=enc, synchronous=False)
         ev[3].record()
         torch.cuda.synchronize()
         ms_plain += ev[0].elapsed_time(ev[1])
         ms_warm += ev[2].elapsed_time(ev[3])
         # reports (synchronous reruns are bitwise identical: the engine is deterministic)
         plain = N4Batch(vols, param)
-        warm = N4Batch(vols, param, warm_lattices=[warm_lat[i] for i in range(m)])
+        warm = N4Batch(vols, param, encoder=enc)
         for i, (a, b) in enumerate(zip(plain, warm)):
             it_plain.append(sum(a.report["iterations"][:a.report["levels"]]))
             it_warm.append(sum(b.report["iterations"][:b.report["levels"]]))
@@ -185,32 +174,6 @@ def evaluate(enc: Encoder, n_eval=256, shape=(256, 256, 176), seed=5_000_000, ch
 
 def load_encoder(path=WEIGHTS, max_batch=64) -> Encoder:
     return Encoder(max_batch=max_batch, params=np.load(path))
-
-
-class WarmBatch:
-    """Warm-started batched N4 over fixed device buffers: every ``run()``
-    pools the inputs, predicts first-level lattices with the encoder and
-    launches the recorded batch graph with them as warm lattices."""
-
-    def __init__(self, enc: Encoder, volumes, param, ctx=None, low_value=0.0):
-        import torch
-        self.enc = enc
-        self.volumes = volumes
-        self.low = low_value
-        dev = volumes[0][0].device
-        n = len(volumes)
-        self.x = torch.empty((n, 32, 32, 24), dtype=torch.bfloat16, device=dev)
-        self.warm = torch.zeros((n, 4, 4, 4), dtype=torch.float32, device=dev)
-        self.graph = N4BatchGraph(volumes, param, warm_lattices=[self.warm[i] for i in range(n)], ctx=ctx)
-
-    def run(self):
-        for i, (im, mask) in enumerate(self.graph.inputs):
-            pool_input(im, mask, self.low, out=self.x[i])
-        self.warm.copy_(self.enc.predict(self.x))
-        self.graph.launch()
-
-    def sync(self):
-        return self.graph.sync()
 
 
 def main(argv=None):

@@ -44,6 +44,10 @@ typedef enum {
                                       /* caller's buffers, as the reference does (cudaN4.cu:1459) */
 #define N4_FLAG_FORCE_GRID      0x8u  /* run the whole-GPU path even when a cluster path fits      */
 #define N4_FLAG_FORCE_CLUSTER   0x10u /* fail with N4_ERR_TOO_LARGE rather than use the grid path */
+/* Bits 8-12: run the cluster path with exactly k CTAs per volume (1..16),
+ * overriding the autotuner; N4_ERR_TOO_LARGE when a volume's share does not
+ * fit one CTA's shared memory.  0 = choose automatically. */
+#define N4_FLAG_CLUSTER_SIZE(k) (((unsigned int)(k) & 31u) << 8)
 
 /* Mirrors N4Param (cudaN4.h:24-94).  Obtain defaults from n4_params_default. */
 typedef struct {
@@ -137,8 +141,10 @@ n4_status_t n4_sync(n4_context_t *ctx, n4_report_t *reports, int n);
 /* A batched run recorded once as a CUDA graph (no counterpart in the
  * reference).  Every launch repeats the run on the same buffers (the
  * caller may refill the inputs in between) without host-side planning.
- * The graph uses the context's workspaces: do not run other work on the
- * context while a launch is in flight. */
+ * The graph uses the context's workspaces as sized at its creation: do not
+ * run other work on the context while a launch is in flight, and give each
+ * graph a context of its own (a later run that needs larger workspaces
+ * reallocates them under the graph). */
 typedef struct n4_batch_graph n4_batch_graph_t;
 n4_status_t n4_batch_graph_create(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols,
                                   n4_batch_graph_t **graph);
@@ -146,6 +152,27 @@ n4_status_t n4_batch_graph_launch(n4_batch_graph_t *graph, void *stream);
 /* Wait for the last launch and fill its reports (n entries, may be NULL). */
 n4_status_t n4_batch_graph_sync(n4_batch_graph_t *graph, n4_report_t *reports, int n);
 n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *graph);
+
+/* ---- autotuning (no counterpart in the reference) ----
+ * n4_autotune runs the given volumes once per execution configuration that
+ * fits them: thread-block clusters of 16, 12, 8, 6, 4 and 2 CTAs per volume
+ * (a cluster keeps its volume in shared memory; smaller clusters run more
+ * volumes side by side) and, for a single volume, the whole-GPU path.  It
+ * records the fastest in the context under the key (lattice, levels, bins,
+ * fitting-grid size of every volume, in order); later n4_run,
+ * n4_run_batched and n4_batch_graph_create calls with the same key use it
+ * unless a FORCE flag is set.  The outputs of the volumes are written as by
+ * a run.  Synchronous. */
+#define N4_TUNE_MAX 8
+typedef struct {
+  int candidates;                  /* configurations timed                   */
+  int cluster_size[N4_TUNE_MAX];   /* CTAs per volume; 0 = whole-GPU path    */
+  float ms[N4_TUNE_MAX];           /* device time of one run of the volumes  */
+  int chosen;                      /* index of the configuration recorded    */
+} n4_tune_report_t;
+
+n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *params, int n,
+                        const n4_volume_t *volumes, void *stream, n4_tune_report_t *report);
 
 /* ---- measurement (no counterpart in the reference) ----
  * With profiling enabled, every call records CUDA events around its kernels
@@ -222,12 +249,12 @@ n4_status_t n4_convergence(n4_context_t *ctx, const float *d_field1, const float
 /* ---- learned warm start (no counterpart in the reference) ----
  * A small 3-D convolutional encoder (4 conv 3x3x3 stride 2 layers of
  * 16/32/64/64 channels with ReLU, then a linear layer to 64 outputs) that
- * predicts the first-level 4x4x4 log-bias lattice from the masked log volume
- * average-pooled to 32x32x24.  BF16 weights and activations, FP32
- * accumulation on the tensor cores; FP32 master weights and Adam moments.
- * Inputs are device arrays of batch x 32 x 32 x 24 BF16 values
- * (n4_encoder_pool_input writes one); outputs batch x 64 floats, which are
- * first-level lattices to pass as `warm_lattice`. */
+ * predicts the first-level 4x4x4 log-bias lattice from the masked log
+ * fitting grid average-pooled to 32x32x24.  BF16 weights and activations,
+ * FP32 accumulation on the tensor cores; FP32 master weights and Adam
+ * moments.  Inputs are device arrays of batch x 32 x 32 x 24 BF16 values
+ * (n4_warm_inputs writes them); outputs batch x 64 floats, first-level
+ * lattices (n4_run_batched_warm uses them as warm starts). */
 typedef struct n4_encoder n4_encoder_t;
 
 size_t n4_encoder_num_params(void);
@@ -242,10 +269,29 @@ n4_status_t n4_encoder_predict(n4_encoder_t *enc, const void *d_x, int batch, fl
  * lr > 0.  h_loss (may be NULL) receives the batch loss (synchronises). */
 n4_status_t n4_encoder_train_step(n4_encoder_t *enc, const void *d_x, const float *d_target, int batch,
                                   float lr, float *h_loss, void *stream);
-/* Network input of one volume: mean of log(im) over masked voxels above
- * low_value in each of 32x32x24 adaptive pooling cells, as BF16. */
-n4_status_t n4_encoder_pool_input(const float *d_im, const float *d_mask, unsigned int fx, unsigned int fy,
-                                  unsigned int fz, float low_value, void *d_x, void *stream);
+
+
+/* ---- learned warm start inside a batched run (no counterpart in the
+ * reference) ----
+ * The network input of a volume is its masked log fitting grid (the
+ * threshold/shrink/log prologue of a run, background excluded) averaged over
+ * 32x32x24 adaptive cells, BF16 [32][32][24].  n4_warm_inputs writes the
+ * inputs of n volumes to d_x (n x 24576 BF16 values) without running N4
+ * (training data).  n4_run_batched_warm runs prologue -> pooling -> encoder
+ * -> N4 with the predicted lattices as warm starts -> correction on the
+ * stream, with the usual first-iteration rule per volume (a prediction whose
+ * first convergence value exceeds the zero lattice's is discarded); the
+ * volumes' warm_lattice fields must be NULL and the first-level lattice
+ * 4x4x4.  n4_batch_graph_create_warm records the same run as a CUDA graph.
+ * The encoder's buffers are used by one run at a time. */
+n4_status_t n4_warm_inputs(n4_context_t *ctx, const n4_params_t *p, int n,
+                           const n4_volume_t *vols, void *d_x, void *stream);
+n4_status_t n4_run_batched_warm(n4_context_t *ctx, const n4_params_t *p, int n,
+                                const n4_volume_t *vols, n4_encoder_t *encoder, void *stream,
+                                n4_report_t *reports);
+n4_status_t n4_batch_graph_create_warm(n4_context_t *ctx, const n4_params_t *p, int n,
+                                       const n4_volume_t *vols, n4_encoder_t *encoder,
+                                       n4_batch_graph_t **graph);
 
 #ifdef __cplusplus
 }

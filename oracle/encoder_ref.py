@@ -109,9 +109,10 @@ def backward(p, x, target):
     return np.concatenate(flat), out
 
 
-def pool_input(im, mask, low=0.0, shape=(32, 32, 24)):
-    """Adaptive average pooling of the masked log volume."""
-    X, Y, Z = im.shape
+def pool_fitgrid(imlog, shape=(32, 32, 24)):
+    """Warm-start network input: adaptive mean over the finite entries of
+    a masked log fitting grid (NaN outside the mask); 0 for empty cells."""
+    X, Y, Z = imlog.shape
     out = np.zeros(shape)
     for i in range(shape[0]):
         x0, x1 = i * X // shape[0], -(-(i + 1) * X // shape[0])
@@ -119,7 +120,7 @@ def pool_input(im, mask, low=0.0, shape=(32, 32, 24)):
             y0, y1 = j * Y // shape[1], -(-(j + 1) * Y // shape[1])
             for k in range(shape[2]):
                 z0, z1 = k * Z // shape[2], -(-(k + 1) * Z // shape[2])
-                v = im[x0:x1, y0:y1, z0:z1]
-                m = (mask[x0:x1, y0:y1, z0:z1] != 0) & (v > low)
-                out[i, j, k] = np.log(v[m]).mean() if m.any() else 0.0
+                v = imlog[x0:x1, y0:y1, z0:z1]
+                v = v[~np.isnan(v)]
+                out[i, j, k] = v.mean() if v.size else 0.0
     return out

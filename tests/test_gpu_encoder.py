@@ -80,11 +80,18 @@ def test_training_reduces_loss(cuda):
     assert rep.losses[-1] < 0.2 * first
 
 
-def test_pool_input(cuda):
-    from n4b200.encoder import pool_input
+def test_warm_inputs_pool_the_fitting_grid(cuda):
+    """n4_warm_inputs: threshold/shrink/log prologue, then 32x32x24 adaptive
+    pooling of the masked log fitting grid (BF16)."""
+    import n4b200
+    import n4_oracle as O
     from n4b200.phantom import make_phantom
-    for shape in ((64, 64, 48), (70, 66, 50)):
-        ph = make_phantom(shape, seed=2)
-        got = pool_input(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"), 0.0)
-        ref = R.pool_input(ph.im, ph.mask, 0.0)
-        assert nrel(got.float().cpu().numpy(), ref) < 5e-3
+    for shape, shrink in (((128, 128, 96), 4), ((96, 112, 80), 2), ((64, 64, 48), 4)):
+        ph = make_phantom(shape, seed=7)
+        p = n4b200.N4Param(ShrinkFactor=shrink, low_value=0.0)
+        got = n4b200.warm_inputs([(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"))], p)
+        mean, mask_s = O.shrink_volume(ph.im, ph.mask, shrink, 0.0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            imlog = np.where((mask_s != 0) & (mean > 0.0), np.log(mean), np.nan)
+        ref = R.pool_fitgrid(imlog)
+        assert nrel(got[0].float().cpu().numpy(), ref) < 5e-3, shape

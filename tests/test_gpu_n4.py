@@ -279,3 +279,55 @@ def test_batch_graph_replays(cuda):
     # a volume in a batch matches its single run to round-off, not bitwise
     assert nrel(res[0].lattice, single.lattice.cpu().numpy().astype(np.float64)) < 1e-6
     g.close()
+
+
+def test_autotune_records_the_fastest_configuration(cuda):
+    """n4_autotune times every cluster size that fits; later runs of volumes
+    of the same sizes use the recorded one."""
+    import n4b200
+    shapes = [(96, 96, 64), (112, 96, 72), (96, 104, 64), (120, 96, 80)]
+    vols = []
+    for i, sh in enumerate(shapes):
+        ph = make_phantom(sh, seed=300 + i)
+        vols.append((cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")))
+    p = param(3, [10] * 3, 0.001, ShrinkFactor=4)
+    ctx = n4b200.Context()
+    ref = n4b200.N4Batch(vols, p, ctx=ctx)
+    assert all(q.report["cluster_size"] == 16 for q in ref)       # untuned: the largest cluster
+    t = n4b200.autotune(vols, p, ctx=ctx)
+    sizes = [k for k, _ in t["candidates"]]
+    assert len(sizes) >= 2 and 16 in sizes
+    assert all(ms > 0 for _, ms in t["candidates"])
+    assert t["chosen"] == min(t["candidates"], key=lambda c: c[1])[0]
+    res = n4b200.N4Batch(vols, p, ctx=ctx)
+    for r in res:
+        assert r.report["status"] == "N4_OK"
+        assert r.report["cluster_size"] == t["chosen"]
+    # another batch shape is not affected by the record
+    other = n4b200.N4Batch(vols[:2], p, ctx=ctx)
+    assert all(r.report["cluster_size"] == 16 for r in other)
+    ctx.close()
+
+
+def test_every_cluster_size_matches_the_oracle(cuda):
+    """Cluster sizes 16 .. 2 (every size whose per-CTA share fits: at
+    256x256x176 only 16 does) on a 128x128x96 phantom at shrink 4 against
+    the FP64 oracle, fixed iterations."""
+    import n4b200
+    ph = make_phantom((128, 128, 96), seed=4, sigma=0.02, grid=6, coeff_std=0.25)
+    im, mk = cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")
+    out, lat, _ = O.N4Shrink(ph.im, ph.mask, 4, low_value=0, maximumNumberOfLevels=4,
+                             maximumNumberOfIterations=[8] * 4, ConvergenceThreshold=0.0, return_log_bias=True)
+    ran = []
+    for K in (16, 12, 8, 6, 4, 2):
+        pk = param(4, [8] * 4, 0.0, ShrinkFactor=4, flags=n4b200.cluster_size_flag(K))
+        try:
+            res = n4b200.N4(im, mk, pk)
+        except n4b200.N4Error as e:
+            assert "N4_ERR_TOO_LARGE" in str(e)
+            continue
+        assert res.report["cluster_size"] == K
+        assert nrel(res.lattice, lat) < TOL, K
+        assert nrel(res.im_normalized, out) < TOL, K
+        ran.append(K)
+    assert len(ran) >= 4, ran
