@@ -1,5 +1,5 @@
 // Warm-start encoder: a small 3-D convolutional network that predicts the
-// first-level 4x4x4 log-bias lattice of N4 from the masked log volume
+// first-level 4x4x4 log-bias lattice of N4 from the masked log fitting grid
 // average-pooled to 32x32x24.  No counterpart in the reference.
 //
 //   input 1x32x32x24 -> conv3x3x3/2 16 -> ReLU -> conv 32 -> ReLU -> conv 64
@@ -45,8 +45,22 @@ __device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], const 
 
 constexpr int BM = 64, BN = 64, BK = 32, PAD = 8;
 
+// Exact floor(k / d) for 0 <= k < 2^24 and 1 <= d < 2^16: with
+// M = ceil(2^40 / d), k*M / 2^40 exceeds k/d by less than 2^-16 < 1/d.
+struct Div {
+  unsigned d;
+  unsigned long long M;
+  Div() : d(1), M(1ull << 40) {}
+  explicit Div(unsigned dd) : d(dd), M(((1ull << 40) + dd - 1) / dd) {}
+  __device__ __forceinline__ int q(int k) const { return (int)(((unsigned long long)(unsigned)k * M) >> 40); }
+};
+
 // C[m][n] = sum_k A(m,k) B(k,n) over this block's K range; P supplies the
-// sizes, the gathers and the store.  128 threads: 4 warps of 32x32.
+// sizes, the gathers and the store.  128 threads: 4 warps of 32x32.  Tile
+// staging: each thread owns half a row of the A tile and half a row of the
+// B tile (16 consecutive k), so the row's index decomposition (P::a_row,
+// P::b_row) is done once per block and the k decomposition uses constant
+// divisors or Div; the 16 values go to shared memory as two 16-byte stores.
 template <class P>
 __global__ void __launch_bounds__(128) k_igemm(const P p) {
   __shared__ __align__(16) bf16 As[BM][BK + PAD];
@@ -57,19 +71,26 @@ __global__ void __launch_bounds__(128) k_igemm(const P p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, tig = lane & 3;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int sr = threadIdx.x >> 1, sc = (threadIdx.x & 1) * 16;   // staged row, first column
+  const bool a_ok = m0 + sr < p.M, b_ok = n0 + sr < p.N;
+  const typename P::ARow ar = p.a_row(a_ok ? m0 + sr : 0);
+  const typename P::BRow br = p.b_row(b_ok ? n0 + sr : 0);
   float acc[2][4][4] = {};
   const bf16 zero = __float2bfloat16(0.0f);
   for (int k0 = kb; k0 < ke; k0 += BK) {
-    for (int i = threadIdx.x; i < BM * BK; i += blockDim.x) {
-      const int r = i / BK, c = i - r * BK;
-      const int m = m0 + r, k = k0 + c;
-      As[r][c] = (m < p.M && k < ke) ? p.a(m, k) : zero;
+    unsigned pa[8], pb[8];   // bf16 pairs, low half first
+#pragma unroll
+    for (int j = 0; j < 16; j += 2) {
+      const int k = k0 + sc + j;
+      const bf16 a0 = (a_ok && k < ke) ? p.a(ar, k) : zero, a1 = (a_ok && k + 1 < ke) ? p.a(ar, k + 1) : zero;
+      const bf16 b0 = (b_ok && k < ke) ? p.b(br, k) : zero, b1 = (b_ok && k + 1 < ke) ? p.b(br, k + 1) : zero;
+      pa[j / 2] = (unsigned)__bfloat16_as_ushort(a0) | ((unsigned)__bfloat16_as_ushort(a1) << 16);
+      pb[j / 2] = (unsigned)__bfloat16_as_ushort(b0) | ((unsigned)__bfloat16_as_ushort(b1) << 16);
     }
-    for (int i = threadIdx.x; i < BN * BK; i += blockDim.x) {
-      const int r = i / BK, c = i - r * BK;
-      const int n = n0 + r, k = k0 + c;
-      Bs[r][c] = (n < p.N && k < ke) ? p.b(k, n) : zero;
-    }
+    *(uint4 *)&As[sr][sc] = make_uint4(pa[0], pa[1], pa[2], pa[3]);
+    *(uint4 *)&As[sr][sc + 8] = make_uint4(pa[4], pa[5], pa[6], pa[7]);
+    *(uint4 *)&Bs[sr][sc] = make_uint4(pb[0], pb[1], pb[2], pb[3]);
+    *(uint4 *)&Bs[sr][sc + 8] = make_uint4(pb[4], pb[5], pb[6], pb[7]);
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 16) {
@@ -114,6 +135,13 @@ struct Shape {
   __host__ __device__ int out_pos() const { return Do * Ho * Wo; }
 };
 
+// Output position decomposition (b, od, oh, ow) of a flat index.
+struct PosDiv {
+  Div op, hw, w;
+  PosDiv() {}
+  PosDiv(int out_pos, int hwo, int wo) : op(out_pos), hw(hwo), w(wo) {}
+};
+
 // y = relu(conv(x, w) + bias): M = B*outpos, N = Co, K = Ci*27
 struct ConvFwd {
   int M, N, K;
@@ -122,16 +150,22 @@ struct ConvFwd {
   const float *bias;
   bf16 *y;
   int relu;
-  __device__ bf16 a(int m, int k) const {
+  struct ARow { const bf16 *xb; int id0, ih0, iw0; };   // batch image, corner of the 3x3x3 window
+  struct BRow { const bf16 *wn; };
+  __device__ ARow a_row(int m) const {
     const int op = s.out_pos();
     const int b = m / op, r = m - b * op;
     const int od = r / (s.Ho * s.Wo), oh = (r / s.Wo) % s.Ho, ow = r % s.Wo;
-    const int ci = k / 27, t = k - ci * 27;
-    const int id = 2 * od + t / 9 - 1, ih = 2 * oh + (t / 3) % 3 - 1, iw = 2 * ow + t % 3 - 1;
-    if (id < 0 || id >= s.D || ih < 0 || ih >= s.H || iw < 0 || iw >= s.W) return __float2bfloat16(0.0f);
-    return x[(((size_t)b * s.Ci + ci) * s.D + id) * s.H * s.W + ih * s.W + iw];
+    return ARow{x + (size_t)b * s.Ci * s.in_pos(), 2 * od - 1, 2 * oh - 1, 2 * ow - 1};
   }
-  __device__ bf16 b(int k, int n) const { return w[(size_t)n * K + k]; }
+  __device__ bf16 a(const ARow &R, int k) const {
+    const int ci = k / 27, t = k - ci * 27;
+    const int id = R.id0 + t / 9, ih = R.ih0 + (t / 3) % 3, iw = R.iw0 + t % 3;
+    if (id < 0 || id >= s.D || ih < 0 || ih >= s.H || iw < 0 || iw >= s.W) return __float2bfloat16(0.0f);
+    return R.xb[((size_t)ci * s.D + id) * s.H * s.W + ih * s.W + iw];
+  }
+  __device__ BRow b_row(int n) const { return BRow{w + (size_t)n * K}; }
+  __device__ bf16 b(const BRow &R, int k) const { return R.wn[k]; }
   __device__ void store(int m, int n, int, float v) const {
     const int op = s.out_pos();
     const int b = m / op, r = m - b * op;
@@ -154,21 +188,27 @@ struct ConvDgrad {
   const bf16 *dy, *y, *w;
   bf16 *dx;
   int relu;
-  __device__ bf16 a(int m, int k) const {
+  struct ARow { size_t base; int pd0, ph0, pw0; };   // batch offset in dy, input position + 1
+  struct BRow { int n; };
+  __device__ ARow a_row(int m) const {
     const int ip = s.in_pos();
     const int b = m / ip, r = m - b * ip;
     const int id = r / (s.H * s.W), ih = (r / s.W) % s.H, iw = r % s.W;
+    return ARow{(size_t)b * s.Co * s.out_pos(), id + 1, ih + 1, iw + 1};
+  }
+  __device__ bf16 a(const ARow &R, int k) const {
     const int co = k / 27, t = k - co * 27;
-    const int pd = id + 1 - t / 9, ph = ih + 1 - (t / 3) % 3, pw = iw + 1 - t % 3;
+    const int pd = R.pd0 - t / 9, ph = R.ph0 - (t / 3) % 3, pw = R.pw0 - t % 3;
     if ((pd | ph | pw) & 1) return __float2bfloat16(0.0f);   // also rejects odd negatives
     const int od = pd >> 1, oh = ph >> 1, ow = pw >> 1;
     if (pd < 0 || ph < 0 || pw < 0 || od >= s.Do || oh >= s.Ho || ow >= s.Wo) return __float2bfloat16(0.0f);
-    const size_t i = ((size_t)b * s.Co + co) * s.out_pos() + (od * s.Ho + oh) * s.Wo + ow;
+    const size_t i = R.base + (size_t)co * s.out_pos() + (od * s.Ho + oh) * s.Wo + ow;
     return __float2bfloat16(dact(dy, y, i, relu));
   }
-  __device__ bf16 b(int k, int n) const {
+  __device__ BRow b_row(int n) const { return BRow{n}; }
+  __device__ bf16 b(const BRow &R, int k) const {
     const int co = k / 27, t = k - co * 27;
-    return w[((size_t)co * s.Ci + n) * 27 + t];
+    return w[((size_t)co * s.Ci + R.n) * 27 + t];
   }
   __device__ void store(int m, int n, int, float v) const {
     const int ip = s.in_pos();
@@ -184,19 +224,27 @@ struct ConvWgrad {
   const bf16 *x, *dy, *y;
   float *part;   // [splits][Co][Ci*27]
   int relu;
-  __device__ bf16 a(int m, int k) const {
+  PosDiv pd;     // decomposition of a position index k into (b, od, oh, ow)
+  struct ARow { int m; };
+  struct BRow { int ci, kd, kh, kw; };
+  __device__ ARow a_row(int m) const { return ARow{m}; }
+  __device__ bf16 a(const ARow &R, int k) const {
     const int op = s.out_pos();
-    const int b = k / op, r = k - b * op;
-    return __float2bfloat16(dact(dy, y, ((size_t)b * s.Co + m) * op + r, relu));
+    const int b = pd.op.q(k), r = k - b * op;
+    return __float2bfloat16(dact(dy, y, ((size_t)b * s.Co + R.m) * op + r, relu));
   }
-  __device__ bf16 b(int k, int n) const {
-    const int op = s.out_pos();
-    const int bb = k / op, r = k - bb * op;
-    const int od = r / (s.Ho * s.Wo), oh = (r / s.Wo) % s.Ho, ow = r % s.Wo;
+  __device__ BRow b_row(int n) const {
     const int ci = n / 27, t = n - ci * 27;
-    const int id = 2 * od + t / 9 - 1, ih = 2 * oh + (t / 3) % 3 - 1, iw = 2 * ow + t % 3 - 1;
+    return BRow{ci, t / 9 - 1, (t / 3) % 3 - 1, t % 3 - 1};
+  }
+  __device__ bf16 b(const BRow &R, int k) const {
+    const int op = s.out_pos();
+    const int bb = pd.op.q(k), r = k - bb * op;
+    const int od = pd.hw.q(r), r2 = r - od * s.Ho * s.Wo;
+    const int oh = pd.w.q(r2), ow = r2 - oh * s.Wo;
+    const int id = 2 * od + R.kd, ih = 2 * oh + R.kh, iw = 2 * ow + R.kw;
     if (id < 0 || id >= s.D || ih < 0 || ih >= s.H || iw < 0 || iw >= s.W) return __float2bfloat16(0.0f);
-    return x[(((size_t)bb * s.Ci + ci) * s.D + id) * s.H * s.W + ih * s.W + iw];
+    return x[(((size_t)bb * s.Ci + R.ci) * s.D + id) * s.H * s.W + ih * s.W + iw];
   }
   __device__ void store(int m, int n, int z, float v) const { part[((size_t)z * M + m) * N + n] = v; }
 };
@@ -207,8 +255,12 @@ struct LinFwd {
   const bf16 *x, *w;
   const float *bias;
   float *y;
-  __device__ bf16 a(int m, int k) const { return x[(size_t)m * K + k]; }
-  __device__ bf16 b(int k, int n) const { return w[(size_t)n * K + k]; }
+  struct ARow { const bf16 *r; };
+  struct BRow { const bf16 *r; };
+  __device__ ARow a_row(int m) const { return ARow{x + (size_t)m * K}; }
+  __device__ bf16 a(const ARow &R, int k) const { return R.r[k]; }
+  __device__ BRow b_row(int n) const { return BRow{w + (size_t)n * K}; }
+  __device__ bf16 b(const BRow &R, int k) const { return R.r[k]; }
   __device__ void store(int m, int n, int, float v) const { y[(size_t)m * N + n] = v + bias[n]; }
 };
 // dx = dy W: M = B, N = in, K = out
@@ -216,8 +268,12 @@ struct LinDgrad {
   int M, N, K;
   const bf16 *dy, *w;
   bf16 *dx;
-  __device__ bf16 a(int m, int k) const { return dy[(size_t)m * K + k]; }
-  __device__ bf16 b(int k, int n) const { return w[(size_t)k * N + n]; }
+  struct ARow { const bf16 *r; };
+  struct BRow { int n; };
+  __device__ ARow a_row(int m) const { return ARow{dy + (size_t)m * K}; }
+  __device__ bf16 a(const ARow &R, int k) const { return R.r[k]; }
+  __device__ BRow b_row(int n) const { return BRow{n}; }
+  __device__ bf16 b(const BRow &R, int k) const { return w[(size_t)k * N + R.n]; }
   __device__ void store(int m, int n, int, float v) const { dx[(size_t)m * N + n] = __float2bfloat16(v); }
 };
 // dW = dy^T x: M = out, N = in, K = B
@@ -225,8 +281,12 @@ struct LinWgrad {
   int M, N, K;
   const bf16 *dy, *x;
   float *part;
-  __device__ bf16 a(int m, int k) const { return dy[(size_t)k * M + m]; }
-  __device__ bf16 b(int k, int n) const { return x[(size_t)k * N + n]; }
+  struct ARow { int m; };
+  struct BRow { int n; };
+  __device__ ARow a_row(int m) const { return ARow{m}; }
+  __device__ bf16 a(const ARow &R, int k) const { return dy[(size_t)k * M + R.m]; }
+  __device__ BRow b_row(int n) const { return BRow{n}; }
+  __device__ bf16 b(const BRow &R, int k) const { return x[(size_t)k * N + R.n]; }
   __device__ void store(int m, int n, int z, float v) const { part[((size_t)z * M + m) * N + n] = v; }
 };
 
@@ -295,9 +355,6 @@ __global__ void k_to_bf16(const float *a, int n, bf16 *b) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = __float2bfloat16(a[i]);
 }
 
-// Adaptive average pool of a volume's masked log intensity to 32x32x24:
-// cell (i,j,k) covers [floor(i D/32), ceil((i+1) D/32)) per axis; the value
-// is the mean of log(im) over masked voxels with im > low (0 when none).
 // ------------------------------------------------------------------ host side
 template <class P>
 cudaError_t run_gemm(const P &p, int splits, cudaStream_t st) {
@@ -495,7 +552,8 @@ n4_status_t n4_encoder_train_step(n4_encoder_t *e, const void *d_x, const float 
     const Shape &sh = L.s[l];
     const long long K = (long long)B * sh.out_pos();
     const int splits = wgrad_splits(K);
-    ConvWgrad wg{sh.Co, sh.Ci * 27, (int)K, sh, e->act[l], e->dact_[l + 1], e->act[l + 1], e->part, 1};
+    ConvWgrad wg{sh.Co, sh.Ci * 27, (int)K, sh, e->act[l], e->dact_[l + 1], e->act[l + 1], e->part, 1,
+                 PosDiv(sh.out_pos(), sh.Ho * sh.Wo, sh.Wo)};
     ECK(run_gemm(wg, splits, st));
     k_sum_splits<<<64, 256, 0, st>>>(e->part, splits, sh.Co * sh.Ci * 27, e->g + L.w[l]);
     k_bias_grad<<<sh.Co, 256, 0, st>>>(e->dact_[l + 1], e->act[l + 1], B, sh.Co, sh.out_pos(), 1, e->g + L.b[l]);
