@@ -185,6 +185,46 @@ def cpu_baseline_single(seconds=12.0):
                       f"on one core ({iters / n:.1f} iterations per volume, phantom generation untimed)"}
 
 
+def measure_components(dev, ctx, hbm_peak, reps=10):
+    """Standalone HBM-bound kernels at the 512x512x320 scale: the fit's z
+    contraction (k_fit_rows_v4) on the 256x256x160 fitting grid (reads field
+    4 B + float mask 4 B per voxel) and the dense evaluation (k_correct) at
+    full resolution (writes 4 B per voxel); device time of the kernel alone
+    from the library's stage events, mean of `reps` calls."""
+    import numpy as np
+    import torch
+    import n4b200
+    gen = torch.Generator(device=dev).manual_seed(5)
+    fit_shape, full_shape = (256, 256, 160), (512, 512, 320)
+    field = torch.randn(fit_shape, device=dev, generator=gen)
+    fmask = (torch.rand(fit_shape, device=dev, generator=gen) > 0.4).float()
+    lat11 = torch.randn((11, 11, 11), device=dev, generator=gen) * 0.1
+
+    def kernel_ms(fn, stage):
+        fn()
+        ctx.set_profiling(True)
+        tot = 0.0
+        for _ in range(reps):
+            fn()
+            tot += ctx.last_timings()["stage_ms"][stage]
+        ctx.set_profiling(False)
+        return tot / reps
+    ms_fit = kernel_ms(lambda: n4b200.FitBspline3D(field, fmask, (11, 11, 11), ctx=ctx), 0)
+    ms_eval = kernel_ms(lambda: n4b200.EvaluateBspline3D(lat11, (11, 11, 11), full_shape, ctx=ctx), 1)
+    nfit, nfull = field.numel(), int(np.prod(full_shape))
+    del field, fmask
+    fit = 8 * nfit / (ms_fit / 1000) / 1e9
+    ups = 4 * nfull / (ms_eval / 1000) / 1e9
+    return {
+        "fit_gbs": {"value": fit, "frac": fit / hbm_peak, "ms": ms_fit,
+                    "workload": "FitBspline3D z-contraction pass (k_fit_rows_v4) over a 256x256x160 field + "
+                                "float mask, 11^3 lattice (8 B per voxel read)"},
+        "upsample_gbs": {"value": ups, "frac": ups / hbm_peak, "ms": ms_eval,
+                         "workload": "EvaluateBspline3D dense evaluation (k_correct) of an 11^3 lattice at "
+                                     "512x512x320 (4 B per voxel written)"},
+    }
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local_rank):
     import numpy as np
@@ -380,38 +420,7 @@ def run_ours(args, rank, world, local_rank):
     h2d = sum(a.numel() * 4 + b.numel() * 4 for a, b in vols_host)
     d2h = sum(o.numel() * 4 for o in out_h) + sum(l.numel() * 4 for l in lat_h)
 
-    # ---- standalone HBM-bound kernels at the 512x512x320 scale: the fit on
-    # its 256x256x160 fitting grid (reads field 4 B + float mask 4 B per voxel)
-    # and the dense evaluation at full resolution (writes 4 B per voxel)
-    def timed(fn, reps=10):
-        fn()
-        torch.cuda.synchronize(dev)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(reps):
-            fn()
-        b.record(stream)
-        torch.cuda.synchronize(dev)
-        return a.elapsed_time(b) / reps
-    gen = torch.Generator(device=dev).manual_seed(5)
-    fit_shape, full_shape = (256, 256, 160), (512, 512, 320)
-    field = torch.randn(fit_shape, device=dev, generator=gen)
-    fmask = (torch.rand(fit_shape, device=dev, generator=gen) > 0.4).float()
-    lat11 = torch.randn((11, 11, 11), device=dev, generator=gen) * 0.1
-    def kernel_ms(fn, stage, reps=10):
-        """Device time of one stage of a component call (library events)."""
-        fn()
-        ctx.set_profiling(True)
-        tot = 0.0
-        for _ in range(reps):
-            fn()
-            tot += ctx.last_timings()["stage_ms"][stage]
-        ctx.set_profiling(False)
-        return tot / reps
-    ms_fit = kernel_ms(lambda: n4b200.FitBspline3D(field, fmask, (11, 11, 11), ctx=ctx), 0)
-    ms_eval = kernel_ms(lambda: n4b200.EvaluateBspline3D(lat11, (11, 11, 11), full_shape, ctx=ctx), 1)
-    nfit, nfull = field.numel(), int(np.prod(full_shape))
-    del field, fmask
+    comp = measure_components(dev, ctx, peaks()[0])
 
     line = {
         "metric": METRIC, "value": value, "unit": "volumes/s", "n_gpus": world, "steps": args.steps,
@@ -445,13 +454,8 @@ def run_ours(args, rank, world, local_rank):
         "stages_ms_per_batch_warm": dict(zip(("prologue_pool_encoder", "n4_levels_iterations", "tables",
                                               "correction"), t_w["stage_ms"])),
         "stage_gbs": {"correct": corr_gbs, "prologue": pro_gbs},
-        "fit_gbs": {"value": 8 * nfit / (ms_fit / 1000) / 1e9, "frac": 8 * nfit / (ms_fit / 1000) / 1e9 / hbm_peak,
-                    "ms": ms_fit, "workload": "FitBspline3D z-contraction pass (k_fit_rows) over a 256x256x160 field + "
-                                              "float mask, 11^3 lattice (8 B per voxel read)"},
-        "upsample_gbs": {"value": 4 * nfull / (ms_eval / 1000) / 1e9,
-                         "frac": 4 * nfull / (ms_eval / 1000) / 1e9 / hbm_peak, "ms": ms_eval,
-                         "workload": "EvaluateBspline3D dense evaluation (k_correct) of an 11^3 lattice at "
-                                     "512x512x320 (4 B per voxel written)"},
+        "fit_gbs": comp["fit_gbs"],
+        "upsample_gbs": comp["upsample_gbs"],
         "iterations_per_volume": sum(iters_w) / B,
         "host_enqueue_ms_per_step": host_ms,
     }
@@ -473,12 +477,21 @@ def main():
     ap.add_argument("--batch", type=int, default=48)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--components-only", action="store_true",
+                    help="only the standalone fit / evaluation kernels at the 512x512x320 scale (for profiling)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.components_only:
+        import torch
+        import n4b200
+        torch.cuda.set_device(local_rank)
+        dev = torch.device("cuda", local_rank)
+        print(json.dumps(measure_components(dev, n4b200.Context(local_rank), peaks()[0])), flush=True)
+        return 0
     return run_ours(args, rank, world if "RANK" in os.environ else 1, local_rank)
 
 

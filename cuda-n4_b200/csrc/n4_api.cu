@@ -1324,10 +1324,12 @@ n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *g) {
 // starts on a 16-byte boundary, the scalar one otherwise (same arithmetic).
 static void launch_fit_rows(const float *field, const float *mask, long long rows, int Z, const Axis &az,
                             float *t1n, float *t1d, cudaStream_t st) {
-  const bool v4 = Z % 4 == 0 && ((uintptr_t)field & 15u) == 0 && ((uintptr_t)mask & 15u) == 0;
+  // the vectorised kernel's z table (36 B per voxel) stays within the default
+  // 48 KB of dynamic shared memory beside its 18 KB of staging for Z <= 800
+  const bool v4 = Z % 4 == 0 && Z <= 800 && ((uintptr_t)field & 15u) == 0 && ((uintptr_t)mask & 15u) == 0;
   if (v4)
-    k_fit_rows_v4<<<(unsigned)((rows + kFitRowsV - 1) / kFitRowsV), kFitRowsV, 0, st>>>(field, mask, rows, Z, az,
-                                                                                         t1n, t1d);
+    k_fit_rows_v4<<<(unsigned)((rows + kFitRowsV - 1) / kFitRowsV), kFitRowsV, kFitTableBytes(Z), st>>>(
+        field, mask, rows, Z, az, t1n, t1d);
   else
     k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(field, mask, rows, Z, az, t1n,
                                                                                    t1d);

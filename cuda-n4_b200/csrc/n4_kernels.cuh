@@ -285,16 +285,17 @@ struct CorrectVol {
   int vec4;              // FZ % 4 == 0 and every pointer 16-byte aligned
 };
 
-constexpr int kRowsPerTile = 16;
+constexpr int kRowsPerTile = 32;
 constexpr int kMaxNcz = 64;
 
 // One CTA per tile of kRowsPerTile full-resolution rows: x/y-contract the
-// lattice for its rows into shared memory, then evaluate z per voxel with
-// float4 I/O.  HBM traffic: read im, write out (+ bias).
-constexpr int kCorrectPre = 6;   // input float4 loads a thread keeps in flight
+// lattice for its rows into shared memory (one warp per row, one lane per z
+// control point), then evaluate z per voxel with float4 I/O.  HBM traffic:
+// read im, write out (+ bias).
+constexpr int kCorrectPre = 4;   // input float4 loads a thread keeps in flight
 
 __global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, const long long *tile_starts,
-                                                 int nvol, float low) {
+                                                    int nvol, float low) {
   __shared__ float Gs[kRowsPerTile * kMaxNcz];
   const int v = find_volume(tile_starts, nvol, blockIdx.x);
   const CorrectVol &C = vols[v];
@@ -306,15 +307,37 @@ __global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, cons
   const int FZ = C.FZ;
   const long long base = row0 * FZ;
   // float4 path: each thread owns 4 consecutive z (weights in registers) and
-  // rows r_first, r_first + rpp, ...; its first kCorrectPre input float4s
-  // are requested before the lattice contraction, so the HBM latency of the
-  // tile overlaps the contraction's L1/L2 gathers
+  // rows r_first, r_first + rpp, ...; it requests kCorrectPre input float4s
+  // at a time, the first ones before the barrier that ends the contraction
   const bool vec = C.vec4 != 0;
   const int nz4 = vec ? FZ >> 2 : 1;
   const int rpp = vec ? (int)blockDim.x / nz4 : 0;          // rows per pass (nz4 <= 256)
   const bool act = vec && (int)threadIdx.x < rpp * nz4;
   const int z = act ? ((int)threadIdx.x % nz4) * 4 : 0;
   const int r_first = act ? (int)threadIdx.x / nz4 : 0;
+  {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    const unsigned FY = (unsigned)C.FY;
+    for (int r = warp; r < nr; r += nwarp) {
+      const unsigned row = (unsigned)(row0 + r);   // rows of one volume < 2^32
+      const int vx = (int)(row / FY), vy = (int)(row - (unsigned)vx * FY);
+      const int sx = ax.s[vx], sy = ay.s[vy];
+      const float4 wx = ax.w[vx], wy = ay.w[vy];
+      const float wxa[4] = {wx.x, wx.y, wx.z, wx.w}, wya[4] = {wy.x, wy.y, wy.z, wy.w};
+      for (int cz = lane; cz < ncz; cz += 32) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int jx = 0; jx < 4; ++jx) {
+          const float *lp = C.lattice + ((sx + jx) * ncy + sy) * ncz + cz;
+          float s = 0.0f;
+#pragma unroll
+          for (int jy = 0; jy < 4; ++jy) s = __fmaf_rn(wya[jy], __ldg(lp + jy * ncz), s);
+          acc = __fmaf_rn(wxa[jx], s, acc);
+        }
+        Gs[r * ncz + cz] = acc;
+      }
+    }
+  }
   float4 xin[kCorrectPre];
   if (act && C.im) {
 #pragma unroll
@@ -323,31 +346,32 @@ __global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, cons
       xin[k] = r < nr ? __ldcs((const float4 *)(C.im + base + (long long)r * FZ + z)) : make_float4(0.f, 0.f, 0.f, 0.f);
     }
   }
-  for (int t = threadIdx.x; t < nr * ncz; t += blockDim.x) {
-    const int r = t / ncz, cz = t - r * ncz;
-    const long long row = row0 + r;
-    const int vx = (int)(row / C.FY), vy = (int)(row - (long long)vx * C.FY);
-    const int sx = ax.s[vx], sy = ay.s[vy];
-    const float4 wx = ax.w[vx], wy = ay.w[vy];
-    const float wxa[4] = {wx.x, wx.y, wx.z, wx.w}, wya[4] = {wy.x, wy.y, wy.z, wy.w};
-    float acc = 0.0f;
-#pragma unroll
-    for (int jx = 0; jx < 4; ++jx) {
-      const float *lp = C.lattice + ((sx + jx) * ncy + sy) * ncz + cz;
-      float s = 0.0f;
-#pragma unroll
-      for (int jy = 0; jy < 4; ++jy) s = __fmaf_rn(wya[jy], __ldg(lp + jy * ncz), s);
-      acc = __fmaf_rn(wxa[jx], s, acc);
-    }
-    Gs[t] = acc;
-  }
   __syncthreads();
   if (vec) {
     if (!act) return;
     int sz[4];
-    float4 wz[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) { sz[k] = az.s[z + k]; wz[k] = az.w[z + k]; }
+    for (int k = 0; k < 4; ++k) sz[k] = az.s[z + k];
+    // When the thread's 4 voxels lie in at most two spans (spans of >= 4
+    // voxels), every row needs only G[s0 .. s0+4]: voxel q's value is
+    // sum_j c[q][j] G[s0+j] with its 4 weights shifted by sz[q] - s0 and a
+    // zero beside them, the same products and additions in the same order
+    // as dot4 (a zero weight adds an exact zero).  5 shared loads per row
+    // instead of 16.
+    const int s0 = sz[0];
+    const bool two = sz[3] - s0 <= 1;
+    const bool has5 = s0 + 4 < ncz;
+    float cq[4][5];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 w = az.w[z + q];
+      const bool sh = sz[q] != s0;
+      cq[q][0] = sh ? 0.0f : w.x;
+      cq[q][1] = sh ? w.x : w.y;
+      cq[q][2] = sh ? w.y : w.z;
+      cq[q][3] = sh ? w.z : w.w;
+      cq[q][4] = sh ? w.w : 0.0f;
+    }
     for (int rb = r_first; rb < nr; rb += kCorrectPre * rpp) {
       if (rb != r_first && C.im) {
 #pragma unroll
@@ -363,17 +387,36 @@ __global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, cons
         if (r >= nr) break;
         const float *g = Gs + r * ncz;
         float bz[4];
+        if (two) {
+          const float g0 = g[s0], g1 = g[s0 + 1], g2 = g[s0 + 2], g3 = g[s0 + 3];
+          const float g4 = has5 ? g[s0 + 4] : 0.0f;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) bz[q] = dot4(wz[q], g + sz[q]);
+          for (int q = 0; q < 4; ++q) {
+            float b = __fmul_rn(cq[q][0], g0);
+            b = __fmaf_rn(cq[q][1], g1, b);
+            b = __fmaf_rn(cq[q][2], g2, b);
+            b = __fmaf_rn(cq[q][3], g3, b);
+            bz[q] = __fmaf_rn(cq[q][4], g4, b);
+          }
+        } else {   // short spans: the general form (weights re-read, rare)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) bz[q] = dot4(az.w[z + q], g + sz[q]);
+        }
         const long long off = base + (long long)r * FZ + z;
         if (C.im) {
-          // exp/divide use the fast intrinsics (a few ulp)
+          // im / exp(b) as im * exp(-b): one special-function op per voxel
+          // (fast intrinsic, a few ulp); exp(b) only when it is an output
           const float xa[4] = {xin[k].x, xin[k].y, xin[k].z, xin[k].w};
-          float o[4], e[4];
+          float o[4];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) { e[q] = __expf(bz[q]); o[q] = xa[q] > low ? __fdividef(xa[q], e[q]) : 0.0f; }
+          for (int q = 0; q < 4; ++q) o[q] = xa[q] > low ? xa[q] * __expf(-bz[q]) : 0.0f;
+          if (C.bias) {
+            float e[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) e[q] = __expf(bz[q]);
+            __stcs((float4 *)(C.bias + off), make_float4(e[0], e[1], e[2], e[3]));
+          }
           __stcs((float4 *)(C.out + off), make_float4(o[0], o[1], o[2], o[3]));
-          if (C.bias) __stcs((float4 *)(C.bias + off), make_float4(e[0], e[1], e[2], e[3]));
         } else {
           __stcs((float4 *)(C.out + off), make_float4(bz[0], bz[1], bz[2], bz[3]));
         }
@@ -386,9 +429,8 @@ __global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, cons
       const float b = dot4(az.w[zz], Gs + r * ncz + az.s[zz]);
       if (C.im) {
         const float x = C.im[off];
-        const float e = __expf(b);
-        C.out[off] = x > low ? __fdividef(x, e) : 0.0f;
-        if (C.bias) C.bias[off] = e;
+        C.out[off] = x > low ? x * __expf(-b) : 0.0f;
+        if (C.bias) C.bias[off] = __expf(b);
       } else {
         C.out[off] = b;
       }
@@ -462,18 +504,34 @@ __global__ void __launch_bounds__(kFitRows) k_fit_rows(const float *field, const
 // built for HBM bandwidth: 64 rows per CTA (every CTA of a 256x256-row field
 // resident at once), coalesced float4 streaming loads of the next 32-voxel
 // chunk issued into registers before the current chunk is walked from
-// shared memory, and a shared row stride of 36 floats so that the per-row
-// float4 reads of a quarter warp fall in 8 distinct 16-byte bank groups.
-// The per-voxel arithmetic and its order are those of k_fit_rows.
+// shared memory, a shared row stride of 36 floats so that the per-row float4
+// reads of a quarter warp fall in 8 distinct 16-byte bank groups, and the
+// z-axis table (span, numerator and denominator weights) copied to shared
+// memory so that the walk's table reads neither wait on L1 nor alias the
+// row-sum stores.  The sums are bitwise those of k_fit_rows (same operations
+// in the same order; masked-out voxels add exact zeros).  Dynamic shared
+// memory: kFitTableBytes(Z).
 constexpr int kFitRowsV = 64;
 constexpr int kFitChunkV = 32;
 constexpr int kFitStrideV = kFitChunkV + 4;
 constexpr int kFitLoadsV = kFitChunkV / 4;   // float4 per thread (one row each) per array and chunk
+__host__ __device__ inline size_t kFitTableBytes(int Z) { return (size_t)Z * 36; }
 
-__global__ void __launch_bounds__(kFitRowsV, 8) k_fit_rows_v4(const float *field, const float *mask, long long rows,
-                                                           int Z, Axis az, float *t1n, float *t1d) {
+__global__ void __launch_bounds__(kFitRowsV, 8) k_fit_rows_v4(const float *__restrict__ field,
+                                                              const float *__restrict__ mask, long long rows, int Z,
+                                                              Axis az, float *__restrict__ t1n,
+                                                              float *__restrict__ t1d) {
   __shared__ __align__(16) float fs[kFitRowsV * kFitStrideV];
   __shared__ __align__(16) float ms[kFitRowsV * kFitStrideV];
+  extern __shared__ __align__(16) char fit_tab[];
+  float4 *sp4 = (float4 *)fit_tab;                  // [Z] numerator weights
+  float4 *sq4 = sp4 + Z;                            // [Z] denominator weights
+  int *ss = (int *)(sq4 + Z);                       // [Z] span index
+  for (int i = threadIdx.x; i < Z; i += blockDim.x) {
+    sp4[i] = az.p4[i];
+    sq4[i] = az.q4[i];
+    ss[i] = az.s[i];
+  }
   const long long row0 = (long long)blockIdx.x * kFitRowsV;
   const int nr = (int)min((long long)kFitRowsV, rows - row0);
   const int t = threadIdx.x;
@@ -496,6 +554,7 @@ __global__ void __launch_bounds__(kFitRowsV, 8) k_fit_rows_v4(const float *field
   };
   float n0 = 0.f, n1 = 0.f, n2 = 0.f, n3 = 0.f, d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
   int cur = 0;
+  float *on = t1n + (row0 + t) * ncz, *od = t1d + (row0 + t) * ncz;
   load(0);
   for (int z0 = 0; z0 < Z; z0 += kFitChunkV) {
     __syncthreads();
@@ -509,38 +568,56 @@ __global__ void __launch_bounds__(kFitRowsV, 8) k_fit_rows_v4(const float *field
     __syncthreads();
     if (z0 + kFitChunkV < Z) load(z0 + kFitChunkV);
     if (t < nr) {
+      // branch-free per voxel: a masked-out voxel adds p*0 and q*0, which
+      // leaves the sums bitwise unchanged (and ignores a non-finite value
+      // there); a masked voxel adds fma(p, f, n) and fma(q, 1, d) = d + q
       const int nq = min(kFitChunkV, Z - z0) >> 2;
       for (int q = 0; q < nq; ++q) {
         const float4 f4 = *(const float4 *)(fs + t * kFitStrideV + 4 * q);
         const float4 m4 = *(const float4 *)(ms + t * kFitStrideV + 4 * q);
         const float fa[4] = {f4.x, f4.y, f4.z, f4.w}, ma[4] = {m4.x, m4.y, m4.z, m4.w};
+        const int vq = z0 + 4 * q;
+        if (ss[vq + 3] != cur) {
+          // a span ends inside these 4 voxels: voxel by voxel
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int vz = z0 + 4 * q + k;
-          const int sp = az.s[vz];
-          while (cur < sp) {
-            t1n[(row0 + t) * ncz + cur] = n0;
-            t1d[(row0 + t) * ncz + cur] = d0;
-            n0 = n1; n1 = n2; n2 = n3; n3 = 0.f;
-            d0 = d1; d1 = d2; d2 = d3; d3 = 0.f;
-            ++cur;
+          for (int k = 0; k < 4; ++k) {
+            const int sp = ss[vq + k];
+            while (cur < sp) {
+              on[cur] = n0;
+              od[cur] = d0;
+              n0 = n1; n1 = n2; n2 = n3; n3 = 0.f;
+              d0 = d1; d1 = d2; d2 = d3; d3 = 0.f;
+              ++cur;
+            }
+            const bool in = ma[k] != 0.0f;
+            const float f = in ? fa[k] : 0.0f, u = in ? 1.0f : 0.0f;
+            const float4 p = sp4[vq + k], w = sq4[vq + k];
+            n0 = __fmaf_rn(p.x, f, n0); n1 = __fmaf_rn(p.y, f, n1);
+            n2 = __fmaf_rn(p.z, f, n2); n3 = __fmaf_rn(p.w, f, n3);
+            d0 = __fmaf_rn(w.x, u, d0); d1 = __fmaf_rn(w.y, u, d1);
+            d2 = __fmaf_rn(w.z, u, d2); d3 = __fmaf_rn(w.w, u, d3);
           }
-          if (ma[k] == 0.0f) continue;
-          const float f = fa[k];
-          const float4 p = az.p4[vz], w = az.q4[vz];
-          n0 = __fmaf_rn(p.x, f, n0); n1 = __fmaf_rn(p.y, f, n1);
-          n2 = __fmaf_rn(p.z, f, n2); n3 = __fmaf_rn(p.w, f, n3);
-          d0 += w.x; d1 += w.y; d2 += w.z; d3 += w.w;
+        } else {
+          // all 4 voxels in the open span (the common case)
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const bool in = ma[k] != 0.0f;
+            const float f = in ? fa[k] : 0.0f, u = in ? 1.0f : 0.0f;
+            const float4 p = sp4[vq + k], w = sq4[vq + k];
+            n0 = __fmaf_rn(p.x, f, n0); n1 = __fmaf_rn(p.y, f, n1);
+            n2 = __fmaf_rn(p.z, f, n2); n3 = __fmaf_rn(p.w, f, n3);
+            d0 = __fmaf_rn(w.x, u, d0); d1 = __fmaf_rn(w.y, u, d1);
+            d2 = __fmaf_rn(w.z, u, d2); d3 = __fmaf_rn(w.w, u, d3);
+          }
         }
       }
     }
   }
   if (t < nr) {
-    const float nn[4] = {n0, n1, n2, n3}, dd[4] = {d0, d1, d2, d3};
     for (int c = cur; c < ncz; ++c) {
       const int k = c - cur;
-      t1n[(row0 + t) * ncz + c] = k < 4 ? nn[k] : 0.0f;
-      t1d[(row0 + t) * ncz + c] = k < 4 ? dd[k] : 0.0f;
+      on[c] = k == 0 ? n0 : k == 1 ? n1 : k == 2 ? n2 : k == 3 ? n3 : 0.0f;
+      od[c] = k == 0 ? d0 : k == 1 ? d1 : k == 2 ? d2 : k == 3 ? d3 : 0.0f;
     }
   }
 }
