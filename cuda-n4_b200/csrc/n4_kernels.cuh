@@ -285,18 +285,23 @@ struct CorrectVol {
   int vec4;              // FZ % 4 == 0 and every pointer 16-byte aligned
 };
 
-constexpr int kRowsPerTile = 32;
+constexpr int kRowsPerTile = 64;
 constexpr int kMaxNcz = 64;
+constexpr int kLxMax = 2048;    // x-contracted lattice slice ncy*ncz held per x-plane
 
-// One CTA per tile of kRowsPerTile full-resolution rows: x/y-contract the
-// lattice for its rows into shared memory (one warp per row, one lane per z
-// control point), then evaluate z per voxel with float4 I/O.  HBM traffic:
-// read im, write out (+ bias).
+// One CTA per tile of kRowsPerTile full-resolution rows (vy fastest within
+// an x-plane).  Contraction of the lattice for the tile's rows into shared
+// memory, separable: per x-plane the tile touches, Lx[cy][cz] =
+// sum_jx wx L[sx+jx][cy][cz]; per row, G[r][cz] = sum_jy wy Lx[sy+jy][cz]
+// (a tile spanning more than two planes, or a slice larger than kLxMax,
+// contracts each row directly).  Then z is evaluated per voxel with float4
+// I/O.  HBM traffic: read im, write out (+ bias).
 constexpr int kCorrectPre = 4;   // input float4 loads a thread keeps in flight
 
 __global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, const long long *tile_starts,
                                                     int nvol, float low) {
   __shared__ float Gs[kRowsPerTile * kMaxNcz];
+  __shared__ float Lx[2 * kLxMax];
   const int v = find_volume(tile_starts, nvol, blockIdx.x);
   const CorrectVol &C = vols[v];
   const Axis ax = axis_at(C.tx, C.FX, C.ncx), ay = axis_at(C.ty, C.FY, C.ncy), az = axis_at(C.tz, C.FZ, C.ncz);
@@ -316,25 +321,58 @@ __global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, cons
   const int z = act ? ((int)threadIdx.x % nz4) * 4 : 0;
   const int r_first = act ? (int)threadIdx.x / nz4 : 0;
   {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
     const unsigned FY = (unsigned)C.FY;
-    for (int r = warp; r < nr; r += nwarp) {
-      const unsigned row = (unsigned)(row0 + r);   // rows of one volume < 2^32
-      const int vx = (int)(row / FY), vy = (int)(row - (unsigned)vx * FY);
-      const int sx = ax.s[vx], sy = ay.s[vy];
-      const float4 wx = ax.w[vx], wy = ay.w[vy];
-      const float wxa[4] = {wx.x, wx.y, wx.z, wx.w}, wya[4] = {wy.x, wy.y, wy.z, wy.w};
-      for (int cz = lane; cz < ncz; cz += 32) {
-        float acc = 0.0f;
+    const unsigned rw0 = (unsigned)row0;                     // rows of one volume < 2^32
+    const int vxa = (int)(rw0 / FY), vxb = (int)((rw0 + (unsigned)nr - 1u) / FY);
+    const int slice = ncy * ncz;
+    if (vxb - vxa <= 1 && slice <= kLxMax) {
+      const int np = vxb - vxa + 1;
+      for (int t = threadIdx.x; t < np * slice; t += blockDim.x) {
+        const int pl = t >= slice ? 1 : 0, c = t - pl * slice;
+        const int vx = vxa + pl;
+        const int sx = ax.s[vx];
+        const float4 wx = ax.w[vx];
+        const float *lp = C.lattice + (size_t)sx * slice + c;
+        float acc = __fmul_rn(wx.x, __ldg(lp));
+        acc = __fmaf_rn(wx.y, __ldg(lp + slice), acc);
+        acc = __fmaf_rn(wx.z, __ldg(lp + 2 * slice), acc);
+        Lx[t] = __fmaf_rn(wx.w, __ldg(lp + 3 * slice), acc);
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < nr * ncz; t += blockDim.x) {
+        const int r = t / ncz, cz = t - r * ncz;
+        const unsigned row = rw0 + (unsigned)r;
+        const int vx = (int)(row / FY), vy = (int)(row - (unsigned)vx * FY);
+        const float *lx = Lx + (vx - vxa) * slice + ay.s[vy] * ncz + cz;
+        const float4 wy = ay.w[vy];
+        float acc = __fmul_rn(wy.x, lx[0]);
+        acc = __fmaf_rn(wy.y, lx[ncz], acc);
+        acc = __fmaf_rn(wy.z, lx[2 * ncz], acc);
+        Gs[t] = __fmaf_rn(wy.w, lx[3 * ncz], acc);
+      }
+    } else {
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+      for (int r = warp; r < nr; r += nwarp) {
+        const unsigned row = rw0 + (unsigned)r;
+        const int vx = (int)(row / FY), vy = (int)(row - (unsigned)vx * FY);
+        const int sx = ax.s[vx], sy = ay.s[vy];
+        const float4 wx = ax.w[vx], wy = ay.w[vy];
+        const float wxa[4] = {wx.x, wx.y, wx.z, wx.w}, wya[4] = {wy.x, wy.y, wy.z, wy.w};
+        for (int cz = lane; cz < ncz; cz += 32) {
+          float lxv[4];
 #pragma unroll
-        for (int jx = 0; jx < 4; ++jx) {
-          const float *lp = C.lattice + ((sx + jx) * ncy + sy) * ncz + cz;
-          float s = 0.0f;
+          for (int jy = 0; jy < 4; ++jy) {
+            const float *lp = C.lattice + ((size_t)sx * ncy + sy + jy) * ncz + cz;
+            float acc = __fmul_rn(wxa[0], __ldg(lp));
 #pragma unroll
-          for (int jy = 0; jy < 4; ++jy) s = __fmaf_rn(wya[jy], __ldg(lp + jy * ncz), s);
-          acc = __fmaf_rn(wxa[jx], s, acc);
+            for (int jx = 1; jx < 4; ++jx) acc = __fmaf_rn(wxa[jx], __ldg(lp + (size_t)jx * ncy * ncz), acc);
+            lxv[jy] = acc;
+          }
+          float acc = __fmul_rn(wya[0], lxv[0]);
+#pragma unroll
+          for (int jy = 1; jy < 4; ++jy) acc = __fmaf_rn(wya[jy], lxv[jy], acc);
+          Gs[r * ncz + cz] = acc;
         }
-        Gs[r * ncz + cz] = acc;
       }
     }
   }
