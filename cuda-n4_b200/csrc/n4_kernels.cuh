@@ -540,7 +540,8 @@ __global__ void __launch_bounds__(kFitRows) k_fit_rows(const float *field, const
 
 // The same contraction for Z % 4 == 0 and 16-byte aligned field and mask,
 // built for HBM bandwidth: 64 rows per CTA (every CTA of a 256x256-row field
-// resident at once), coalesced float4 streaming loads of the next 32-voxel
+// resident at once), one L2 bulk prefetch of the CTA's contiguous rows,
+// coalesced float4 streaming loads of the next 32-voxel
 // chunk issued into registers before the current chunk is walked from
 // shared memory, a shared row stride of 36 floats so that the per-row float4
 // reads of a quarter warp fall in 8 distinct 16-byte bank groups, and the
@@ -574,6 +575,14 @@ __global__ void __launch_bounds__(kFitRowsV, 8) k_fit_rows_v4(const float *__res
   const int nr = (int)min((long long)kFitRowsV, rows - row0);
   const int t = threadIdx.x;
   const int ncz = az.nc;
+  // The CTA's rows are one contiguous range of field and mask: ask L2 for all
+  // of it at once (bulk prefetch, sequential in DRAM), so the strided
+  // 32-voxel chunk loads below are served from L2.
+  if (t == 0) {
+    const unsigned bytes = (unsigned)nr * (unsigned)Z * 4u;   // multiple of 16: Z % 4 == 0
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(field + row0 * Z), "r"(bytes) : "memory");
+    if (mask) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(mask + row0 * Z), "r"(bytes) : "memory");
+  }
   float4 pf[kFitLoadsV], pm[kFitLoadsV];
   const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f), one4 = make_float4(1.f, 1.f, 1.f, 1.f);
   auto load = [&](int z0) {
