@@ -225,6 +225,69 @@ def measure_components(dev, ctx, hbm_peak, reps=10):
     }
 
 
+def measure_c3(dev, ctx, reps=2):
+    """One 512x512x320 volume (0.5 mm phantom, 8^3-grid bias N(0, 0.25^2),
+    Rician 0.02) through n4_run at shrink 2 (256x256x160 fitting grid, the
+    whole-GPU path), 4 levels, <= 50 iterations, convergence 0.001."""
+    import torch
+    import n4b200
+    from n4b200.warmstart import phantoms_gpu
+    im, mk = phantoms_gpu(1, (512, 512, 320), seed=77, sigma=0.02, grid=8, coeff_std=0.25, device=dev)
+    p = n4b200.N4Param(NumberOfFittingLevels=4, MaximumNumberOfIterations=50, ConvergenceThreshold=0.001,
+                       low_value=0.0, ShrinkFactor=2)
+    res = n4b200.N4(im[0], mk[0], p, ctx=ctx)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(reps):
+        n4b200.N4(im[0], mk[0], p, ctx=ctx, synchronous=False)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / reps
+    return {"workload": "512x512x320 float32 phantom, shrink 2 -> 256x256x160, 4 levels, <=50 it/level, CV<0.001",
+            "ms_per_volume": ms, "volumes_per_s": 1000.0 / ms, "iterations": res.report["iterations"][:4],
+            "path": res.report["path"], "ctas": res.report["cluster_size"]}
+
+
+def measure_c4(dev, enc, n=48, reps=5):
+    """48 phantoms with every axis drawn from 96, 104, ..., 288 (4^3-grid bias
+    N(0, 0.15^2), Rician 0.03), shrink 4, 4 levels, <= 50 iterations,
+    convergence 0.001: one batched run each, with and without the learned
+    warm start, after autotuning the batch."""
+    import torch
+    import n4b200
+    from n4b200.phantom import batch_dims
+    from n4b200.warmstart import phantoms_gpu
+    vols = []
+    for i, sh in enumerate(batch_dims(n, seed=2024)):
+        im, mk = phantoms_gpu(1, sh, seed=3000 + i, sigma=0.03, grid=4, coeff_std=0.15, device=dev)
+        vols.append((im[0], mk[0]))
+    p = n4b200.N4Param(NumberOfFittingLevels=4, MaximumNumberOfIterations=50, ConvergenceThreshold=0.001,
+                       low_value=0.0, ShrinkFactor=4)
+    ctx = n4b200.Context(dev.index or 0)
+    tune = n4b200.autotune(vols, p, ctx=ctx)
+    out = {"workload": f"{n} phantoms, axes uniform in 96..288 step 8, shrink 4, 4 levels, <=50 it/level, CV<0.001",
+           "autotune": tune}
+    for name, kw in (("plain", {}), ("warm", {"encoder": enc})):
+        for _ in range(2):
+            res = n4b200.N4Batch(vols, p, ctx=ctx, **kw)
+        times = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record()
+            n4b200.N4Batch(vols, p, ctx=ctx, synchronous=False, **kw)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            times.append(e0.elapsed_time(e1))
+        ms = sorted(times)[len(times) // 2]
+        out[name] = {"volumes_per_s": n * 1000.0 / ms, "ms_per_batch_median": ms, "ms_per_batch_all": times,
+                     "iterations_per_volume": sum(sum(r.report["iterations"][:r.report["levels"]]) for r in res) / n,
+                     "paths": {k: sum(1 for r in res if r.report["path"] == k) for k in ("cluster", "grid")}}
+    ctx.close()
+    return out
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local_rank):
     import numpy as np
@@ -232,17 +295,15 @@ def run_ours(args, rank, world, local_rank):
     import n4b200
     from n4b200.phantom import make_phantom
 
+    from n4b200.replicas import Replicas, volume_seeds
+
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    rep = Replicas(world, dev)
     B = args.batch
     vols_host, vols_dev = [], []
-    for i in range(B):
-        ph = make_phantom(SHAPE, seed=1000 * rank + i, **GEN)
+    for seed in volume_seeds(rank, B):
+        ph = make_phantom(SHAPE, seed=seed, **GEN)
         im_h = torch.from_numpy(ph.im).pin_memory()
         mk_h = torch.from_numpy(ph.mask).pin_memory()
         vols_host.append((im_h, mk_h))
@@ -252,17 +313,8 @@ def run_ours(args, rank, world, local_rank):
     ctx = n4b200.Context(local_rank)
     stream = torch.cuda.current_stream(dev)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = rep.barrier
+    max_over_ranks = rep.max_over_ranks
 
     def step_batched():
         return n4b200.N4Batch(vols_dev, p, ctx=ctx, synchronous=False)
@@ -421,6 +473,8 @@ def run_ours(args, rank, world, local_rank):
     d2h = sum(o.numel() * 4 for o in out_h) + sum(l.numel() * 4 for l in lat_h)
 
     comp = measure_components(dev, ctx, peaks()[0])
+    c3 = measure_c3(dev, ctx)
+    c4 = measure_c4(dev, enc)
 
     line = {
         "metric": METRIC, "value": value, "unit": "volumes/s", "n_gpus": world, "steps": args.steps,
@@ -457,15 +511,15 @@ def run_ours(args, rank, world, local_rank):
         "fit_gbs": comp["fit_gbs"],
         "upsample_gbs": comp["upsample_gbs"],
         "iterations_per_volume": sum(iters_w) / B,
+        "c3_single_volume": c3,
+        "c4_batched_uneven": c4,
         "host_enqueue_ms_per_step": host_ms,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_single()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 

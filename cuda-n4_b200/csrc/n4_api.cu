@@ -355,6 +355,31 @@ n4_status_t choose_cluster(n4_context *ctx, const n4_params_t *p, const std::vec
   return N4_OK;
 }
 
+// Volumes (indices into dims) that run on a cluster of K CTAs: one launch
+// shares one shared-memory layout, sized by the maxima over its volumes, so
+// volumes are added largest first while that layout still fits; the others
+// go to `rest`.
+std::vector<int> cluster_subset(const n4_context *ctx, const n4_params_t *p, const std::vector<Dims> &dims,
+                                const std::vector<int> &idx, int K, std::vector<int> *rest) {
+  std::vector<int> order = idx, fit;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (long long)dims[a].X * dims[a].Y * dims[a].Z > (long long)dims[b].X * dims[b].Y * dims[b].Z;
+  });
+  std::vector<Dims> sub;
+  for (int i : order) {
+    sub.push_back(dims[i]);
+    if (cluster_fits(ctx, make_plan(p, K, sub, false))) {
+      fit.push_back(i);
+    } else {
+      sub.pop_back();
+      if (rest) rest->push_back(i);
+    }
+  }
+  std::sort(fit.begin(), fit.end());
+  if (rest) std::sort(rest->begin(), rest->end());
+  return fit;
+}
+
 // ------------------------------------------------------------------ upload ring
 struct Upload {
   Slot *slot;
@@ -601,20 +626,36 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
   } else if (n == 1) {
     P.in_grid.push_back(0);
   } else {
-    // batch with volumes too large for a cluster: split by fit
-    for (int i = 0; i < n; ++i) {
-      std::vector<Dims> one{dims[i]};
-      int K = 0;
-      TRY(choose_cluster(ctx, p, one, 1024, &K));
-      (K ? P.in_cluster : P.in_grid).push_back(i);
-    }
+    // batch with volumes too large for a cluster: the largest cluster size
+    // (the smallest per-CTA share) takes every volume its shared-memory
+    // layout can hold, the whole-GPU path the rest
+    std::vector<int> all(n), rest;
+    for (int i = 0; i < n; ++i) all[i] = i;
+    P.in_cluster = cluster_subset(ctx, p, dims, all, 16, &rest);
+    P.in_grid = rest;
     if (!P.in_cluster.empty()) {
       std::vector<Dims> sub;
       for (int i : P.in_cluster) sub.push_back(dims[i]);
-      ch.grid = false;
-      ch.nt = 1024;
-      TRY(choose_cluster(ctx, p, sub, 1024, &ch.K));
+      const Plan pl = make_plan(p, 16, sub, false);
+      int cap = 0;
+      TRY(capacity(ctx, 1024, 16, pl.sm_bytes + pl.big_bytes, &cap));
+      if (cap > 0) {
+        ch.grid = false;
+        ch.nt = 1024;
+        ch.K = 16;
+      } else {
+        for (int i : P.in_cluster) P.in_grid.push_back(i);
+        std::sort(P.in_grid.begin(), P.in_grid.end());
+        P.in_cluster.clear();
+      }
     }
+  }
+  if (!ch.grid && n > 1 && !(p->flags & N4_FLAG_CLUSTER_SIZE(31))) {
+    // a recorded cluster size (autotuner): volumes whose share does not fit
+    // a CTA of that cluster run on the whole-GPU path
+    std::vector<int> rest;
+    P.in_cluster = cluster_subset(ctx, p, dims, P.in_cluster, ch.K, &rest);
+    for (int i : rest) P.in_grid.push_back(i);
   }
   P.ch = ch;
   for (int i : P.in_grid) TRY(ensure_grid_workspace(ctx, p, dims[i]));
@@ -1074,8 +1115,15 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
   // and the whole-GPU path for a single volume
   std::vector<Choice> cand;
   for (int K : {16, 12, 8, 6, 4, 2}) {
-    Plan pl = make_plan(p, K, dims, false);
-    if (!cluster_fits(ctx, pl)) continue;
+    // the volumes whose per-CTA share fits this cluster size (the others
+    // take the whole-GPU path in a run with this choice)
+    std::vector<int> all(n);
+    for (int i = 0; i < n; ++i) all[i] = i;
+    const std::vector<int> fit = cluster_subset(ctx, p, dims, all, K, nullptr);
+    if (fit.empty()) continue;
+    std::vector<Dims> sub;
+    for (int i : fit) sub.push_back(dims[i]);
+    Plan pl = make_plan(p, K, sub, false);
     int cap = 0;
     TRY(capacity(ctx, 1024, K, pl.sm_bytes + pl.big_bytes, &cap));
     if (cap > 0) cand.push_back(Choice{false, K, 1024});

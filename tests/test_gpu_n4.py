@@ -331,3 +331,29 @@ def test_every_cluster_size_matches_the_oracle(cuda):
         assert nrel(res.im_normalized, out) < TOL, K
         ran.append(K)
     assert len(ran) >= 4, ran
+
+
+def test_batch_mixing_cluster_and_whole_gpu_volumes(cuda):
+    """A batch whose largest volume does not fit a cluster: the others run
+    on the cluster path, it on the whole-GPU path, each as in a single run;
+    the autotuner's record keeps that split."""
+    import n4b200
+    shapes = [(64, 64, 48), (288, 288, 288), (96, 80, 64)]
+    vols = []
+    for i, sh in enumerate(shapes):
+        ph = make_phantom(sh, seed=400 + i)
+        vols.append((cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")))
+    p = param(3, [10] * 3, 0.001, ShrinkFactor=4)
+    ctx = n4b200.Context()
+    res = n4b200.N4Batch(vols, p, ctx=ctx)
+    assert [r.report["path"] for r in res] == ["cluster", "grid", "cluster"]
+    for (im, mk), r in zip(vols, res):
+        single = n4b200.N4(im, mk, p, ctx=ctx)
+        assert r.report["status"] == "N4_OK" and r.report["iterations"] == single.report["iterations"]
+        assert nrel(r.lattice, single.lattice.cpu().numpy().astype(np.float64)) < 1e-6
+        assert nrel(r.im_normalized, single.im_normalized.cpu().numpy().astype(np.float64)) < 1e-6
+    t = n4b200.autotune(vols, p, ctx=ctx)
+    tuned = n4b200.N4Batch(vols, p, ctx=ctx)
+    assert tuned[1].report["path"] == "grid"
+    assert all(r.report["cluster_size"] == t["chosen"] for r in (tuned[0], tuned[2]))
+    ctx.close()
