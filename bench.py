@@ -50,6 +50,10 @@ SHRINK, LEVELS, ITERS, THR = 4, 4, 50, 0.001
 ITER_BYTES_PER_VOXEL = 27
 # final correction: read im 4 + write corrected 4 per full-resolution voxel
 CORRECT_BYTES_PER_VOXEL = 8
+# DRAM bytes (read + write) of one k_n4_cluster launch per volume of this
+# workload, from an ncu capture of a 4-volume launch (5.677 MB read + 27.6 KB
+# written): the volume stays in shared memory, so only its initial load moves
+TRAFFIC_PER_VOLUME = (5.677056e6 + 27.648e3) / 4
 
 
 def workload_desc(batch):
@@ -483,7 +487,9 @@ def run_ours(args, rank, world, local_rank):
         "config": workload_desc(B),
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-            "frac": achieved / hbm_peak, "traffic": None,
+            "frac": achieved / hbm_peak, "traffic": TRAFFIC_PER_VOLUME * B,
+            "traffic_basis": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 4-volume launch, scaled to "
+                             "the batch (grows in proportion: one load of each fitting grid)",
             "kernel": "k_n4_cluster (all levels/iterations of a batch)",
             "basis": f"{ITER_BYTES_PER_VOXEL} B per fitting voxel per iteration "
                      f"(fit 5 + histogram 5 + evaluate/CV/update 17) x iterations / kernel time; "
