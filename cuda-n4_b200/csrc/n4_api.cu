@@ -115,7 +115,7 @@ struct n4_context {
   int device = 0;
   int nsm = 0;
   int max_smem = 0;
-  DevBuf imlog, tables, logu, big, red, bar;
+  DevBuf imlog, tables, big, red, bar;
   DevBuf s1, s2, s3, s4, s5;   // component scratch
   DevBuf warm_x, warm_lat;     // learned warm start: network inputs, predicted lattices
   DevBuf h_im, h_mask, h_out, h_lat, h_bias, h_warm;   // host-run staging
@@ -257,24 +257,30 @@ Plan make_plan(const n4_params_t *p, int K, const std::vector<Dims> &vols, bool 
   pl.o_den = take((size_t)pl.NLAT * 4);
   pl.o_tmp = take((size_t)pl.NLAT * 4);
   pl.o_aux = take((size_t)pl.NLAT * 4);
-  pl.o_hist = take((size_t)kHistCopies * pl.bins * 4);
+  // cluster path: the histogram copies and the two FFT work buffers share
+  // the Gd region (see Plan::alias_sharpen); grid path: shared memory
+  const size_t hist_bytes = (size_t)kHistCopies * pl.bins * 4, fft_bytes = (size_t)pl.npad * 16;
+  pl.alias_sharpen = grid ? 0 : 1;
+  if (grid) {
+    pl.o_hist = take(hist_bytes);
+    pl.o_fa = take(fft_bytes);
+    pl.o_fb = take(fft_bytes);
+  }
   pl.o_H64 = take((size_t)pl.bins * 8);
   pl.o_H = take((size_t)pl.bins * 8);
   pl.o_E = take((size_t)pl.bins * 8);
-  pl.o_fa = take((size_t)pl.npad * 16);
-  pl.o_fb = take((size_t)pl.npad * 16);
   pl.o_tw = take((size_t)pl.npad * 16);
   pl.o_ff = take((size_t)pl.npad * 8);
   pl.o_red = take(160 * 8);
   pl.o_misc = take(64);
   pl.sm_bytes = (int)align_up(o, 128);
   o = 0;
-  if (!grid) {
-    pl.b_imlog = take(((size_t)pl.slab_floats + 8) * 4);
-    pl.b_logu = take((size_t)pl.slab_floats * 4);
-  }
+  if (!grid) pl.b_imlog = take(((size_t)pl.slab_floats + 8) * 4);
   pl.b_G = take((size_t)pl.rows_max * pl.NCZ * 4);
-  pl.b_Gd = take((size_t)pl.rows_max * pl.NCZ * 4);
+  pl.a_fa = 0;
+  pl.a_fb = (int)fft_bytes;
+  pl.a_hist = (int)(2 * fft_bytes);
+  pl.b_Gd = take(std::max((size_t)pl.rows_max * pl.NCZ * 4, grid ? 0 : 2 * fft_bytes + hist_bytes));
   pl.b_T2 = take((size_t)pl.nvxl * pl.NCY * pl.NCZ * 4);
   pl.b_slotA = take(sizeof(Stats));
   pl.b_slotB = take((size_t)pl.bins * 8);
@@ -449,8 +455,6 @@ struct RunVol {
 n4_status_t ensure_grid_workspace(n4_context *ctx, const n4_params_t *p, const Dims &d) {
   std::vector<Dims> one{d};
   Plan pl = make_plan(p, ctx->nsm, one, true);
-  const size_t nfit = (size_t)d.X * d.Y * d.Z;
-  TRY(ctx->logu.ensure(nfit * 4 + 64, "logU"));
   TRY(ctx->big.ensure((size_t)pl.big_bytes * ctx->nsm, "grid workspace"));
   TRY(ctx->red.ensure(std::max((size_t)pl.bins * 8, (size_t)pl.NLAT * 4) + 64, "grid reduction"));
   TRY(ctx->bar.ensure(64, "grid barrier"));
@@ -464,10 +468,8 @@ n4_status_t launch_grid_path(n4_context *ctx, const n4_params_t *p, const Params
   Plan pl = make_plan(p, nblk, one, true);
   if (pl.sm_bytes + kStaticSmemReserve > ctx->max_smem)
     return fail(N4_ERR_TOO_LARGE, "histogram/lattice workspace exceeds shared memory");
-  const size_t nfit = (size_t)rv.d.X * rv.d.Y * rv.d.Z;
   if ((long long)pl.rows_max * rv.d.Z >= (1ll << 22))
     return fail(N4_ERR_TOO_LARGE, "fitting grid too large for one GPU (raise ShrinkFactor)");
-  TRY(ctx->logu.ensure(nfit * 4 + 64, "logU"));
   TRY(ctx->big.ensure((size_t)pl.big_bytes * nblk, "grid workspace"));
   TRY(ctx->red.ensure(std::max((size_t)pl.bins * 8, (size_t)pl.NLAT * 4) + 64, "grid reduction"));
   TRY(ctx->bar.ensure(64, "grid barrier"));
@@ -476,7 +478,6 @@ n4_status_t launch_grid_path(n4_context *ctx, const n4_params_t *p, const Params
   a.pl = pl;
   a.pr = pr;
   a.job = job0;
-  a.job.logu = ctx->logu.as<float>();
   a.big_base = ctx->big.as<char>();
   a.big_stride = pl.big_bytes;
   a.bar.count = ctx->bar.as<unsigned>();
@@ -717,7 +718,7 @@ void fill_descriptors(n4_context *ctx, const n4_params_t *p, Prepared &P, const 
                         d.X, d.Y, d.Z, il, fit_total};
     pst[i] = fit_total;
     fit_total += (long long)d.X * d.Y * d.Z;
-    jb[i] = VolJob{d.X, d.Y, d.Z, il, nullptr, r.warm, r.lat, B.dp<n4_report_t>(P.o_rep) + i};
+    jb[i] = VolJob{d.X, d.Y, d.Z, il, r.warm, r.lat, B.dp<n4_report_t>(P.o_rep) + i};
     B.hp<PoolJob>(P.o_pool)[i] = PoolJob{il, d.X, d.Y, d.Z};
     char *tx = tabs + P.tab_off[i];
     char *ty = tx + align_up(axis_bytes(d.FX, P.NCX - 3), 256);
@@ -951,7 +952,7 @@ n4_status_t n4_destroy(n4_context_t *c) {
   if (!c) return N4_OK;
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
-  for (DevBuf *b : {&c->imlog, &c->tables, &c->logu, &c->big, &c->red, &c->bar, &c->s1, &c->s2, &c->s3, &c->s4,
+  for (DevBuf *b : {&c->imlog, &c->tables, &c->big, &c->red, &c->bar, &c->s1, &c->s2, &c->s3, &c->s4,
                     &c->s5, &c->h_im, &c->h_mask, &c->h_out, &c->h_lat, &c->h_bias, &c->h_warm, &c->warm_x,
                     &c->warm_lat})
     b->release();

@@ -40,7 +40,10 @@ struct Plan {
   int o_fa, o_fb, o_tw, o_ff, o_red, o_misc;
   int sm_bytes;
   // big
-  int b_imlog, b_logu, b_G, b_Gd, b_T2, b_slotA, b_slotB, b_slotC, b_slice, big_bytes;
+  int b_imlog, b_G, b_Gd, b_T2, b_slotA, b_slotB, b_slotC, b_slice, big_bytes;
+  // cluster path: the FFT work buffers and the histogram copies live in the
+  // Gd region (dead from the end of pass A until the update) at these offsets
+  int alias_sharpen, a_fa, a_fb, a_hist;
 };
 
 struct Params {
@@ -54,7 +57,6 @@ struct Params {
 struct VolJob {
   int X, Y, Z;                  // fitting-resolution dimensions
   const float *imlog;           // [X*Y*Z] log intensity, NaN outside the mask
-  float *logu;                  // grid path: [X*Y*Z] scratch
   const float *warm;            // first-level lattice or nullptr
   float *lattice_out;           // final lattice
   n4_report_t *report;
@@ -128,7 +130,6 @@ struct Engine {
   int r0, nplane;
   FastDiv divZ;
   const float *imlog;
-  float *logu;
   // level
   int ncx, ncy, ncz, nlat;
   Axis ax, ay, az;
@@ -152,6 +153,10 @@ struct Engine {
     fa = (double2 *)(sm + pl.o_fa); fb = (double2 *)(sm + pl.o_fb); tw = (double2 *)(sm + pl.o_tw);
     Ff = (double *)(sm + pl.o_ff); red = (double *)(sm + pl.o_red);
     G = (float *)(big + pl.b_G); Gd = (float *)(big + pl.b_Gd); T2 = (float *)(big + pl.b_T2);
+    if (pl.alias_sharpen) {
+      fa = (double2 *)(big + pl.b_Gd + pl.a_fa); fb = (double2 *)(big + pl.b_Gd + pl.a_fb);
+      hist = (unsigned *)(big + pl.b_Gd + pl.a_hist);
+    }
     slotA = (Stats *)(big + pl.b_slotA); slotB = (unsigned long long *)(big + pl.b_slotB);
     slotC = (float *)(big + pl.b_slotC);
   }
@@ -273,7 +278,7 @@ struct Engine {
   //                 a fixed order
   //   T2[vx][cy][cz] y contraction over the CTA's rows of each x-plane
   //   slotC[c]       x contraction (the CTA's partial lattice)
-  __device__ void contract(bool num_mode) {
+  __device__ void contract(bool num_mode, const BinMap *bm = nullptr, bool degenerate = false) {
     float *T1 = Gd;   // Gd is dead between pass A and the next update
     const int nt1 = nrow * ncz;
     for (int t = threadIdx.x; t < nt1; t += blockDim.x) T1[t] = 0.0f;
@@ -287,10 +292,22 @@ struct Engine {
         const int lo = az.lo[sp], hi = az.hi[sp];
         float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
         if (num_mode) {
-          const float *rv = logu + (size_t)rl * Z;   // residuals (NaN outside the mask)
+          // residual R = logU - E(logU) of each masked voxel, with logU =
+          // im_log - eval(G) recomputed exactly as pass A computes it (every
+          // voxel of span sp evaluates the same 4 entries of its row of G)
+          const float *iv = imlog + (size_t)rl * Z;
+          const float *gr = G + rl * ncz + sp;
+          const float g0 = gr[0], g1 = gr[1], g2 = gr[2], g3 = gr[3];
           for (int vz = lo; vz < hi; ++vz) {
-            const float r = rv[vz];
-            if (isnan(r)) continue;
+            const float v = iv[vz];
+            if (isnan(v)) continue;
+            const float4 we = az.w[vz];
+            float b = __fmul_rn(we.x, g0);
+            b = __fmaf_rn(we.y, g1, b);
+            b = __fmaf_rn(we.z, g2, b);
+            b = __fmaf_rn(we.w, g3, b);
+            const float lu = __fsub_rn(v, b);
+            const float r = degenerate ? 0.0f : (float)((double)lu - sharpened_value(bm->coord(lu), E, pr.bins));
             const float4 w = W4[vz];
             a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
             a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
@@ -378,17 +395,17 @@ struct Engine {
     }
   }
 
-  // ---- pass A: logU, masked min/max and the previous update's CV sums
+  // ---- pass A: logU = im_log - eval(G) (not stored: the passes that need it
+  // recompute it bitwise), masked min/max and the previous update's CV sums
   __device__ bool pass_a(bool need_cv, double st[4]) {
     float vmin = INFINITY, vmax = -INFINITY;
     double sy = 0.0, syy = 0.0;
     const int n = nrow * Z;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const float v = imlog[i];
-      if (isnan(v)) continue;   // logu keeps NaN there (set when the volume starts)
+      if (isnan(v)) continue;   // outside the mask
       const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
       const float lu = __fsub_rn(v, eval(G, rl, vz));
-      logu[i] = lu;
       vmin = fminf(vmin, lu);
       vmax = fmaxf(vmax, lu);
       if (need_cv) {
@@ -423,8 +440,12 @@ struct Engine {
       int key = -1;
       unsigned qlo = 0, qhi = 0;
       if (i < n) {
-        const float lu = logu[i];
-        if (!isnan(lu)) key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
+        const float v = imlog[i];
+        if (!isnan(v)) {
+          const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
+          const float lu = __fsub_rn(v, eval(G, rl, vz));
+          key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
+        }
       }
       if (key >= 0) {
         atomicAdd(&hc[key], qlo);
@@ -452,18 +473,6 @@ struct Engine {
     return true;
   }
 
-  // ---- pass C: residual R = logU - remap(logU) in place (masked voxels only;
-  // the others stay NaN)
-  __device__ void pass_c(const BinMap &bm, bool degenerate) {
-    const int n = nrow * Z;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const float lu = logu[i];
-      if (isnan(lu)) continue;
-      logu[i] = degenerate ? 0.0f : (float)((double)lu - sharpened_value(bm.coord(lu), E, pr.bins));
-    }
-    __syncthreads();
-  }
-
   // ---- one sharpen + fit step from the current G; leaves the update in D
   __device__ bool fit_step(const double st[4]) {
     // bin range of the masked logU (N4.py:14-15); st holds FP32 values
@@ -472,9 +481,8 @@ struct Engine {
     const bool degenerate = !(slope > 0.0) || !isfinite(slope);
     const BinMap bm(bmin, degenerate ? 1.0 : slope, pr.bins);
     if (!degenerate) { if (!pass_b(bm)) return false; }
-    pass_c(bm, degenerate);
     N4_MARK(PH_C);
-    contract(true);
+    contract(true, &bm, degenerate);   // the residual is formed inside the z contraction
     __syncthreads();
     N4_MARK(PH_F_P);
     if (!allreduce(slotC, D, nlat)) return false;
@@ -495,7 +503,7 @@ struct Engine {
   }
 
   // ---- the whole volume
-  __device__ void run(const VolJob &job, const float *imlog_in, float *logu_in) {
+  __device__ void run(const VolJob &job, const float *imlog_in) {
     X = job.X; Y = job.Y; Z = job.Z;
     rank = g.rank(); K = g.size();
     const int rows = X * Y;
@@ -510,7 +518,6 @@ struct Engine {
     }
     divZ = FastDiv((unsigned)Z);
     imlog = imlog_in;
-    logu = logu_in;
     const bool lead = (rank == 0 && threadIdx.x == 0);
     n4_report_t *rep = job.report;
 
@@ -518,7 +525,6 @@ struct Engine {
     if (threadIdx.x == 0) ph_last = clock64();
 #endif
     fft_twiddles(tw, pl.npad);
-    for (int i = threadIdx.x; i < nrow * Z; i += blockDim.x) logu[i] = imlog[i];
     // foreground count of the group
     float cnt = 0.0f;
     double cntd = 0.0;

@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(NT, 1) k_n4_cluster(const __grid_constant__ Cl
       break;
     }
     Engine<ClusterGroup> e(g, s_pl, s_pr, sm, big, nullptr);
-    e.run(job, slab, (float *)(big + s_pl.b_logu));
+    e.run(job, slab);
   }
 }
 
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(NT, 1) k_n4_grid(const __grid_constant__ GridA
   int r0, r1;
   row_range(a.job.X * a.job.Y, g.rank(), g.size(), r0, r1);
   Engine<GridGroup> e(g, s_pl, s_pr, smem, big, a.red_global);
-  e.run(a.job, a.job.imlog + (size_t)r0 * a.job.Z, a.job.logu + (size_t)r0 * a.job.Z);
+  e.run(a.job, a.job.imlog + (size_t)r0 * a.job.Z);
 }
 
 // ------------------------------------------------------------------ tables

@@ -338,12 +338,13 @@ def test_batch_mixing_cluster_and_whole_gpu_volumes(cuda):
     on the cluster path, it on the whole-GPU path, each as in a single run;
     the autotuner's record keeps that split."""
     import n4b200
-    shapes = [(64, 64, 48), (288, 288, 288), (96, 80, 64)]
+    # fitting grids 32x32x24, 96x96x64 (more than a 16-CTA cluster holds), 48x40x32
+    shapes = [(64, 64, 48), (192, 192, 128), (96, 80, 64)]
     vols = []
     for i, sh in enumerate(shapes):
         ph = make_phantom(sh, seed=400 + i)
         vols.append((cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")))
-    p = param(3, [10] * 3, 0.001, ShrinkFactor=4)
+    p = param(3, [10] * 3, 0.001, ShrinkFactor=2)
     ctx = n4b200.Context()
     res = n4b200.N4Batch(vols, p, ctx=ctx)
     assert [r.report["path"] for r in res] == ["cluster", "grid", "cluster"]
