@@ -539,7 +539,7 @@ TuneKey tune_key(const n4_params_t *p, const std::vector<Dims> &vols) {
 n4_status_t choose_path(n4_context *ctx, const n4_params_t *p, const std::vector<Dims> &vols, bool batch,
                         Choice &c) {
   const Dims &d0 = vols[0];
-  c.nt = 1024;
+  c.nt = (p->flags & N4_FLAG_CTA_512) ? 512 : 1024;
   c.grid = false;
   c.K = 0;
   (void)d0;
@@ -559,7 +559,7 @@ n4_status_t choose_path(n4_context *ctx, const n4_params_t *p, const std::vector
     if (it != ctx->tune.end()) {
       c.grid = it->second.grid != 0;
       c.K = it->second.K;
-      c.nt = it->second.nt;
+      if (!(p->flags & N4_FLAG_CTA_512)) c.nt = it->second.nt;
       return N4_OK;
     }
   }
@@ -1095,8 +1095,9 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
                         n4_tune_report_t *report) {
   if (!ctx || !vols || n < 1) return fail(N4_ERR_INVALID_ARG, "bad batch");
   TRY(check_params(p));
-  if (p->flags & (N4_FLAG_FORCE_GRID | N4_FLAG_FORCE_CLUSTER | N4_FLAG_CLUSTER_SIZE(31)))
-    return fail(N4_ERR_INVALID_ARG, "autotuning chooses the path itself: clear the FORCE and cluster-size flags");
+  if (p->flags & (N4_FLAG_FORCE_GRID | N4_FLAG_FORCE_CLUSTER | N4_FLAG_CLUSTER_SIZE(31) | N4_FLAG_CTA_512))
+    return fail(N4_ERR_INVALID_ARG,
+                "autotuning chooses the path itself: clear the FORCE, cluster-size and thread flags");
   std::vector<RunVol> v(n);
   std::vector<Dims> dims(n);
   for (int i = 0; i < n; ++i) {
@@ -1125,11 +1126,16 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
     std::vector<Dims> sub;
     for (int i : fit) sub.push_back(dims[i]);
     Plan pl = make_plan(p, K, sub, false);
-    int cap = 0;
-    TRY(capacity(ctx, 1024, K, pl.sm_bytes + pl.big_bytes, &cap));
-    if (cap > 0) cand.push_back(Choice{false, K, 1024});
+    for (int nt : {1024, 512}) {
+      int cap = 0;
+      TRY(capacity(ctx, nt, K, pl.sm_bytes + pl.big_bytes, &cap));
+      if (cap > 0) cand.push_back(Choice{false, K, nt});
+    }
   }
-  if (n == 1) cand.push_back(Choice{true, 0, 1024});
+  if (n == 1) {
+    cand.push_back(Choice{true, 0, 1024});
+    cand.push_back(Choice{true, 0, 512});
+  }
   if ((int)cand.size() > N4_TUNE_MAX) cand.resize(N4_TUNE_MAX);
   cudaStream_t st = (cudaStream_t)stream;
   const int saved_prof = ctx->profiling;
@@ -1161,6 +1167,7 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
     ms /= kReps;
     const int k = rep.candidates++;
     rep.cluster_size[k] = ch.grid ? 0 : ch.K;
+    rep.threads[k] = ch.nt;
     rep.ms[k] = ms;
     if (best < 0 || ms < best_ms) { best = k; best_ms = ms; }
   }
@@ -1171,7 +1178,7 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
   if (best < 0) return fail(N4_ERR_TOO_LARGE, "no execution path fits these volumes");
   rep.chosen = best;
   const int K = rep.cluster_size[best];
-  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, 1024};
+  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, rep.threads[best]};
   if (report) *report = rep;
   return N4_OK;
 }

@@ -233,16 +233,55 @@ __device__ void stockham_pass(const double2 *x, double2 *y, int N, int Ns, const
   }
 }
 
-// Forward FFT of a (length N = 2^m, 4 <= N <= 4096).  Ping-pongs between a
-// and b; returns the buffer that holds the result.  Caller synchronised.
-__device__ double2 *fft_forward(double2 *a, double2 *b, int N, const double2 *tw) {
-  int Ns = 1;
-  int rem = N;
+template <int R> __device__ __forceinline__ void dft_r(double2 *v);
+template <> __device__ __forceinline__ void dft_r<2>(double2 *v) { dft2(v); }
+template <> __device__ __forceinline__ void dft_r<4>(double2 *v) { dft4(v[0], v[1], v[2], v[3]); }
+template <> __device__ __forceinline__ void dft_r<8>(double2 *v) { dft8(v); }
+
+// Largest radix used by the FFT passes (4: five passes for N = 512).
+#ifndef N4_FFT_MAX_RADIX
+#define N4_FFT_MAX_RADIX 4
+#endif
+__device__ __forceinline__ int fft_radix(int rem) {
+  return (N4_FFT_MAX_RADIX >= 8 && rem % 8 == 0) ? 8 : (rem % 4 == 0 ? 4 : 2);
+}
+
+// First Stockham pass (Ns = 1: every twiddle is 1) of an FFT whose input
+// x[i] = in(i) is produced on the fly, so that the elementwise step before an
+// FFT needs no pass and no barrier of its own.
+template <int R, class In>
+__device__ void stockham_first(const In &in, double2 *y, int N) {
+  const int T = N / R;
+  for (int j = threadIdx.x; j < T; j += blockDim.x) {
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = in(j + r * T);
+    dft_r<R>(v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) y[j * R + r] = v[r];
+  }
+}
+
+// Forward FFT (length N = 2^m, 4 <= N <= 4096) of in(0..N): first pass into
+// a, then the remaining passes ping-ponging a and b, each ending with a CTA
+// barrier.  Returns the buffer that holds the result.
+template <class In>
+__device__ double2 *fft_from(const In &in, double2 *a, double2 *b, int N, const double2 *tw) {
+  const int R0 = fft_radix(N);
+  if (R0 == 8) stockham_first<8>(in, a, N);
+  else if (R0 == 4) stockham_first<4>(in, a, N);
+  else stockham_first<2>(in, a, N);
+  __syncthreads();
+  int Ns = R0, rem = N / R0;
   while (rem > 1) {
-    if (rem % 4 == 0) { stockham_pass<4>(a, b, N, Ns, tw); Ns *= 4; rem /= 4; }
-    else { stockham_pass<2>(a, b, N, Ns, tw); Ns *= 2; rem /= 2; }
+    const int R = fft_radix(rem);
+    if (R == 8) stockham_pass<8>(a, b, N, Ns, tw);
+    else if (R == 4) stockham_pass<4>(a, b, N, Ns, tw);
+    else stockham_pass<2>(a, b, N, Ns, tw);
     __syncthreads();
     double2 *t = a; a = b; b = t;
+    Ns *= R;
+    rem /= R;
   }
   return a;
 }
@@ -254,54 +293,57 @@ struct SharpenBufs {
   double *Ff;        // [N] real Fourier transform of the Gaussian
 };
 
-// E[0..bins) from the fractional histogram H (N4.py:32-101, cudaN4.cu:733-817),
-// all in FP64.  H, E in shared memory; all threads of the CTA call it.
-__device__ void sharpen_map(const double *H, int bins, int N, int off, double binMin, double slope,
+// E[0..bins) from the fractional histogram (bin b's weight hv(b)) (N4.py:32-101,
+// cudaN4.cu:733-817), all in FP64; all threads of the CTA call it.  Four FFTs;
+// each elementwise step is folded into the first pass of the FFT after it.
+template <class HistF>
+__device__ void sharpen_map(const HistF &hv, int bins, int N, int off, double binMin, double slope,
                             double wiener, double fwhm, const SharpenBufs &sb, double *E) {
   const double ln2 = 0.69314718055994530942;
   const double scaledFWHM = fwhm / slope;
   const double expFactor = 4.0 * ln2 / (scaledFWHM * scaledFWHM);
   const double scaleFactor = 2.0 * sqrt(ln2 / 3.14159265358979323846) / scaledFWHM;
+  const double invN = 1.0 / (double)N;
   // z = V + i F : the padded histogram and the periodic Gaussian in one FFT
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    const int d = i <= N / 2 ? i : N - i;
-    const double F = scaleFactor * exp(-(double)d * (double)d * expFactor);
-    const double V = (i >= off && i < off + bins) ? H[i - off] : 0.0;
-    sb.a[i] = make_double2(V, F);
-  }
-  __syncthreads();
-  double2 *Z = fft_forward(sb.a, sb.b, N, sb.tw);
+  double2 *Z = fft_from(
+      [&](int i) {
+        const int d = i <= N / 2 ? i : N - i;
+        const double F = scaleFactor * exp(-(double)d * (double)d * expFactor);
+        const double V = (i >= off && i < off + bins) ? hv(i - off) : 0.0;
+        return make_double2(V, F);
+      },
+      sb.a, sb.b, N, sb.tw);
   double2 *W = (Z == sb.a) ? sb.b : sb.a;
-  // split the packed transform; Wiener filter Re(conj(Ff)/(|Ff|^2 + w)) with Ff real
-  for (int k = threadIdx.x; k < N; k += blockDim.x) {
-    const double2 zk = Z[k], zn = Z[(N - k) & (N - 1)];
-    const double2 Vf = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y - zn.y));
-    const double Ff = 0.5 * (zk.y + zn.y);
-    const double g = Ff / (Ff * Ff + wiener);
-    sb.Ff[k] = Ff;
-    W[k] = make_double2(Vf.x * g, -Vf.y * g);   // conj(Uf): inverse by conjugation
-  }
-  __syncthreads();
-  double2 *Y = fft_forward(W, Z, N, sb.tw);
+  // split the packed transform; Wiener filter Re(conj(Ff)/(|Ff|^2 + w)) with
+  // Ff real; conj(Uf), so that the forward FFT inverts
+  double2 *Y = fft_from(
+      [&](int k) {
+        const double2 zk = Z[k], zn = Z[(N - k) & (N - 1)];
+        const double2 Vf = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y - zn.y));
+        const double Ff = 0.5 * (zk.y + zn.y);
+        const double g = Ff / (Ff * Ff + wiener);
+        sb.Ff[k] = Ff;
+        return make_double2(Vf.x * g, -Vf.y * g);
+      },
+      W, Z, N, sb.tw);
   double2 *Y2 = (Y == W) ? Z : W;
   // U = max(Re(ifft(Uf)), 0); pack the numerator c_i U_i (real) and U (imaginary)
-  const double invN = 1.0 / (double)N;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    const double U = fmax(Y[i].x * invN, 0.0);
-    const double c = binMin + (double)(i - off) * slope;
-    Y2[i] = make_double2(c * U, U);
-  }
-  __syncthreads();
-  // Gaussian smoothing of both: multiply by the (real) Ff, inverse transform
-  double2 *P = fft_forward(Y2, Y, N, sb.tw);
+  double2 *P = fft_from(
+      [&](int i) {
+        const double U = fmax(Y[i].x * invN, 0.0);
+        const double c = binMin + (double)(i - off) * slope;
+        return make_double2(c * U, U);
+      },
+      Y2, Y, N, sb.tw);
   double2 *P2 = (P == Y2) ? Y : Y2;
-  for (int k = threadIdx.x; k < N; k += blockDim.x) {
-    const double2 v = P[k];
-    const double f = sb.Ff[k];
-    P2[k] = make_double2(v.x * f, -v.y * f);
-  }
-  __syncthreads();
-  double2 *S = fft_forward(P2, P, N, sb.tw);
+  // Gaussian smoothing of both: multiply by the (real) Ff, inverse transform
+  double2 *S = fft_from(
+      [&](int k) {
+        const double2 v = P[k];
+        const double f = sb.Ff[k];
+        return make_double2(v.x * f, -v.y * f);
+      },
+      P2, P, N, sb.tw);
   for (int b = threadIdx.x; b < bins; b += blockDim.x) {
     const double2 v = S[off + b];
     const double nu = v.x * invN, de = -v.y * invN;

@@ -341,6 +341,7 @@ struct Engine {
           if (sp < 0 || sp >= ay.nsp) continue;
           const int lo = max(ay.lo[sp], -rb), hi = min(ay.hi[sp], nrow - rb);
           const float *wy = PY + j * Y;
+#pragma unroll 4
           for (int vy = lo; vy < hi; ++vy) acc = __fmaf_rn(wy[vy], T1[(rb + vy) * ncz + cz], acc);
         }
         T2[t] = acc;
@@ -372,6 +373,7 @@ struct Engine {
         const int sp = cy - j;
         if (sp < 0 || sp >= ay.nsp) continue;
         const float *wy = PY + j * Y;
+#pragma unroll 4
         for (int vy = ay.lo[sp]; vy < ay.hi[sp]; ++vy) acc = __fmaf_rn(wy[vy], t1[vy * ncz], acc);
       }
       T2[t] = acc;
@@ -463,12 +465,12 @@ struct Engine {
     N4_MARK(PH_B_MERGE);
     if (!allreduce(slotB, H64, bins)) return false;
     N4_MARK(PH_B_RED);
-    const double inv = ldexp(1.0, -shift);
-    for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (double)H64[b] * inv;
-    __syncthreads();
     N4_MARK(PH_B);
+    const double inv = ldexp(1.0, -shift);
+    const unsigned long long *h64 = H64;
     SharpenBufs sb{fa, fb, tw, Ff};
-    sharpen_map(H, bins, pl.npad, pl.hoff, bm.binMin, bm.slope, pr.wiener, pr.fwhm, sb, E);
+    sharpen_map([=](int b) { return (double)h64[b] * inv; }, bins, pl.npad, pl.hoff, bm.binMin, bm.slope,
+                pr.wiener, pr.fwhm, sb, E);
     N4_MARK(PH_SHARP);
     return true;
   }

@@ -772,14 +772,14 @@ __global__ void k_sharpen(const unsigned long long *hist, const double *stats, i
   extern __shared__ __align__(16) char sm[];
   double2 *fa = (double2 *)sm, *fb = fa + npad, *tw = fb + npad;
   double *Ff = (double *)(tw + npad);
-  double *H = Ff + npad;
-  double *E = H + bins;
+  double *E = Ff + npad;
   fft_twiddles(tw, npad);
-  for (int b = threadIdx.x; b < bins; b += blockDim.x) H[b] = (double)hist[b] * ldexp(1.0, -shift);
   __syncthreads();
   if (stats[3] > 0.0) {
     SharpenBufs sb{fa, fb, tw, Ff};
-    sharpen_map(H, bins, npad, hoff, stats[0], stats[2], wiener, fwhm, sb, E);
+    const double inv = ldexp(1.0, -shift);
+    sharpen_map([=](int b) { return (double)hist[b] * inv; }, bins, npad, hoff, stats[0], stats[2], wiener, fwhm,
+                sb, E);
     for (int b = threadIdx.x; b < bins; b += blockDim.x) E_out[b] = E[b];
   } else {
     for (int b = threadIdx.x; b < bins; b += blockDim.x) E_out[b] = 0.0;

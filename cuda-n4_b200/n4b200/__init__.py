@@ -336,8 +336,9 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     """Time every execution configuration that fits these volumes
     (``n4_autotune``) and record the fastest in the context for later runs
     of volumes of the same sizes with the same lattice, levels and bins.
-    Returns ``{"candidates": [(cluster_size, ms), ...], "chosen": cluster_size}``
-    (cluster size 0 = whole-GPU path)."""
+    Returns ``{"candidates": [(cluster_size, threads, ms), ...], "chosen":
+    cluster_size, "chosen_threads": threads}`` (cluster size 0 = whole-GPU
+    path)."""
     torch = _torch()
     param = param or N4Param()
     cpar = param.to_c()
@@ -358,8 +359,8 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     c = ctx or Context.default(dev.index or 0)
     rep = _lib.n4_tune_report_t()
     check(_lib.load().n4_autotune(c.handle, C.byref(cpar), n, arr, _stream(dev), C.byref(rep)))
-    cands = [(int(rep.cluster_size[k]), float(rep.ms[k])) for k in range(rep.candidates)]
-    return {"candidates": cands, "chosen": cands[rep.chosen][0]}
+    cands = [(int(rep.cluster_size[k]), int(rep.threads[k]), float(rep.ms[k])) for k in range(rep.candidates)]
+    return {"candidates": cands, "chosen": cands[rep.chosen][0], "chosen_threads": cands[rep.chosen][1]}
 
 
 class N4BatchGraph:

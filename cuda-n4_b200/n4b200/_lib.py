@@ -18,6 +18,7 @@ STATUS = {
 }
 
 FLAG_CV_DDOF1 = 0x1
+FLAG_CTA_512 = 0x2000
 FLAG_FIT_ZERO_DEN = 0x2
 FLAG_INPLACE_THRESH = 0x4
 FLAG_FORCE_GRID = 0x8
@@ -67,12 +68,13 @@ class n4_volume_t(C.Structure):
     ]
 
 
-N4_TUNE_MAX = 8
+N4_TUNE_MAX = 16
 
 
 class n4_tune_report_t(C.Structure):
     _fields_ = [
-        ("candidates", C.c_int), ("cluster_size", C.c_int * N4_TUNE_MAX), ("ms", C.c_float * N4_TUNE_MAX),
+        ("candidates", C.c_int), ("cluster_size", C.c_int * N4_TUNE_MAX), ("threads", C.c_int * N4_TUNE_MAX),
+        ("ms", C.c_float * N4_TUNE_MAX),
         ("chosen", C.c_int),
     ]
 

@@ -48,6 +48,9 @@ typedef enum {
  * overriding the autotuner; N4_ERR_TOO_LARGE when a volume's share does not
  * fit one CTA's shared memory.  0 = choose automatically. */
 #define N4_FLAG_CLUSTER_SIZE(k) (((unsigned int)(k) & 31u) << 8)
+/* Bit 13: 512 threads per CTA instead of 1024 (twice the registers per
+ * thread); overrides the autotuner's choice of threads. */
+#define N4_FLAG_CTA_512         0x2000u
 
 /* Mirrors N4Param (cudaN4.h:24-94).  Obtain defaults from n4_params_default. */
 typedef struct {
@@ -157,16 +160,18 @@ n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *graph);
  * n4_autotune runs the given volumes once per execution configuration that
  * fits them: thread-block clusters of 16, 12, 8, 6, 4 and 2 CTAs per volume
  * (a cluster keeps its volume in shared memory; smaller clusters run more
- * volumes side by side) and, for a single volume, the whole-GPU path.  It
+ * volumes side by side) and, for a single volume, the whole-GPU path, each
+ * with 1024 and with 512 threads per CTA.  It
  * records the fastest in the context under the key (lattice, levels, bins,
  * fitting-grid size of every volume, in order); later n4_run,
  * n4_run_batched and n4_batch_graph_create calls with the same key use it
  * unless a FORCE flag is set.  The outputs of the volumes are written as by
  * a run.  Synchronous. */
-#define N4_TUNE_MAX 8
+#define N4_TUNE_MAX 16
 typedef struct {
   int candidates;                  /* configurations timed                   */
   int cluster_size[N4_TUNE_MAX];   /* CTAs per volume; 0 = whole-GPU path    */
+  int threads[N4_TUNE_MAX];        /* threads per CTA                        */
   float ms[N4_TUNE_MAX];           /* device time of one run of the volumes  */
   int chosen;                      /* index of the configuration recorded    */
 } n4_tune_report_t;

@@ -114,6 +114,9 @@ def test_cluster_and_grid_paths_agree(cuda):
     # different partitions sum in different orders; N4 amplifies the FP32
     # difference (~2e-5 here), so the paths are compared at the parity bound
     assert nrel(a.lattice, b.lattice.cpu().numpy().astype(np.float64)) < TOL
+    c = n4b200.N4(im, mk, param(3, [10] * 3, 0.0, flags=0x8 | n4b200._lib.FLAG_CTA_512))
+    assert c.report["path"] == "grid"
+    assert nrel(c.lattice, b.lattice.cpu().numpy().astype(np.float64)) < TOL
 
 
 def test_deterministic(cuda):
@@ -295,10 +298,12 @@ def test_autotune_records_the_fastest_configuration(cuda):
     ref = n4b200.N4Batch(vols, p, ctx=ctx)
     assert all(q.report["cluster_size"] == 16 for q in ref)       # untuned: the largest cluster
     t = n4b200.autotune(vols, p, ctx=ctx)
-    sizes = [k for k, _ in t["candidates"]]
-    assert len(sizes) >= 2 and 16 in sizes
-    assert all(ms > 0 for _, ms in t["candidates"])
-    assert t["chosen"] == min(t["candidates"], key=lambda c: c[1])[0]
+    sizes = [k for k, _, _ in t["candidates"]]
+    assert len(sizes) >= 4 and 16 in sizes
+    assert {nt for _, nt, _ in t["candidates"]} == {512, 1024}
+    assert all(ms > 0 for _, _, ms in t["candidates"])
+    best = min(t["candidates"], key=lambda c: c[2])
+    assert (t["chosen"], t["chosen_threads"]) == (best[0], best[1])
     res = n4b200.N4Batch(vols, p, ctx=ctx)
     for r in res:
         assert r.report["status"] == "N4_OK"
@@ -310,9 +315,9 @@ def test_autotune_records_the_fastest_configuration(cuda):
 
 
 def test_every_cluster_size_matches_the_oracle(cuda):
-    """Cluster sizes 16 .. 2 (every size whose per-CTA share fits: at
-    256x256x176 only 16 does) on a 128x128x96 phantom at shrink 4 against
-    the FP64 oracle, fixed iterations."""
+    """Cluster sizes 16 .. 2 (every size whose per-CTA share fits), with 1024
+    and 512 threads per CTA, on a 128x128x96 phantom at shrink 4 against the
+    FP64 oracle, fixed iterations."""
     import n4b200
     ph = make_phantom((128, 128, 96), seed=4, sigma=0.02, grid=6, coeff_std=0.25)
     im, mk = cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")
@@ -320,17 +325,18 @@ def test_every_cluster_size_matches_the_oracle(cuda):
                              maximumNumberOfIterations=[8] * 4, ConvergenceThreshold=0.0, return_log_bias=True)
     ran = []
     for K in (16, 12, 8, 6, 4, 2):
-        pk = param(4, [8] * 4, 0.0, ShrinkFactor=4, flags=n4b200.cluster_size_flag(K))
-        try:
-            res = n4b200.N4(im, mk, pk)
-        except n4b200.N4Error as e:
-            assert "N4_ERR_TOO_LARGE" in str(e)
-            continue
-        assert res.report["cluster_size"] == K
-        assert nrel(res.lattice, lat) < TOL, K
-        assert nrel(res.im_normalized, out) < TOL, K
-        ran.append(K)
-    assert len(ran) >= 4, ran
+        for threads_flag in (0, n4b200._lib.FLAG_CTA_512):
+            pk = param(4, [8] * 4, 0.0, ShrinkFactor=4, flags=n4b200.cluster_size_flag(K) | threads_flag)
+            try:
+                res = n4b200.N4(im, mk, pk)
+            except n4b200.N4Error as e:
+                assert "N4_ERR_TOO_LARGE" in str(e)
+                continue
+            assert res.report["cluster_size"] == K
+            assert nrel(res.lattice, lat) < TOL, (K, threads_flag)
+            assert nrel(res.im_normalized, out) < TOL, (K, threads_flag)
+            ran.append((K, threads_flag))
+    assert len(ran) >= 8, ran
 
 
 def test_batch_mixing_cluster_and_whole_gpu_volumes(cuda):
