@@ -51,9 +51,9 @@ ITER_BYTES_PER_VOXEL = 27
 # final correction: read im 4 + write corrected 4 per full-resolution voxel
 CORRECT_BYTES_PER_VOXEL = 8
 # DRAM bytes (read + write) of one k_n4_cluster launch per volume of this
-# workload, from an ncu capture of a 4-volume launch (5.677 MB read + 27.6 KB
+# workload, from an ncu capture of a 4-volume launch (3.323 MB read, nothing
 # written): the volume stays in shared memory, so only its initial load moves
-TRAFFIC_PER_VOLUME = (5.677056e6 + 27.648e3) / 4
+TRAFFIC_PER_VOLUME = 3.323392e6 / 4
 
 
 def workload_desc(batch):

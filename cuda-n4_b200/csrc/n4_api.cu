@@ -1115,6 +1115,14 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
   CK(cudaSetDevice(ctx->device));
   // candidates: every cluster size whose per-CTA share of every volume fits,
   // and the whole-GPU path for a single volume
+  // a size that leaves more volumes to the whole-GPU path than another size
+  // does cannot be faster: only sizes that keep the most volumes on clusters
+  size_t most = 0;
+  for (int K : {16, 12, 8, 6, 4, 2}) {
+    std::vector<int> all(n);
+    for (int i = 0; i < n; ++i) all[i] = i;
+    most = std::max(most, cluster_subset(ctx, p, dims, all, K, nullptr).size());
+  }
   std::vector<Choice> cand;
   for (int K : {16, 12, 8, 6, 4, 2}) {
     // the volumes whose per-CTA share fits this cluster size (the others
@@ -1122,7 +1130,7 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
     std::vector<int> all(n);
     for (int i = 0; i < n; ++i) all[i] = i;
     const std::vector<int> fit = cluster_subset(ctx, p, dims, all, K, nullptr);
-    if (fit.empty()) continue;
+    if (fit.empty() || fit.size() < most) continue;
     std::vector<Dims> sub;
     for (int i : fit) sub.push_back(dims[i]);
     Plan pl = make_plan(p, K, sub, false);
