@@ -445,34 +445,42 @@ def run_ours(args, rank, world, local_rank):
         n4b200.autotune(dev_in[:per], p, ctx=c2)
     encs = [load_encoder(max_batch=per) for _ in range(3)]      # one per stream: an encoder serves one run at a time
 
-    def step_e2e():
+    def step_e2e(host, dev_vols):
         for k in range(nsub):
             st = streams[k % 3]
             sl = slice(k * per, (k + 1) * per)
             with torch.cuda.stream(st):
-                for (ih, mh), (idv, mdv) in zip(vols_host[sl], dev_in[sl]):
+                for (ih, mh), (idv, mdv) in zip(host[sl], dev_vols[sl]):
                     idv.copy_(ih, non_blocking=True)
                     mdv.copy_(mh, non_blocking=True)
-                rs = n4b200.N4Batch(dev_in[sl], p, ctx=ctxs[k % 3], synchronous=False, encoder=encs[k % 3])
+                rs = n4b200.N4Batch(dev_vols[sl], p, ctx=ctxs[k % 3], synchronous=False, encoder=encs[k % 3])
                 for r, o, l in zip(rs, out_h[sl], lat_h[sl]):
                     o.copy_(r.im_normalized, non_blocking=True)
                     l.copy_(r.lattice, non_blocking=True)
 
-    for _ in range(min(args.warmup, 2)):
-        step_e2e()
-    barrier()
-    e0.record(stream)
-    for s2 in streams:
-        s2.wait_event(e0)
-    for _ in range(args.steps):
-        step_e2e()
-    for s2 in streams:
-        ev = torch.cuda.Event()
-        ev.record(s2)
-        stream.wait_event(ev)
-    e1.record(stream)
-    barrier()
-    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    def time_e2e(host, dev_vols):
+        for _ in range(min(args.warmup, 2)):
+            step_e2e(host, dev_vols)
+        barrier()
+        e0.record(stream)
+        for s2 in streams:
+            s2.wait_event(e0)
+        for _ in range(args.steps):
+            step_e2e(host, dev_vols)
+        for s2 in streams:
+            ev = torch.cuda.Event()
+            ev.record(s2)
+            stream.wait_event(ev)
+        e1.record(stream)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    ms_e2e = time_e2e(vols_host, dev_in)
+    # the same with byte masks (N4_FLAG_MASK_U8): 1 B instead of 4 B per mask voxel over PCIe
+    host_u8 = [(ih, (mh != 0).to(torch.uint8).pin_memory()) for ih, mh in vols_host]
+    dev_u8 = [(idv, torch.empty(mh.shape, dtype=torch.uint8, device=dev)) for (idv, _), (_, mh) in zip(dev_in, host_u8)]
+    ms_e2e_u8 = time_e2e(host_u8, dev_u8)
+    h2d_u8 = sum(a.numel() * 4 + b.numel() for a, b in host_u8)
     h2d = sum(a.numel() * 4 + b.numel() * 4 for a, b in vols_host)
     d2h = sum(o.numel() * 4 for o in out_h) + sum(l.numel() * 4 for l in lat_h)
 
@@ -497,6 +505,9 @@ def run_ours(args, rank, world, local_rank):
         },
         "e2e": {"value": world * B * args.steps / (ms_e2e / 1000.0), "unit": "volumes/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e_byte_masks": {"value": world * B * args.steps / (ms_e2e_u8 / 1000.0), "unit": "volumes/s",
+                           "h2d_bytes_per_step": h2d_u8, "d2h_bytes_per_step": d2h,
+                           "path": "same as e2e with uint8 masks (N4_FLAG_MASK_U8)"},
         "gpu_launches": t_w["launches"] * args.steps,
         "clocks": clk,
         "plain": {"value": plain, "unit": "volumes/s", "ms_per_volume": ms_plain / (args.steps * B),

@@ -444,10 +444,12 @@ n4_status_t prof_mark(n4_context *ctx, int k, cudaStream_t st) {
 
 // ------------------------------------------------------------------ the run
 struct RunVol {
-  const float *im, *mask;
+  const float *im;
+  const void *mask;            // float or byte (N4_FLAG_MASK_U8)
   float *out, *lat, *bias;
   const float *warm;
-  float *im_w, *mask_w;
+  float *im_w;
+  void *mask_w;
   Dims d;
 };
 
@@ -715,7 +717,7 @@ void fill_descriptors(n4_context *ctx, const n4_params_t *p, Prepared &P, const 
     const Dims &d = P.dims[i];
     float *il = (float *)(ctx->imlog.as<char>() + P.imlog_off[i]);
     pv[i] = PrologueVol{r.im, r.mask, r.im_w, r.mask_w, d.FX, d.FY, d.FZ, (int)p->ShrinkFactor,
-                        d.X, d.Y, d.Z, il, fit_total};
+                        d.X, d.Y, d.Z, il, fit_total, (p->flags & N4_FLAG_MASK_U8) ? 1 : 0};
     pst[i] = fit_total;
     fit_total += (long long)d.X * d.Y * d.Z;
     jb[i] = VolJob{d.X, d.Y, d.Z, il, r.warm, r.lat, B.dp<n4_report_t>(P.o_rep) + i};
@@ -770,7 +772,7 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
         const long long nf = (long long)P.dims[i].FX * P.dims[i].FY * P.dims[i].FZ;
         if (P.rvs[i].im_w) {
           k_threshold_inplace<<<(int)std::min<long long>((nf + 255) / 256, ctx->nsm * 16LL), 256, 0, st>>>(
-              P.rvs[i].im_w, P.rvs[i].mask_w, nf, p->low_value);
+              P.rvs[i].im_w, P.rvs[i].mask_w, (p->flags & N4_FLAG_MASK_U8) ? 1 : 0, nf, p->low_value);
           ++launches;
           CK(cudaGetLastError());
         }
@@ -1074,7 +1076,8 @@ n4_status_t n4_warm_inputs(n4_context_t *ctx, const n4_params_t *p, int n, const
     const Dims &d = v[i].d;
     float *il = (float *)(ctx->imlog.as<char>() + P.imlog_off[i]);
     B.hp<PrologueVol>(P.o_pro)[i] = PrologueVol{v[i].im, v[i].mask, nullptr, nullptr, d.FX, d.FY, d.FZ,
-                                                (int)p->ShrinkFactor, d.X, d.Y, d.Z, il, fit_total};
+                                                (int)p->ShrinkFactor, d.X, d.Y, d.Z, il, fit_total,
+                                                (p->flags & N4_FLAG_MASK_U8) ? 1 : 0};
     B.hp<long long>(P.o_pst)[i] = fit_total;
     B.hp<PoolJob>(P.o_pool)[i] = PoolJob{il, d.X, d.Y, d.Z};
     fit_total += (long long)d.X * d.Y * d.Z;
@@ -1230,12 +1233,13 @@ n4_status_t n4_run_host(n4_context_t *ctx, const n4_params_t *p, const float *h_
   TRY(ctx->h_im.ensure(nv * 4, "input"));
   TRY(ctx->h_out.ensure(nv * 4, "output"));
   TRY(ctx->h_lat.ensure(nlat * 4, "lattice"));
-  if (h_mask) TRY(ctx->h_mask.ensure(nv * 4, "mask"));
+  const size_t mask_bytes = nv * ((p->flags & N4_FLAG_MASK_U8) ? 1 : 4);
+  if (h_mask) TRY(ctx->h_mask.ensure(mask_bytes, "mask"));
   if (h_bias_field) TRY(ctx->h_bias.ensure(nv * 4, "bias"));
   if (h_warm_lattice) TRY(ctx->h_warm.ensure(nwarm * 4, "warm lattice"));
   cudaStream_t st = nullptr;
   CK(cudaMemcpyAsync(ctx->h_im.p, h_im, nv * 4, cudaMemcpyHostToDevice, st));
-  if (h_mask) CK(cudaMemcpyAsync(ctx->h_mask.p, h_mask, nv * 4, cudaMemcpyHostToDevice, st));
+  if (h_mask) CK(cudaMemcpyAsync(ctx->h_mask.p, h_mask, mask_bytes, cudaMemcpyHostToDevice, st));
   if (h_warm_lattice) CK(cudaMemcpyAsync(ctx->h_warm.p, h_warm_lattice, nwarm * 4, cudaMemcpyHostToDevice, st));
   n4_report_t rep;
   n4_status_t s = n4_run(ctx, p, ctx->h_im.as<float>(), h_mask ? ctx->h_mask.as<float>() : nullptr, fx, fy, fz,

@@ -22,13 +22,24 @@ namespace n4 {
 
 // ------------------------------------------------------------------ prologue
 struct PrologueVol {
-  const float *im, *mask;   // full resolution (mask may be null)
-  float *im_w, *mask_w;     // optional in-place threshold write-back
+  const float *im;          // full resolution
+  const void *mask;         // float or byte mask (mask_u8), may be null
+  float *im_w;              // optional in-place threshold write-back
+  void *mask_w;             //   (the mask in its own type)
   int FX, FY, FZ, s;        // full dims, shrink
   int X, Y, Z;              // fitting dims
   float *imlog;             // [X*Y*Z]
   long long start;          // first fitting voxel of this volume in the batch
+  int mask_u8;              // mask and mask_w hold uint8_t
 };
+
+__device__ __forceinline__ bool mask_on(const void *m, int u8, long long i) {
+  return u8 ? ((const unsigned char *)m)[i] != 0 : ((const float *)m)[i] != 0.0f;
+}
+__device__ __forceinline__ void mask_clear(void *m, int u8, long long i) {
+  if (u8) ((unsigned char *)m)[i] = 0;
+  else ((float *)m)[i] = 0.0f;
+}
 
 __device__ __forceinline__ int find_volume(const long long *starts, int n, long long gi) {
   int lo = 0, hi = n - 1;
@@ -48,10 +59,10 @@ __global__ void k_prologue(const PrologueVol *vols, const long long *starts, int
     float out;
     if (s == 1) {
       const float val = P.im[li];
-      const bool m = (P.mask ? P.mask[li] != 0.0f : true) && val > low;
+      const bool m = (P.mask ? mask_on(P.mask, P.mask_u8, li) : true) && val > low;
       if (m && !isfinite(val)) atomicExch(flag_nonfinite, 1);
       out = m ? logf(val) : __int_as_float(0x7fc00000);
-      if (P.im_w && !(val > low)) { P.im_w[li] = 0.0f; if (P.mask_w) P.mask_w[li] = 0.0f; }
+      if (P.im_w && !(val > low)) { P.im_w[li] = 0.0f; if (P.mask_w) mask_clear(P.mask_w, P.mask_u8, li); }
     } else {
       float sum = 0.0f;
       int cnt = 0;
@@ -60,7 +71,7 @@ __global__ void k_prologue(const PrologueVol *vols, const long long *starts, int
           const long long rowb = ((long long)(x * s + dx) * P.FY + (y * s + dy)) * P.FZ + (long long)z * s;
           for (int dz = 0; dz < s; ++dz) {
             const float val = P.im[rowb + dz];
-            const bool m = (P.mask ? P.mask[rowb + dz] != 0.0f : true) && val > low;
+            const bool m = (P.mask ? mask_on(P.mask, P.mask_u8, rowb + dz) : true) && val > low;
             if (m) { sum += val; ++cnt; if (!isfinite(val)) atomicExch(flag_nonfinite, 1); }
           }
         }
@@ -72,10 +83,10 @@ __global__ void k_prologue(const PrologueVol *vols, const long long *starts, int
 }
 
 // In-place threshold of the caller's full-resolution buffers (shrink > 1).
-__global__ void k_threshold_inplace(float *im, float *mask, long long n, float low) {
+__global__ void k_threshold_inplace(float *im, void *mask, int mask_u8, long long n, float low) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    if (!(im[i] > low)) { im[i] = 0.0f; if (mask) mask[i] = 0.0f; }
+    if (!(im[i] > low)) { im[i] = 0.0f; if (mask) mask_clear(mask, mask_u8, i); }
   }
 }
 

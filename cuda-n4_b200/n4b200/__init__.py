@@ -191,6 +191,31 @@ def _dev_f32(x, device=None):
     return t.contiguous()
 
 
+def _dev_mask(m, device=None):
+    """CUDA mask tensor and whether it is a byte mask: bool/uint8 input stays
+    one byte per voxel (``N4_FLAG_MASK_U8``), anything else becomes float32."""
+    torch = _torch()
+    if m is None:
+        return None, None
+    if isinstance(m, torch.Tensor):
+        t = m if m.is_cuda else m.to(device or "cuda")
+        if t.dtype in (torch.uint8, torch.bool):
+            return t.to(torch.uint8).contiguous(), True
+        return (t if t.dtype == torch.float32 else t.float()).contiguous(), False
+    a = np.asarray(m)
+    if a.dtype in (np.uint8, np.bool_):
+        return torch.from_numpy(np.ascontiguousarray(a.astype(np.uint8))).to(device or "cuda"), True
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(device or "cuda"), False
+
+
+def _mask_flag(kinds) -> int:
+    """N4_FLAG_MASK_U8 when the (non-None) masks of a call are byte masks."""
+    k = {x for x in kinds if x is not None}
+    if len(k) > 1:
+        raise ValueError("the masks of one call must all be byte masks or all float masks")
+    return _lib.FLAG_MASK_U8 if k == {True} else 0
+
+
 def _ptr(t) -> Optional[int]:
     return None if t is None else t.data_ptr()
 
@@ -225,8 +250,8 @@ def N4(im, mask=None, param: Optional[N4Param] = None, warm_lattice=None, return
        ctx: Optional[Context] = None, synchronous: bool = True) -> N4Result:
     """Bias-correct one volume.
 
-    ``im``/``mask``: float32 ``[fx][fy][fz]`` (mask != 0 is foreground; None
-    = every voxel).  CUDA tensors run on their device and stream; numpy arrays
+    ``im``/``mask``: float32 ``[fx][fy][fz]`` (mask != 0 is foreground; a
+    bool/uint8 mask is passed as bytes; None = every voxel).  CUDA tensors run on their device and stream; numpy arrays
     take the host path (``n4_run_host``).  Returns the corrected volume, the
     final control lattice and, with ``return_bias``, ``exp(log bias)``.
     """
@@ -239,7 +264,8 @@ def N4(im, mask=None, param: Optional[N4Param] = None, warm_lattice=None, return
     if _is_cuda(im):
         torch = _torch()
         imt = _dev_f32(im)
-        mk = None if mask is None else _dev_f32(mask, imt.device)
+        mk, u8 = _dev_mask(mask, imt.device)
+        cpar.flags |= _mask_flag([u8])
         wl = None if warm_lattice is None else _dev_f32(warm_lattice, imt.device)
         out = torch.empty_like(imt)
         lat = torch.empty(dims, dtype=torch.float32, device=imt.device)
@@ -250,7 +276,14 @@ def N4(im, mask=None, param: Optional[N4Param] = None, warm_lattice=None, return
         check(st)
         return N4Result(out, lat, bias, _report_dict(rep) if synchronous else {})
     imh = np.ascontiguousarray(np.asarray(im, dtype=np.float32))
-    mkh = None if mask is None else np.ascontiguousarray(np.asarray(mask, dtype=np.float32))
+    mkh = None
+    if mask is not None:
+        ma = np.asarray(mask)
+        if ma.dtype in (np.uint8, np.bool_):
+            mkh = np.ascontiguousarray(ma.astype(np.uint8))
+            cpar.flags |= _lib.FLAG_MASK_U8
+        else:
+            mkh = np.ascontiguousarray(ma, dtype=np.float32)
     wlh = None if warm_lattice is None else np.ascontiguousarray(np.asarray(warm_lattice, dtype=np.float32))
     out = np.empty_like(imh)
     lat = np.empty(dims, dtype=np.float32)
@@ -272,6 +305,7 @@ def N4Batch(volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=No
     torch = _torch()
     param = param or N4Param()
     cpar = param.to_c()
+    kinds = []
     dims = lattice_dims(param)
     n = len(volumes)
     arr = (n4_volume_t * n)()
@@ -280,7 +314,8 @@ def N4Batch(volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=No
     for i, (im, mask) in enumerate(volumes):
         imt = _dev_f32(im)
         dev = imt.device
-        mk = None if mask is None else _dev_f32(mask, dev)
+        mk, u8 = _dev_mask(mask, dev)
+        kinds.append(u8)
         wl = None if warm_lattices is None or warm_lattices[i] is None else _dev_f32(warm_lattices[i], dev)
         out = torch.empty_like(imt)
         lat = torch.empty(dims, dtype=torch.float32, device=dev)
@@ -289,6 +324,7 @@ def N4Batch(volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=No
         fx, fy, fz = (int(d) for d in imt.shape)
         arr[i] = n4_volume_t(_ptr(imt), _ptr(mk), fx, fy, fz, _ptr(out), _ptr(lat), _ptr(bias), _ptr(wl))
         results.append(N4Result(out, lat, bias, {}))
+    cpar.flags |= _mask_flag(kinds)
     reps = (n4_report_t * n)()
     c = ctx or Context.default(dev.index or 0)
     if encoder is not None:
@@ -310,6 +346,7 @@ def warm_inputs(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optiona
     torch = _torch()
     param = param or N4Param()
     cpar = param.to_c()
+    kinds = []
     n = len(volumes)
     arr = (n4_volume_t * n)()
     keep = []
@@ -317,10 +354,12 @@ def warm_inputs(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optiona
     for i, (im, mask) in enumerate(volumes):
         imt = _dev_f32(im)
         dev = imt.device
-        mk = None if mask is None else _dev_f32(mask, dev)
+        mk, u8 = _dev_mask(mask, dev)
+        kinds.append(u8)
         keep += [imt, mk]
         fx, fy, fz = (int(d) for d in imt.shape)
         arr[i] = n4_volume_t(_ptr(imt), _ptr(mk), fx, fy, fz, None, None, None, None)
+    cpar.flags |= _mask_flag(kinds)
     x = torch.empty((n, 32, 32, 24), dtype=torch.bfloat16, device=dev)
     c = ctx or Context.default(dev.index or 0)
     check(_lib.load().n4_warm_inputs(c.handle, C.byref(cpar), n, arr, x.data_ptr(), _stream(dev)))
@@ -342,6 +381,7 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     torch = _torch()
     param = param or N4Param()
     cpar = param.to_c()
+    kinds = []
     dims = lattice_dims(param)
     n = len(volumes)
     arr = (n4_volume_t * n)()
@@ -350,12 +390,14 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     for i, (im, mask) in enumerate(volumes):
         imt = _dev_f32(im)
         dev = imt.device
-        mk = None if mask is None else _dev_f32(mask, dev)
+        mk, u8 = _dev_mask(mask, dev)
+        kinds.append(u8)
         out = torch.empty_like(imt)
         lat = torch.empty(dims, dtype=torch.float32, device=dev)
         keep += [imt, mk, out, lat]
         fx, fy, fz = (int(d) for d in imt.shape)
         arr[i] = n4_volume_t(_ptr(imt), _ptr(mk), fx, fy, fz, _ptr(out), _ptr(lat), None, None)
+    cpar.flags |= _mask_flag(kinds)
     c = ctx or Context.default(dev.index or 0)
     rep = _lib.n4_tune_report_t()
     check(_lib.load().n4_autotune(c.handle, C.byref(cpar), n, arr, _stream(dev), C.byref(rep)))
@@ -374,6 +416,7 @@ class N4BatchGraph:
         torch = _torch()
         param = param or N4Param()
         self._cpar = param.to_c()
+        kinds = []
         dims = lattice_dims(param)
         n = len(volumes)
         arr = (n4_volume_t * n)()
@@ -382,7 +425,8 @@ class N4BatchGraph:
         for i, (im, mask) in enumerate(volumes):
             imt = _dev_f32(im)
             dev = imt.device
-            mk = None if mask is None else _dev_f32(mask, dev)
+            mk, u8 = _dev_mask(mask, dev)
+            kinds.append(u8)
             wl = None if warm_lattices is None or warm_lattices[i] is None else _dev_f32(warm_lattices[i], dev)
             out = torch.empty_like(imt)
             lat = torch.empty(dims, dtype=torch.float32, device=dev)
@@ -391,6 +435,7 @@ class N4BatchGraph:
             fx, fy, fz = (int(d) for d in imt.shape)
             arr[i] = n4_volume_t(_ptr(imt), _ptr(mk), fx, fy, fz, _ptr(out), _ptr(lat), _ptr(bias), _ptr(wl))
             self.results.append(N4Result(out, lat, bias, {}))
+        self._cpar.flags |= _mask_flag(kinds)
         self.inputs = [(self._keep[3 * i], self._keep[3 * i + 1]) for i in range(n)]
         self.ctx = ctx or Context.default(dev.index or 0)
         self.device = dev

@@ -19,6 +19,7 @@ STATUS = {
 
 FLAG_CV_DDOF1 = 0x1
 FLAG_CTA_512 = 0x2000
+FLAG_MASK_U8 = 0x4000
 FLAG_FIT_ZERO_DEN = 0x2
 FLAG_INPLACE_THRESH = 0x4
 FLAG_FORCE_GRID = 0x8

@@ -4,8 +4,8 @@
  * C ABI.  Plain pointers and sizes only; every call returns an n4_status_t
  * and never exits or traps.  Volumes are float32, row-major [fx][fy][fz]
  * with fz fastest, exactly the layout of the reference N4 (cudaN4.cu:476).
- * A mask voxel is foreground when it is non-zero (float masks, as in the
- * reference) or when its byte is non-zero (uint8 masks).
+ * A mask voxel is foreground when it is non-zero: float masks as in the
+ * reference, or byte masks (uint8_t, with N4_FLAG_MASK_U8).
  *
  * Device-pointer calls are asynchronous on the given stream (NULL = the
  * legacy default stream) unless a report is requested; host-pointer calls
@@ -51,6 +51,11 @@ typedef enum {
 /* Bit 13: 512 threads per CTA instead of 1024 (twice the registers per
  * thread); overrides the autotuner's choice of threads. */
 #define N4_FLAG_CTA_512         0x2000u
+/* Bit 14: every mask pointer of a run (n4_run, n4_run_host, n4_run_batched*,
+ * n4_batch_graph_create*, n4_warm_inputs, n4_autotune) points to uint8_t
+ * bytes, one per voxel, non-zero = foreground, instead of floats (a quarter of
+ * the bytes to move; the component entry points take float masks). */
+#define N4_FLAG_MASK_U8         0x4000u
 
 /* Mirrors N4Param (cudaN4.h:24-94).  Obtain defaults from n4_params_default. */
 typedef struct {

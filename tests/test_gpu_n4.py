@@ -364,3 +364,39 @@ def test_batch_mixing_cluster_and_whole_gpu_volumes(cuda):
     assert tuned[1].report["path"] == "grid"
     assert all(r.report["cluster_size"] == t["chosen"] for r in (tuned[0], tuned[2]))
     ctx.close()
+
+
+def test_byte_masks_match_float_masks(cuda):
+    """N4_FLAG_MASK_U8: a uint8 mask gives bitwise the float mask's result on
+    every entry point that takes a run's masks (single, host, batched, graph,
+    warm inputs), and the in-place threshold clears its bytes."""
+    import n4b200
+    ph = make_phantom((64, 64, 48), seed=21)
+    im = cuda.tensor(ph.im, device="cuda")
+    mf = cuda.tensor(ph.mask, device="cuda")
+    mb = (mf != 0).to(cuda.uint8)
+    p = param(2, [6, 6], 0.001, ShrinkFactor=2)
+    a, b = n4b200.N4(im, mf, p), n4b200.N4(im, mb, p)
+    assert cuda.equal(a.lattice, b.lattice) and cuda.equal(a.im_normalized, b.im_normalized)
+    h = n4b200.N4(ph.im, (ph.mask != 0).astype(np.uint8), p)
+    assert np.array_equal(h.lattice, a.lattice.cpu().numpy())
+    ra = n4b200.N4Batch([(im, mf), (im * 1.5, mf)], p)
+    rb = n4b200.N4Batch([(im, mb), (im * 1.5, mb)], p)
+    for x, y in zip(ra, rb):
+        assert cuda.equal(x.lattice, y.lattice) and cuda.equal(x.im_normalized, y.im_normalized)
+    g = n4b200.N4BatchGraph([(im, mb)], p)
+    g.launch()
+    assert cuda.equal(g.sync()[0].lattice, a.lattice)
+    g.close()
+    assert cuda.equal(n4b200.warm_inputs([(im, mf)], p), n4b200.warm_inputs([(im, mb)], p))
+    with pytest.raises(ValueError):
+        n4b200.N4Batch([(im, mf), (im, mb)], p)
+    # in-place threshold on a byte mask (shrink 1)
+    low = 0.5
+    p1 = param(1, [2], 0.0, flags=0x4)
+    p1.low_value = low
+    im2, mb2 = im.clone(), mb.clone()
+    n4b200.N4(im2, mb2, p1)
+    below = im <= low
+    assert int(mb2[below].max()) == 0 and float(im2[below].abs().max()) == 0.0
+    assert cuda.equal(mb2[~below], mb[~below])
