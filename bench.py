@@ -191,10 +191,11 @@ def cpu_baseline_single(seconds=12.0):
 
 def measure_components(dev, ctx, hbm_peak, reps=10):
     """Standalone HBM-bound kernels at the 512x512x320 scale: the fit's z
-    contraction (k_fit_rows_v4) on the 256x256x160 fitting grid (reads field
+    contraction (k_fit_rows_v5) on the 256x256x160 fitting grid (reads field
     4 B + float mask 4 B per voxel) and the dense evaluation (k_correct) at
     full resolution (writes 4 B per voxel); device time of the kernel alone
-    from the library's stage events, mean of `reps` calls."""
+    from the library's stage events, mean of `reps` calls, L2 evicted before
+    each."""
     import numpy as np
     import torch
     import n4b200
@@ -204,11 +205,17 @@ def measure_components(dev, ctx, hbm_peak, reps=10):
     fmask = (torch.rand(fit_shape, device=dev, generator=gen) > 0.4).float()
     lat11 = torch.randn((11, 11, 11), device=dev, generator=gen) * 0.1
 
+    # L2 eviction before every timed call: reading a 256 MB buffer (twice the
+    # L2) leaves only its clean lines there, so the timed kernel neither hits
+    # its own inputs in L2 nor pays for writing back a flush's dirty lines
+    flush = torch.zeros(64 << 20, dtype=torch.float32, device=dev)
+
     def kernel_ms(fn, stage):
         fn()
         ctx.set_profiling(True)
         tot = 0.0
         for _ in range(reps):
+            flush.sum()
             fn()
             tot += ctx.last_timings()["stage_ms"][stage]
         ctx.set_profiling(False)
@@ -216,13 +223,13 @@ def measure_components(dev, ctx, hbm_peak, reps=10):
     ms_fit = kernel_ms(lambda: n4b200.FitBspline3D(field, fmask, (11, 11, 11), ctx=ctx), 0)
     ms_eval = kernel_ms(lambda: n4b200.EvaluateBspline3D(lat11, (11, 11, 11), full_shape, ctx=ctx), 1)
     nfit, nfull = field.numel(), int(np.prod(full_shape))
-    del field, fmask
+    del field, fmask, flush
     fit = 8 * nfit / (ms_fit / 1000) / 1e9
     ups = 4 * nfull / (ms_eval / 1000) / 1e9
     return {
         "fit_gbs": {"value": fit, "frac": fit / hbm_peak, "ms": ms_fit,
-                    "workload": "FitBspline3D z-contraction pass (k_fit_rows_v4) over a 256x256x160 field + "
-                                "float mask, 11^3 lattice (8 B per voxel read)"},
+                    "workload": "FitBspline3D z-contraction pass (k_fit_rows_v5) over a 256x256x160 field + "
+                                "float mask, 11^3 lattice (8 B per voxel read; L2 evicted before each call)"},
         "upsample_gbs": {"value": ups, "frac": ups / hbm_peak, "ms": ms_eval,
                          "workload": "EvaluateBspline3D dense evaluation (k_correct) of an 11^3 lattice at "
                                      "512x512x320 (4 B per voxel written)"},
@@ -545,7 +552,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--batch", type=int, default=48)
+    ap.add_argument("--batch", type=int, default=96)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--components-only", action="store_true",

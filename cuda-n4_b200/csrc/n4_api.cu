@@ -1388,16 +1388,20 @@ n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *g) {
 }
 
 // ---------------------------------------------------------------- components
-// z contraction of a standalone fit: the vectorised kernel when every row
-// starts on a 16-byte boundary, the scalar one otherwise (same arithmetic).
+// z contraction of a standalone fit: rows read in 8-voxel (32-byte) register
+// steps when Z % 8 == 0 and field and mask start on 32-byte boundaries, in
+// 4-voxel (16-byte) steps when Z % 4 == 0 and they start on 16-byte
+// boundaries, both while the z table fits the default 48 KB of shared memory
+// (Z <= 1024); the scalar kernel otherwise.  Same arithmetic, bitwise the
+// same sums.
 static void launch_fit_rows(const float *field, const float *mask, long long rows, int Z, const Axis &az,
                             float *t1n, float *t1d, cudaStream_t st) {
-  // the vectorised kernel's z table (36 B per voxel) stays within the default
-  // 48 KB of dynamic shared memory beside its 18 KB of staging for Z <= 800
-  const bool v4 = Z % 4 == 0 && Z <= 800 && ((uintptr_t)field & 15u) == 0 && ((uintptr_t)mask & 15u) == 0;
-  if (v4)
-    k_fit_rows_v4<<<(unsigned)((rows + kFitRowsV - 1) / kFitRowsV), kFitRowsV, kFitTableBytes(Z), st>>>(
-        field, mask, rows, Z, az, t1n, t1d);
+  const uintptr_t al = (uintptr_t)field | (uintptr_t)mask;
+  const unsigned grid = (unsigned)((rows + kFitRowsD - 1) / kFitRowsD);
+  if (Z % 8 == 0 && Z <= kFitZMaxD && (al & 31u) == 0)
+    k_fit_rows_v5<8, 3><<<grid, kFitRowsD, kFitTableBytes(Z), st>>>(field, mask, rows, Z, az, t1n, t1d);
+  else if (Z % 4 == 0 && Z <= kFitZMaxD && (al & 15u) == 0)
+    k_fit_rows_v5<4, 6><<<grid, kFitRowsD, kFitTableBytes(Z), st>>>(field, mask, rows, Z, az, t1n, t1d);
   else
     k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(field, mask, rows, Z, az, t1n,
                                                                                    t1d);

@@ -549,135 +549,150 @@ __global__ void __launch_bounds__(kFitRows) k_fit_rows(const float *field, const
   }
 }
 
-// The same contraction for Z % 4 == 0 and 16-byte aligned field and mask,
-// built for HBM bandwidth: 64 rows per CTA (every CTA of a 256x256-row field
-// resident at once), one L2 bulk prefetch of the CTA's contiguous rows,
-// coalesced float4 streaming loads of the next 32-voxel
-// chunk issued into registers before the current chunk is walked from
-// shared memory, a shared row stride of 36 floats so that the per-row float4
-// reads of a quarter warp fall in 8 distinct 16-byte bank groups, and the
-// z-axis table (span, numerator and denominator weights) copied to shared
-// memory so that the walk's table reads neither wait on L1 nor alias the
-// row-sum stores.  The sums are bitwise those of k_fit_rows (same operations
-// in the same order; masked-out voxels add exact zeros).  Dynamic shared
-// memory: kFitTableBytes(Z).
-constexpr int kFitRowsV = 64;
-constexpr int kFitChunkV = 32;
-constexpr int kFitStrideV = kFitChunkV + 4;
-constexpr int kFitLoadsV = kFitChunkV / 4;   // float4 per thread (one row each) per array and chunk
+// The same contraction for Z % 4 == 0, Z <= 1024 and 16-byte aligned field
+// and mask, built for HBM bandwidth: one thread per row walks its row as in
+// k_fit_rows (the sums are bitwise equal: the same fused multiply-adds in the
+// same order; masked-out voxels add exact zeros), but reads it straight from
+// global memory, S voxels per step and array, with D steps in flight in
+// registers.  No shared-memory staging and no barrier after the z table is
+// loaded: warps never wait for one another, so the loads of some warps
+// overlap the arithmetic of others instead of the whole grid alternating
+// between loading and walking.  S = 8 (Z % 8 == 0, 32-byte aligned rows):
+// one 32-byte load per array and step, exactly one sector, not kept in L1;
+// S = 4: 16-byte loads, the sector's other half served by L1.  Dynamic
+// shared memory: kFitTableBytes(Z) (the z table: numerator and denominator
+// weights and the span of every voxel).
+constexpr int kFitRowsD = 64;     // rows (threads) per CTA
+constexpr int kFitZMaxD = 1024;
 __host__ __device__ inline size_t kFitTableBytes(int Z) { return (size_t)Z * 36; }
 
-__global__ void __launch_bounds__(kFitRowsV, 8) k_fit_rows_v4(const float *__restrict__ field,
-                                                              const float *__restrict__ mask, long long rows, int Z,
-                                                              Axis az, float *__restrict__ t1n,
-                                                              float *__restrict__ t1d) {
-  __shared__ __align__(16) float fs[kFitRowsV * kFitStrideV];
-  __shared__ __align__(16) float ms[kFitRowsV * kFitStrideV];
-  extern __shared__ __align__(16) char fit_tab[];
-  float4 *sp4 = (float4 *)fit_tab;                  // [Z] numerator weights
-  float4 *sq4 = sp4 + Z;                            // [Z] denominator weights
-  int *ss = (int *)(sq4 + Z);                       // [Z] span index
-  for (int i = threadIdx.x; i < Z; i += blockDim.x) {
-    sp4[i] = az.p4[i];
-    sq4[i] = az.q4[i];
-    ss[i] = az.s[i];
-  }
-  const long long row0 = (long long)blockIdx.x * kFitRowsV;
-  const int nr = (int)min((long long)kFitRowsV, rows - row0);
-  const int t = threadIdx.x;
-  const int ncz = az.nc;
-  // The CTA's rows are one contiguous range of field and mask: ask L2 for all
-  // of it at once (bulk prefetch, sequential in DRAM), so the strided
-  // 32-voxel chunk loads below are served from L2.
-  if (t == 0) {
-    const unsigned bytes = (unsigned)nr * (unsigned)Z * 4u;   // multiple of 16: Z % 4 == 0
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(field + row0 * Z), "r"(bytes) : "memory");
-    if (mask) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(mask + row0 * Z), "r"(bytes) : "memory");
-  }
-  float4 pf[kFitLoadsV], pm[kFitLoadsV];
-  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f), one4 = make_float4(1.f, 1.f, 1.f, 1.f);
-  auto load = [&](int z0) {
-#pragma unroll
-    for (int k = 0; k < kFitLoadsV; ++k) {
-      const int i = t + k * kFitRowsV;         // float4 index in the [rows][8] chunk
-      const int r = i >> 3, z = z0 + 4 * (i & 7);
-      pf[k] = zero4;
-      pm[k] = zero4;
-      if (r < nr && z < Z) {
-        const long long g = (row0 + r) * Z + z;
-        pf[k] = __ldcs((const float4 *)(field + g));
-        pm[k] = mask ? __ldcs((const float4 *)(mask + g)) : one4;
-      }
-    }
-  };
+template <int S> struct FitStep { float v[S]; };
+
+__device__ __forceinline__ void fit_load(FitStep<8> &x, const float *p) {
+  asm("ld.global.nc.L1::no_allocate.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(x.v[0]), "=f"(x.v[1]), "=f"(x.v[2]), "=f"(x.v[3]), "=f"(x.v[4]), "=f"(x.v[5]), "=f"(x.v[6]),
+        "=f"(x.v[7])
+      : "l"(p));
+}
+__device__ __forceinline__ void fit_load(FitStep<4> &x, const float *p) {
+  asm("ld.global.nc.v4.f32 {%0,%1,%2,%3}, [%4];"
+      : "=f"(x.v[0]), "=f"(x.v[1]), "=f"(x.v[2]), "=f"(x.v[3])
+      : "l"(p));
+}
+
+// One row's walk: the 4 open targets cur..cur+3 (numerator and denominator),
+// advanced S voxels at a time in the order of k_fit_rows.
+struct FitWalk {
   float n0 = 0.f, n1 = 0.f, n2 = 0.f, n3 = 0.f, d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
-  int cur = 0;
-  float *on = t1n + (row0 + t) * ncz, *od = t1d + (row0 + t) * ncz;
-  load(0);
-  for (int z0 = 0; z0 < Z; z0 += kFitChunkV) {
-    __syncthreads();
+  int cur = 0;             // span of the voxels being walked = first open target
+  int end;                 // first voxel after span cur
+  float *on, *od;          // the row's targets
+
+  __device__ __forceinline__ void add(float f, float u, const float4 &p, const float4 &w) {
+    n0 = __fmaf_rn(p.x, f, n0); n1 = __fmaf_rn(p.y, f, n1);
+    n2 = __fmaf_rn(p.z, f, n2); n3 = __fmaf_rn(p.w, f, n3);
+    d0 = __fmaf_rn(w.x, u, d0); d1 = __fmaf_rn(w.y, u, d1);
+    d2 = __fmaf_rn(w.z, u, d2); d3 = __fmaf_rn(w.w, u, d3);
+  }
+  // voxels vq .. vq + S - 1 with field fa and mask ma
+  template <int S>
+  __device__ __forceinline__ void step(const float (&fa)[S], const float (&ma)[S], int vq, const float4 *sp4,
+                                       const float4 *sq4, const int *ss, const int *span_hi) {
+    if (vq + S > end) {
+      // a span ends inside this step: voxel by voxel
 #pragma unroll
-    for (int k = 0; k < kFitLoadsV; ++k) {
-      const int i = t + k * kFitRowsV;
-      const int o = (i >> 3) * kFitStrideV + 4 * (i & 7);
-      *(float4 *)(fs + o) = pf[k];
-      *(float4 *)(ms + o) = pm[k];
-    }
-    __syncthreads();
-    if (z0 + kFitChunkV < Z) load(z0 + kFitChunkV);
-    if (t < nr) {
-      // branch-free per voxel: a masked-out voxel adds p*0 and q*0, which
-      // leaves the sums bitwise unchanged (and ignores a non-finite value
-      // there); a masked voxel adds fma(p, f, n) and fma(q, 1, d) = d + q
-      const int nq = min(kFitChunkV, Z - z0) >> 2;
-      for (int q = 0; q < nq; ++q) {
-        const float4 f4 = *(const float4 *)(fs + t * kFitStrideV + 4 * q);
-        const float4 m4 = *(const float4 *)(ms + t * kFitStrideV + 4 * q);
-        const float fa[4] = {f4.x, f4.y, f4.z, f4.w}, ma[4] = {m4.x, m4.y, m4.z, m4.w};
-        const int vq = z0 + 4 * q;
-        if (ss[vq + 3] != cur) {
-          // a span ends inside these 4 voxels: voxel by voxel
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const int sp = ss[vq + k];
-            while (cur < sp) {
-              on[cur] = n0;
-              od[cur] = d0;
-              n0 = n1; n1 = n2; n2 = n3; n3 = 0.f;
-              d0 = d1; d1 = d2; d2 = d3; d3 = 0.f;
-              ++cur;
-            }
-            const bool in = ma[k] != 0.0f;
-            const float f = in ? fa[k] : 0.0f, u = in ? 1.0f : 0.0f;
-            const float4 p = sp4[vq + k], w = sq4[vq + k];
-            n0 = __fmaf_rn(p.x, f, n0); n1 = __fmaf_rn(p.y, f, n1);
-            n2 = __fmaf_rn(p.z, f, n2); n3 = __fmaf_rn(p.w, f, n3);
-            d0 = __fmaf_rn(w.x, u, d0); d1 = __fmaf_rn(w.y, u, d1);
-            d2 = __fmaf_rn(w.z, u, d2); d3 = __fmaf_rn(w.w, u, d3);
-          }
-        } else {
-          // all 4 voxels in the open span (the common case)
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const bool in = ma[k] != 0.0f;
-            const float f = in ? fa[k] : 0.0f, u = in ? 1.0f : 0.0f;
-            const float4 p = sp4[vq + k], w = sq4[vq + k];
-            n0 = __fmaf_rn(p.x, f, n0); n1 = __fmaf_rn(p.y, f, n1);
-            n2 = __fmaf_rn(p.z, f, n2); n3 = __fmaf_rn(p.w, f, n3);
-            d0 = __fmaf_rn(w.x, u, d0); d1 = __fmaf_rn(w.y, u, d1);
-            d2 = __fmaf_rn(w.z, u, d2); d3 = __fmaf_rn(w.w, u, d3);
-          }
+      for (int j = 0; j < S; ++j) {
+        const int sp = ss[vq + j];
+        while (cur < sp) {
+          on[cur] = n0;
+          od[cur] = d0;
+          n0 = n1; n1 = n2; n2 = n3; n3 = 0.f;
+          d0 = d1; d1 = d2; d2 = d3; d3 = 0.f;
+          ++cur;
         }
+        const bool in = ma[j] != 0.0f;
+        add(in ? fa[j] : 0.0f, in ? 1.0f : 0.0f, sp4[vq + j], sq4[vq + j]);
+      }
+      end = span_hi[cur];
+    } else {
+      // the whole step in the open span (the common case)
+#pragma unroll
+      for (int j = 0; j < S; ++j) {
+        const bool in = ma[j] != 0.0f;
+        add(in ? fa[j] : 0.0f, in ? 1.0f : 0.0f, sp4[vq + j], sq4[vq + j]);
       }
     }
   }
-  if (t < nr) {
+  // the open window and every target after it
+  __device__ __forceinline__ void flush(int ncz) {
     for (int c = cur; c < ncz; ++c) {
       const int k = c - cur;
       on[c] = k == 0 ? n0 : k == 1 ? n1 : k == 2 ? n2 : k == 3 ? n3 : 0.0f;
       od[c] = k == 0 ? d0 : k == 1 ? d1 : k == 2 ? d2 : k == 3 ? d3 : 0.0f;
     }
   }
+};
+
+__device__ __forceinline__ void fit_table(const Axis &az, int Z, char *tab) {
+  float4 *sp4 = (float4 *)tab, *sq4 = sp4 + Z;
+  int *ss = (int *)(sq4 + Z);
+  for (int i = threadIdx.x; i < Z; i += blockDim.x) {
+    sp4[i] = az.p4[i];
+    sq4[i] = az.q4[i];
+    ss[i] = az.s[i];
+  }
+}
+
+template <int S, int D>
+__global__ void __launch_bounds__(kFitRowsD, 8) k_fit_rows_v5(const float *__restrict__ field,
+                                                              const float *__restrict__ mask, long long rows, int Z,
+                                                              Axis az, float *__restrict__ t1n,
+                                                              float *__restrict__ t1d) {
+  extern __shared__ __align__(16) char fit_tab[];
+  const float4 *sp4 = (const float4 *)fit_tab, *sq4 = sp4 + Z;
+  const int *ss = (const int *)(sq4 + Z);
+  const long long row = (long long)blockIdx.x * kFitRowsD + threadIdx.x;
+  const bool live = row < rows;
+  const int nq = Z / S;                             // steps per row
+  const float *fp = field + (live ? row : 0) * Z;
+  const float *mp = mask ? mask + (live ? row : 0) * Z : nullptr;
+  FitStep<S> F[D], M[D];
+  // the first steps are requested before the table is built
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    if (live && k < nq) {
+      fit_load(F[k], fp + k * S);
+      if (mp) fit_load(M[k], mp + k * S);
+    }
+  }
+  fit_table(az, Z, fit_tab);
+  __syncthreads();
+  if (!live) return;
+  const int ncz = az.nc;
+  FitWalk w;
+  w.end = az.hi[0];
+  w.on = t1n + row * ncz;
+  w.od = t1d + row * ncz;
+  for (int q0 = 0; q0 < nq; q0 += D) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      const int q = q0 + k;
+      if (q >= nq) break;
+      float fa[S], ma[S];
+#pragma unroll
+      for (int j = 0; j < S; ++j) {
+        fa[j] = F[k].v[j];
+        ma[j] = mp ? M[k].v[j] : 1.0f;
+      }
+      // step q is in registers: request step q + D into its slot
+      if (q + D < nq) {
+        fit_load(F[k], fp + (q + D) * S);
+        if (mp) fit_load(M[k], mp + (q + D) * S);
+      }
+      w.step<S>(fa, ma, S * q, sp4, sq4, ss, az.hi);
+    }
+  }
+  w.flush(ncz);
 }
 
 // T2[vx][cy][cz] from T1.

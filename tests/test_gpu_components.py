@@ -44,6 +44,41 @@ def test_fit_zero_den_semantics(cuda):
     assert np.all(np.asarray(a)[-1] == 0.0)
 
 
+@pytest.mark.parametrize("shape,nc", [((64, 48, 160), (8, 7, 11)), ((40, 36, 320), (6, 9, 35)),
+                                      ((20, 18, 400), (5, 5, 19)), ((33, 17, 36), (6, 5, 40)),
+                                      ((16, 16, 8), (5, 4, 7)), ((10, 6, 800), (4, 5, 23)),
+                                      ((8, 8, 1028), (4, 4, 12))])
+def test_fit_row_kernels_agree_bitwise(cuda, shape, nc):
+    """The z contraction has three kernels, chosen by Z and the alignment of
+    the field and mask: rows read in 32-byte steps (Z % 8 == 0, 32-byte
+    aligned), in 16-byte steps (Z % 4 == 0, 16-byte aligned), both for
+    Z <= 1024, and the scalar kernel (otherwise).  All add the same terms in
+    the same order, so the field at a 32-byte boundary, 16 bytes and 4 bytes
+    further on give bitwise the same lattice; NaNs where the mask is 0 are
+    ignored by all.  Covers more spans than voxels along z (empty spans), a
+    target count that is not a multiple of 4 and a Z above the vectorised
+    kernels' limit."""
+    import n4b200
+    rng = np.random.default_rng(7)
+    n = int(np.prod(shape))
+    f = rng.normal(0, 0.3, size=n).astype(np.float32)
+    m = (rng.random(n) < 0.6).astype(np.float32)
+    f[(m == 0) & (rng.random(n) < 0.05)] = np.nan
+    lats = []
+    for off in (0, 4, 1):                         # floats: 32-, 16- and 4-byte aligned starts
+        fb = cuda.empty(n + 8, device="cuda")
+        mb = cuda.empty(n + 8, device="cuda")
+        assert fb.data_ptr() % 32 == 0 and mb.data_ptr() % 32 == 0
+        fb[off:off + n] = cuda.tensor(f, device="cuda")
+        mb[off:off + n] = cuda.tensor(m, device="cuda")
+        lats.append(n4b200.FitBspline3D(fb[off:off + n].view(shape), mb[off:off + n].view(shape), nc))
+    cuda.cuda.synchronize()
+    assert cuda.isfinite(lats[0]).all()
+    assert cuda.equal(lats[0], lats[1]) and cuda.equal(lats[0], lats[2])
+    ref = O.FitBspline3D(np.where(m == 0, 0.0, f).reshape(shape).astype(np.float64), m.reshape(shape), nc)
+    assert nrel(lats[0], ref) < 1e-5
+
+
 @pytest.mark.parametrize("k", [0, 1, 2])
 def test_evaluate(cuda, golden_components, k):
     import n4b200
