@@ -515,7 +515,8 @@ def run_ours(args, rank, world, local_rank):
         "e2e_byte_masks": {"value": world * B * args.steps / (ms_e2e_u8 / 1000.0), "unit": "volumes/s",
                            "h2d_bytes_per_step": h2d_u8, "d2h_bytes_per_step": d2h,
                            "path": "same as e2e with uint8 masks (N4_FLAG_MASK_U8)"},
-        "gpu_launches": t_w["launches"] * args.steps,
+        "gpu_launches": warm.kernel_launches * args.steps,
+        "sub_batches": warm.sub_batches,
         "clocks": clk,
         "plain": {"value": plain, "unit": "volumes/s", "ms_per_volume": ms_plain / (args.steps * B),
                   "path": "n4_run, one volume per call, no warm start"},

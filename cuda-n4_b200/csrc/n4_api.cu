@@ -108,6 +108,7 @@ struct TuneVal {
 
 constexpr int kStaticSmemReserve = 1024;
 constexpr int kSlots = 4;
+constexpr int kMaxSub = 4;   // sub-batches of a pipelined batch
 
 }  // namespace
 
@@ -127,6 +128,10 @@ struct n4_context {
   std::map<TuneKey, TuneVal> tune;
   // max co-resident clusters per (threads, cluster size, shared bytes)
   std::map<std::tuple<int, int, int>, int> cluster_cap;
+  // sub-batch pipeline: N4 launches on two high-priority streams, prologues
+  // and warm starts on one low-priority stream, corrections on another
+  cudaStream_t pipe[4] = {};
+  cudaEvent_t pev[16] = {};
   // profiling
   int profiling = 0;
   cudaEvent_t ev[5] = {};
@@ -590,6 +595,8 @@ struct Prepared {
   n4_encoder_t *enc = nullptr;   // learned warm start run inside the batch
   int enc_batch = 0;             // predictions per encoder call
   long long fit_total = 0, tiles = 0;
+  int nsub = 1;                  // sub-batches (volume ranges sub_lo[k] .. sub_lo[k + 1])
+  std::vector<int> sub_lo;
 };
 
 // Descriptor buffer: pinned host staging and its device copy.
@@ -666,6 +673,22 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
   P.csize.assign(n, 0);
   for (int i : P.in_cluster) { P.path[i] = 1; P.csize[i] = ch.K; }
   for (int i : P.in_grid) { P.path[i] = 2; P.csize[i] = ctx->nsm; }
+  // sub-batches (cluster-path batches only): by default one per two waves of
+  // the clusters that fit at once, so that every sub-batch keeps them busy
+  P.nsub = 1;
+  const int want_sub = (int)((p->flags >> 16) & 7u);
+  if (P.in_grid.empty() && n > 1 && want_sub != 1) {
+    int S = want_sub;
+    if (S == 0) {
+      const Plan pl = make_plan(p, ch.K, dims, false);
+      int cap = 0;
+      TRY(capacity(ctx, ch.nt, ch.K, pl.sm_bytes + pl.big_bytes, &cap));
+      S = cap > 0 ? n / (2 * cap) : 1;
+    }
+    P.nsub = std::max(1, std::min(std::min(S, kMaxSub), n));
+  }
+  P.sub_lo.resize(P.nsub + 1);
+  for (int k = 0; k <= P.nsub; ++k) P.sub_lo[k] = (int)((long long)n * k / P.nsub);
   // workspaces
   P.NCX = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
   P.NCY = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);
@@ -693,7 +716,7 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
   P.o_tst = take(8 * n);
   P.o_rep = take(sizeof(n4_report_t) * n);
   P.o_flg = take(4 * n);
-  P.o_q = take(16);
+  P.o_q = take(16 * kMaxSub);
   P.o_pool = take(sizeof(PoolJob) * n);
   P.bytes = o;
   return N4_OK;
@@ -737,12 +760,21 @@ void fill_descriptors(n4_context *ctx, const n4_params_t *p, Prepared &P, const 
   }
   P.fit_total = fit_total;
   P.tiles = tiles;
-  // longest-first order of the cluster queue
-  std::vector<int> order = P.in_cluster;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-    const Dims &x = P.dims[a], &y = P.dims[b];
-    return (long long)x.X * x.Y * x.Z > (long long)y.X * y.Y * y.Z;
-  });
+  // longest-first order of each sub-batch's cluster queue, the sub-batches
+  // one after the other
+  std::vector<int> order;
+  const int nsub = P.sub_lo.empty() ? 1 : P.nsub;
+  for (int k = 0; k < nsub; ++k) {
+    const int lo = P.sub_lo.empty() ? 0 : P.sub_lo[k], hi = P.sub_lo.empty() ? n : P.sub_lo[k + 1];
+    std::vector<int> part;
+    for (int i : P.in_cluster)
+      if (i >= lo && i < hi) part.push_back(i);
+    std::stable_sort(part.begin(), part.end(), [&](int a, int b) {
+      const Dims &x = P.dims[a], &y = P.dims[b];
+      return (long long)x.X * x.Y * x.Z > (long long)y.X * y.Y * y.Z;
+    });
+    order.insert(order.end(), part.begin(), part.end());
+  }
   for (size_t k = 0; k < order.size(); ++k) ord[k] = order[k];
 }
 
@@ -755,9 +787,130 @@ n4_status_t enqueue_pool(n4_context *ctx, const Prepared &P, const DescBuf &B, _
   return N4_OK;
 }
 
+// The cluster kernel over the queue ord[o0 .. o0 + njobs) with queue counter q.
+n4_status_t launch_engine(n4_context *ctx, const n4_params_t *p, const Prepared &P, const DescBuf &B, int o0,
+                          int njobs, int q, cudaStream_t st) {
+  std::vector<Dims> sub;
+  for (int i : P.in_cluster) sub.push_back(P.dims[i]);
+  Plan pl = make_plan(p, P.ch.K, sub, false);
+  const int smem = pl.sm_bytes + pl.big_bytes;
+  int cap = 0;
+  TRY(capacity(ctx, P.ch.nt, P.ch.K, smem, &cap));
+  if (cap < 1) return fail(N4_ERR_TOO_LARGE, "no cluster of this size fits on the device");
+  ClusterArgs a{};
+  a.pl = pl;
+  a.pr = P.pr;
+  a.jobs = B.dp<VolJob>(P.o_job);
+  a.order = B.dp<int>(P.o_ord) + o0;
+  a.njobs = njobs;
+  a.queue = B.dp<int>(P.o_q) + 4 * q;
+  a.use_tma = 1;
+  const int ncl = std::min<int>(cap, njobs);
+  if (P.ch.nt == 1024) TRY(launch_cluster_kernel<1024>(ctx, a, P.ch.K, ncl, smem, st));
+  else TRY(launch_cluster_kernel<512>(ctx, a, P.ch.K, ncl, smem, st));
+  return N4_OK;
+}
+
+n4_status_t ensure_pipe(n4_context *ctx) {
+  if (ctx->pipe[0]) return N4_OK;
+  int least = 0, greatest = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  for (int i = 0; i < 4; ++i)
+    CK(cudaStreamCreateWithPriority(&ctx->pipe[i], cudaStreamNonBlocking, i < 2 ? greatest : least));
+  for (cudaEvent_t &e : ctx->pev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return N4_OK;
+}
+
+// A cluster-path batch as P.nsub sub-batches (descriptors already on the
+// device; capturable).  Sub-batch k's N4 launch waits only for its own
+// prologue and warm start, and runs on high-priority stream pipe[k % 2], so
+// that it takes the SMs the previous launch frees; the prologues, pooling and
+// encoder calls run in order on pipe[2] and the corrections on pipe[3], at
+// low priority, on the SMs the clusters leave free.  Every kernel reads and
+// writes only its own volumes' buffers; st waits for all four streams.
+n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepared &P, const DescBuf &B,
+                              cudaStream_t st) {
+  TRY(ensure_pipe(ctx));
+  const int S = P.nsub;
+  cudaStream_t side = ctx->pipe[2], corr = ctx->pipe[3];
+  cudaEvent_t *ev = ctx->pev;   // 0 fork, 1 tables, 2+k prologue k, 6+k N4 k, 10+i join of pipe[i]
+  CK(cudaEventRecord(ev[0], st));
+  for (cudaStream_t s2 : ctx->pipe) CK(cudaStreamWaitEvent(s2, ev[0], 0));
+  const int n = P.n;
+  const long long *pst = B.hp<long long>(P.o_pst), *tst = B.hp<long long>(P.o_tst);
+  int launches = 0;
+  // full grids for the prologues and corrections too: limited to the SMs the
+  // clusters leave free they fall behind the N4 launches (measured)
+  k_axis_tables<<<3 * n, 256, 0, side>>>(B.dp<TableJob>(P.o_tab));
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ev[1], side));
+  CK(cudaStreamWaitEvent(corr, ev[1], 0));
+  ++launches;
+  for (int k = 0; k < S; ++k) {
+    const int lo = P.sub_lo[k], hi = P.sub_lo[k + 1], nk = hi - lo;
+    const long long g0 = pst[lo], g1 = hi < n ? pst[hi] : P.fit_total;
+    const int blocks = (int)std::min<long long>((g1 - g0 + 255) / 256, (long long)ctx->nsm * 16);
+    k_prologue<<<std::max(blocks, 1), 256, 0, side>>>(B.dp<PrologueVol>(P.o_pro) + lo, B.dp<long long>(P.o_pst) + lo,
+                                                       nk, g0, g1 - g0, p->low_value, B.dp<int>(P.o_flg) + lo);
+    CK(cudaGetLastError());
+    ++launches;
+    if (p->ShrinkFactor > 1 && (p->flags & N4_FLAG_INPLACE_THRESH)) {
+      for (int i = lo; i < hi; ++i) {
+        const long long nf = (long long)P.dims[i].FX * P.dims[i].FY * P.dims[i].FZ;
+        if (P.rvs[i].im_w) {
+          k_threshold_inplace<<<(int)std::min<long long>((nf + 255) / 256, ctx->nsm * 16LL), 256, 0, side>>>(
+              P.rvs[i].im_w, P.rvs[i].mask_w, (p->flags & N4_FLAG_MASK_U8) ? 1 : 0, nf, p->low_value);
+          CK(cudaGetLastError());
+          ++launches;
+        }
+      }
+    }
+    if (P.enc) {
+      __nv_bfloat16 *x = (__nv_bfloat16 *)ctx->warm_x.p;
+      const long long cells = (long long)nk * kPoolCells;
+      const int pb = (int)std::min<long long>((cells + 255) / 256, (long long)ctx->nsm * 16);
+      k_pool_fitgrid<<<pb, 256, 0, side>>>(B.dp<PoolJob>(P.o_pool) + lo, nk, x + (size_t)lo * kPoolCells);
+      CK(cudaGetLastError());
+      ++launches;
+      for (int c0 = lo; c0 < hi; c0 += P.enc_batch) {
+        const int nb = std::min(P.enc_batch, hi - c0);
+        TRY(n4_encoder_predict(P.enc, x + (size_t)c0 * kPoolCells, nb, ctx->warm_lat.as<float>() + 64 * c0, side));
+        launches += kEncoderLaunches;
+      }
+    }
+    CK(cudaEventRecord(ev[2 + k], side));
+  }
+  for (int k = 0; k < S; ++k) {
+    cudaStream_t es = ctx->pipe[k & 1];
+    CK(cudaStreamWaitEvent(es, ev[2 + k], 0));
+    TRY(launch_engine(ctx, p, P, B, P.sub_lo[k], P.sub_lo[k + 1] - P.sub_lo[k], k, es));
+    CK(cudaEventRecord(ev[6 + k], es));
+    ++launches;
+  }
+  for (int k = 0; k < S; ++k) {
+    const int lo = P.sub_lo[k], hi = P.sub_lo[k + 1];
+    const long long t0 = tst[lo], t1 = hi < n ? tst[hi] : P.tiles;
+    CK(cudaStreamWaitEvent(corr, ev[6 + k], 0));
+    k_correct<<<(unsigned)(t1 - t0), 256, 0, corr>>>(B.dp<CorrectVol>(P.o_cor) + lo, B.dp<long long>(P.o_tst) + lo,
+                                                 hi - lo, t0, t1 - t0, p->low_value);
+    CK(cudaGetLastError());
+    ++launches;
+  }
+  for (int i = 0; i < 4; ++i) {
+    CK(cudaEventRecord(ev[10 + i], ctx->pipe[i]));
+    CK(cudaStreamWaitEvent(st, ev[10 + i], 0));
+  }
+  ctx->prof_launches = launches;
+  ctx->prof_fit = P.fit_total;
+  ctx->prof_full = 0;
+  for (const Dims &d : P.dims) ctx->prof_full += (long long)d.FX * d.FY * d.FZ;
+  return N4_OK;
+}
+
 // The launches of a run (descriptors already on the device); capturable.
 n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P, const DescBuf &B, cudaStream_t st,
                         bool profile) {
+  if (!profile && P.nsub > 1) return enqueue_pipelined(ctx, p, P, B, st);
   const int n = P.n;
   int launches = 0;
   if (profile) TRY(prof_mark(ctx, 0, st));
@@ -765,7 +918,7 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
     ++launches;
     const int blocks = (int)std::min<long long>((P.fit_total + 255) / 256, (long long)ctx->nsm * 16);
     k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(B.dp<PrologueVol>(P.o_pro), B.dp<long long>(P.o_pst), n,
-                                                     P.fit_total, p->low_value, B.dp<int>(P.o_flg));
+                                                     0, P.fit_total, p->low_value, B.dp<int>(P.o_flg));
     CK(cudaGetLastError());
     if (p->ShrinkFactor > 1 && (p->flags & N4_FLAG_INPLACE_THRESH)) {
       for (int i = 0; i < n; ++i) {
@@ -792,24 +945,7 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
   }
   if (profile) TRY(prof_mark(ctx, 1, st));
   if (!P.in_cluster.empty()) {
-    std::vector<Dims> sub;
-    for (int i : P.in_cluster) sub.push_back(P.dims[i]);
-    Plan pl = make_plan(p, P.ch.K, sub, false);
-    const int smem = pl.sm_bytes + pl.big_bytes;
-    int cap = 0;
-    TRY(capacity(ctx, P.ch.nt, P.ch.K, smem, &cap));
-    if (cap < 1) return fail(N4_ERR_TOO_LARGE, "no cluster of this size fits on the device");
-    ClusterArgs a{};
-    a.pl = pl;
-    a.pr = P.pr;
-    a.jobs = B.dp<VolJob>(P.o_job);
-    a.order = B.dp<int>(P.o_ord);
-    a.njobs = (int)P.in_cluster.size();
-    a.queue = B.dp<int>(P.o_q);
-    a.use_tma = 1;
-    const int ncl = std::min<int>(cap, (int)P.in_cluster.size());
-    if (P.ch.nt == 1024) TRY(launch_cluster_kernel<1024>(ctx, a, P.ch.K, ncl, smem, st));
-    else TRY(launch_cluster_kernel<512>(ctx, a, P.ch.K, ncl, smem, st));
+    TRY(launch_engine(ctx, p, P, B, 0, (int)P.in_cluster.size(), 0, st));
     ++launches;
   }
   for (int i : P.in_grid) {
@@ -821,7 +957,8 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
   k_axis_tables<<<3 * n, 256, 0, st>>>(B.dp<TableJob>(P.o_tab));
   CK(cudaGetLastError());
   if (profile) TRY(prof_mark(ctx, 3, st));
-  k_correct<<<(unsigned)P.tiles, 256, 0, st>>>(B.dp<CorrectVol>(P.o_cor), B.dp<long long>(P.o_tst), n, p->low_value);
+  k_correct<<<(unsigned)P.tiles, 256, 0, st>>>(B.dp<CorrectVol>(P.o_cor), B.dp<long long>(P.o_tst), n, 0, P.tiles,
+                                               p->low_value);
   CK(cudaGetLastError());
   if (profile) TRY(prof_mark(ctx, 4, st));
   launches += 2;
@@ -966,6 +1103,10 @@ n4_status_t n4_destroy(n4_context_t *c) {
   if (c->last_done) cudaEventDestroy(c->last_done);
   for (cudaEvent_t e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : c->pev)
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t s : c->pipe)
+    if (s) cudaStreamDestroy(s);
   delete c;
   return N4_OK;
 }
@@ -1086,7 +1227,7 @@ n4_status_t n4_warm_inputs(n4_context_t *ctx, const n4_params_t *p, int n, const
   TRY(begin_run(ctx, st));
   CK(cudaMemcpyAsync(B.d, B.h, P.bytes, cudaMemcpyHostToDevice, st));
   const int blocks = (int)std::min<long long>((fit_total + 255) / 256, (long long)ctx->nsm * 16);
-  k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(B.dp<PrologueVol>(P.o_pro), B.dp<long long>(P.o_pst), n,
+  k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(B.dp<PrologueVol>(P.o_pro), B.dp<long long>(P.o_pst), n, 0,
                                                    fit_total, p->low_value, B.dp<int>(P.o_flg));
   CK(cudaGetLastError());
   TRY(enqueue_pool(ctx, P, B, (__nv_bfloat16 *)d_x, st));
@@ -1173,8 +1314,12 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
     if (s == N4_OK && cudaEventRecord(e1, st) != cudaSuccess) s = fail(N4_ERR_CUDA, "cudaEventRecord failed");
     if (s == N4_OK) s = collect(ctx, reps.data(), n);
     if (s != N4_OK) { status = s; break; }
+    // the run's own completion event precedes e1 on the stream: wait for e1
     float ms = 0.0f;
-    if (cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) { status = fail(N4_ERR_CUDA, "event timing failed"); break; }
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      status = fail(N4_ERR_CUDA, "event timing failed");
+      break;
+    }
     ms /= kReps;
     const int k = rep.candidates++;
     rep.cluster_size[k] = ch.grid ? 0 : ch.K;
@@ -1266,6 +1411,7 @@ struct n4_batch_graph {
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t done = nullptr;
   bool launched = false;
+  int launches = 0;   // kernel launches recorded in the graph
 };
 
 static void graph_free(n4_batch_graph *g) {
@@ -1312,6 +1458,7 @@ static n4_status_t graph_create(n4_context_t *ctx, const n4_params_t *p, int n, 
   std::memset(g->h_rep, 0, g->rep_bytes);
   DescBuf B{g->h_desc, g->d_desc};
   fill_descriptors(ctx, p, g->P, B);
+  if (P.nsub > 1 && (s = ensure_pipe(ctx)) != N4_OK) { graph_free(g); return s; }
   cudaStream_t cs;
   CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   s = N4_OK;
@@ -1322,6 +1469,7 @@ static n4_status_t graph_create(n4_context_t *ctx, const n4_params_t *p, int n, 
     if ((e = cudaMemcpyAsync(B.d, B.h, P.bytes, cudaMemcpyHostToDevice, cs)) != cudaSuccess)
       s = fail(N4_ERR_CUDA, cudaGetErrorString(e));
     if (s == N4_OK) s = enqueue_run(ctx, p, P, B, cs, false);
+    g->launches = ctx->prof_launches;
     if (s == N4_OK &&
         (e = cudaMemcpyAsync(g->h_rep, B.d + P.o_rep, g->rep_bytes, cudaMemcpyDeviceToHost, cs)) != cudaSuccess)
       s = fail(N4_ERR_CUDA, cudaGetErrorString(e));
@@ -1376,6 +1524,13 @@ n4_status_t n4_batch_graph_sync(n4_batch_graph_t *g, n4_report_t *reports, int n
     if (r.status != N4_OK && worst == N4_OK) worst = (n4_status_t)r.status;
   }
   if (worst != N4_OK) return fail(worst, std::string("volume failed: ") + n4_status_string(worst));
+  return N4_OK;
+}
+
+n4_status_t n4_batch_graph_info(const n4_batch_graph_t *g, int *kernel_launches, int *sub_batches) {
+  if (!g) return fail(N4_ERR_INVALID_ARG, "graph is NULL");
+  if (kernel_launches) *kernel_launches = g->launches;
+  if (sub_batches) *sub_batches = g->P.nsub;
   return N4_OK;
 }
 
@@ -1483,7 +1638,7 @@ n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice, uns
   const size_t so = align_up(sizeof(cv), 16);
   const bool prof = ctx->profiling != 0;
   if (prof) TRY(prof_mark(ctx, 1, st));
-  k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0.0f);
+  k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0, tiles, 0.0f);
   CK(cudaGetLastError());
   if (prof) { TRY(prof_mark(ctx, 2, st)); TRY(prof_mark(ctx, 3, st)); TRY(prof_mark(ctx, 4, st)); }
   ctx->prof_launches = 2;

@@ -47,9 +47,14 @@ __device__ __forceinline__ int find_volume(const long long *starts, int n, long 
   return lo;
 }
 
-__global__ void k_prologue(const PrologueVol *vols, const long long *starts, int nvol,
-                           long long total, float low, int *flag_nonfinite) {
-  for (long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < total;
+// Fitting voxels g0 .. g0 + total - 1 of a batch (numbered as in
+// PrologueVol::start) of the volumes vols[0 .. nvol); a non-finite voxel inside
+// the mask sets flag_nonfinite[v] of its volume v.
+__global__ void __launch_bounds__(256, 6) k_prologue(const PrologueVol *vols, const long long *starts, int nvol,
+                                                     long long g0, long long total, float low,
+                                                     int *flag_nonfinite) {
+  const long long end = g0 + total;
+  for (long long gi = g0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < end;
        gi += (long long)gridDim.x * blockDim.x) {
     const int v = find_volume(starts, nvol, gi);
     const PrologueVol &P = vols[v];
@@ -60,7 +65,7 @@ __global__ void k_prologue(const PrologueVol *vols, const long long *starts, int
     if (s == 1) {
       const float val = P.im[li];
       const bool m = (P.mask ? mask_on(P.mask, P.mask_u8, li) : true) && val > low;
-      if (m && !isfinite(val)) atomicExch(flag_nonfinite, 1);
+      if (m && !isfinite(val)) atomicExch(flag_nonfinite + v, 1);
       out = m ? logf(val) : __int_as_float(0x7fc00000);
       if (P.im_w && !(val > low)) { P.im_w[li] = 0.0f; if (P.mask_w) mask_clear(P.mask_w, P.mask_u8, li); }
     } else {
@@ -72,7 +77,7 @@ __global__ void k_prologue(const PrologueVol *vols, const long long *starts, int
           for (int dz = 0; dz < s; ++dz) {
             const float val = P.im[rowb + dz];
             const bool m = (P.mask ? mask_on(P.mask, P.mask_u8, rowb + dz) : true) && val > low;
-            if (m) { sum += val; ++cnt; if (!isfinite(val)) atomicExch(flag_nonfinite, 1); }
+            if (m) { sum += val; ++cnt; if (!isfinite(val)) atomicExch(flag_nonfinite + v, 1); }
           }
         }
       const float mean = cnt ? sum / (float)cnt : 0.0f;
@@ -309,15 +314,15 @@ constexpr int kLxMax = 2048;    // x-contracted lattice slice ncy*ncz held per x
 // I/O.  HBM traffic: read im, write out (+ bias).
 constexpr int kCorrectPre = 4;   // input float4 loads a thread keeps in flight
 
-__global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, const long long *tile_starts,
-                                                    int nvol, float low) {
-  __shared__ float Gs[kRowsPerTile * kMaxNcz];
-  __shared__ float Lx[2 * kLxMax];
-  const int v = find_volume(tile_starts, nvol, blockIdx.x);
+// Tile `tile` of a batch (numbered as in CorrectVol::tile0) of the volumes
+// vols[0 .. nvol); Gs and Lx in shared memory.
+__device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long long *tile_starts, int nvol,
+                                             long long tile, float low, float *Gs, float *Lx) {
+  const int v = find_volume(tile_starts, nvol, tile);
   const CorrectVol &C = vols[v];
   const Axis ax = axis_at(C.tx, C.FX, C.ncx), ay = axis_at(C.ty, C.FY, C.ncy), az = axis_at(C.tz, C.FZ, C.ncz);
   const long long rows = (long long)C.FX * C.FY;
-  const long long row0 = (blockIdx.x - C.tile0) * (long long)kRowsPerTile;
+  const long long row0 = (tile - C.tile0) * (long long)kRowsPerTile;
   const int nr = (int)min((long long)kRowsPerTile, rows - row0);
   const int ncz = C.ncz, ncy = C.ncy;
   const int FZ = C.FZ;
@@ -484,6 +489,18 @@ __global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, cons
         C.out[off] = b;
       }
     }
+  }
+}
+
+// Tiles t0 .. t0 + ntiles - 1 of a batch, grid-stride (a grid of one CTA per
+// tile runs each CTA once).
+__global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, const long long *tile_starts,
+                                                    int nvol, long long t0, long long ntiles, float low) {
+  __shared__ float Gs[kRowsPerTile * kMaxNcz];
+  __shared__ float Lx[2 * kLxMax];
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    if (t != blockIdx.x) __syncthreads();   // every thread is done with the previous tile's Gs
+    correct_tile(vols, tile_starts, nvol, t0 + t, low, Gs, Lx);
   }
 }
 

@@ -409,7 +409,9 @@ class N4BatchGraph:
     """A batched run recorded once as a CUDA graph and replayed with
     ``launch()`` (``n4_batch_graph_*``).  Inputs are read from the given
     CUDA tensors at every launch (refill them in place to correct new data);
-    outputs are written to ``results[i].im_normalized`` etc."""
+    outputs are written to ``results[i].im_normalized`` etc.
+    ``kernel_launches``: the library's kernels per launch; ``sub_batches``:
+    how many sub-batches the run overlaps (``N4_FLAG_SUB_BATCHES``)."""
 
     def __init__(self, volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=None,
                  return_bias=False, ctx: Optional[Context] = None, encoder=None):
@@ -447,6 +449,9 @@ class N4BatchGraph:
         else:
             check(_lib.load().n4_batch_graph_create(self.ctx.handle, C.byref(self._cpar), n, arr,
                                                     C.byref(self._h)))
+        nl, ns = C.c_int(), C.c_int()
+        check(_lib.load().n4_batch_graph_info(self._h, C.byref(nl), C.byref(ns)))
+        self.kernel_launches, self.sub_batches = nl.value, ns.value
 
     def launch(self):
         check(_lib.load().n4_batch_graph_launch(self._h, _stream(self.device)))

@@ -26,6 +26,11 @@ FLAG_FORCE_GRID = 0x8
 FLAG_FORCE_CLUSTER = 0x10
 
 
+def FLAG_SUB_BATCHES(k: int) -> int:
+    """Bits 16-18 of n4_params_t.flags: k sub-batches (0 = automatic, 1 = no overlap)."""
+    return (int(k) & 7) << 16
+
+
 class n4_params_t(C.Structure):
     _fields_ = [
         ("NumberOfHistogramBins", C.c_uint),
@@ -112,6 +117,7 @@ SIGNATURES = [
     ("n4_batch_graph_launch", C.c_int, [_P, _P]),
     ("n4_batch_graph_sync", C.c_int, [_P, C.POINTER(n4_report_t), C.c_int]),
     ("n4_batch_graph_destroy", C.c_int, [_P]),
+    ("n4_batch_graph_info", C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("n4_set_profiling", C.c_int, [_P, C.c_int]),
     ("n4_last_timings", C.c_int, [_P, C.POINTER(n4_timings_t)]),
     ("n4_autotune", C.c_int, [_P, _P, C.c_int, _P, _P, _P]),

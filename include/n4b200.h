@@ -56,6 +56,12 @@ typedef enum {
  * bytes, one per voxel, non-zero = foreground, instead of floats (a quarter of
  * the bytes to move; the component entry points take float masks). */
 #define N4_FLAG_MASK_U8         0x4000u
+/* Bits 16-18: a batch on the cluster path runs as k sub-batches, each
+ * sub-batch's prologue, warm start and correction overlapping the other
+ * sub-batches' N4 iterations on the SMs the clusters leave free (1 = one
+ * pass, no overlap; 0 = choose: one sub-batch per two waves of clusters, at
+ * most 4).  Every volume's result is the same either way. */
+#define N4_FLAG_SUB_BATCHES(k)  (((unsigned int)(k) & 7u) << 16)
 
 /* Mirrors N4Param (cudaN4.h:24-94).  Obtain defaults from n4_params_default. */
 typedef struct {
@@ -160,6 +166,9 @@ n4_status_t n4_batch_graph_launch(n4_batch_graph_t *graph, void *stream);
 /* Wait for the last launch and fill its reports (n entries, may be NULL). */
 n4_status_t n4_batch_graph_sync(n4_batch_graph_t *graph, n4_report_t *reports, int n);
 n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *graph);
+/* The recorded run's kernel launches per graph launch (the library's own
+ * kernels) and its sub-batches (N4_FLAG_SUB_BATCHES); either may be NULL. */
+n4_status_t n4_batch_graph_info(const n4_batch_graph_t *graph, int *kernel_launches, int *sub_batches);
 
 /* ---- autotuning (no counterpart in the reference) ----
  * n4_autotune runs the given volumes once per execution configuration that

@@ -1,0 +1,87 @@
+"""Sub-batch pipelining of cluster-path batches and per-volume reports.
+
+A batch on the cluster path may run as k sub-batches (N4_FLAG_SUB_BATCHES):
+each sub-batch's prologue, warm start and correction overlap the other
+sub-batches' iterations.  Every volume goes through the same kernels with the
+same shared-memory plan either way, so the results must be bitwise those of
+the single pass, eagerly, recorded as a graph and with the learned warm start.
+"""
+import numpy as np
+import pytest
+
+from n4b200.phantom import make_phantom
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(40, 48, 32), (64, 56, 40), (48, 48, 48), (32, 40, 56), (56, 64, 32)]
+
+
+def _param(sub, **kw):
+    import n4b200
+    p = n4b200.N4Param(NumberOfFittingLevels=2, MaximumNumberOfIterations=[8, 8], ConvergenceThreshold=0.0,
+                       low_value=0.0, **kw)
+    p.flags |= n4b200._lib.FLAG_SUB_BATCHES(sub)
+    return p
+
+
+def _volumes(cuda, n, seed):
+    vols = []
+    for i in range(n):
+        ph = make_phantom(SHAPES[i % len(SHAPES)], seed=seed + i)
+        vols.append((cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")))
+    return vols
+
+
+def _same(cuda, a, b):
+    for r, q in zip(a, b):
+        assert r.report["status"] == q.report["status"] == "N4_OK"
+        assert r.report["iterations"] == q.report["iterations"]
+        assert cuda.equal(r.lattice, q.lattice)
+        assert cuda.equal(r.im_normalized, q.im_normalized)
+
+
+@pytest.mark.parametrize("sub", [2, 3, 4])
+def test_sub_batches_match_one_pass(cuda, sub):
+    """Ten volumes of five shapes: 2, 3 and 4 sub-batches (uneven ranges for
+    3 and 4) against one pass, every volume bitwise."""
+    import n4b200
+    vols = _volumes(cuda, 10, 700)
+    one = n4b200.N4Batch(vols, _param(1), return_bias=True)
+    many = n4b200.N4Batch(vols, _param(sub), return_bias=True)
+    _same(cuda, one, many)
+    for r, q in zip(one, many):
+        assert cuda.equal(r.bias_field, q.bias_field)
+
+
+def test_sub_batches_in_a_graph_with_warm_start(cuda):
+    """The graph-recorded warm-started batch (the bench path), 3 sub-batches
+    against one pass, over two replays."""
+    import n4b200
+    from n4b200.warmstart import load_encoder
+    vols = _volumes(cuda, 9, 800)
+    enc = load_encoder(max_batch=16)
+    ref = n4b200.N4Batch(vols, _param(1), encoder=enc)
+    g = n4b200.N4BatchGraph(vols, _param(3), encoder=enc)
+    for _ in range(2):
+        g.launch()
+        _same(cuda, ref, g.sync())
+    g.close()
+
+
+def test_nonfinite_voxel_is_reported_on_its_own_volume(cuda):
+    """A non-finite voxel inside the mask of the third volume of a batch
+    fails that volume only (its sub-batch's prologue flags it by index)."""
+    import n4b200
+    from n4b200 import _lib
+    for sub in (1, 3):
+        vols = _volumes(cuda, 6, 900)
+        im, mk = vols[2]
+        idx = tuple(int(i) for i in np.argwhere(mk.cpu().numpy() != 0)[0])
+        im[idx] = float("inf")
+        ctx = n4b200.Context()
+        n4b200.N4Batch(vols, _param(sub), ctx=ctx, synchronous=False)
+        reps = (_lib.n4_report_t * len(vols))()
+        st = _lib.load().n4_sync(ctx.handle, reps, len(vols))
+        assert _lib.STATUS[st] == "N4_ERR_NONFINITE"
+        got = [_lib.STATUS[r.status] for r in reps]
+        assert got == ["N4_OK", "N4_OK", "N4_ERR_NONFINITE", "N4_OK", "N4_OK", "N4_OK"], (sub, got)
