@@ -778,6 +778,29 @@ void fill_descriptors(n4_context *ctx, const n4_params_t *p, Prepared &P, const 
   for (size_t k = 0; k < order.size(); ++k) ord[k] = order[k];
 }
 
+// k_prologue over the volumes [lo, hi) of a run: the vectorised variant for
+// shrink 2 or 4 when every row of those volumes is aligned for it, else the
+// scalar one (the same values either way).
+void launch_prologue(const n4_params_t *p, const Prepared &P, const DescBuf &B, int lo, int hi, long long g0,
+                     long long count, int blocks, cudaStream_t st) {
+  int S = (int)p->ShrinkFactor;
+  const bool u8 = (p->flags & N4_FLAG_MASK_U8) != 0;
+  if (S != 2 && S != 4) S = 0;
+  for (int i = lo; i < hi && S; ++i) {
+    const Dims &d = P.dims[i];
+    if ((long long)d.X * d.Y * d.Z >= (1ll << 31) || ((uintptr_t)P.rvs[i].im % (4 * S)) != 0 ||
+        (P.rvs[i].mask && ((uintptr_t)P.rvs[i].mask % (u8 ? S : 4 * S)) != 0))
+      S = 0;
+  }
+  const PrologueVol *pv = B.dp<PrologueVol>(P.o_pro) + lo;
+  const long long *pst = B.dp<long long>(P.o_pst) + lo;
+  int *flg = B.dp<int>(P.o_flg) + lo;
+  const int nb = std::max(blocks, 1);
+  if (S == 4) k_prologue<4><<<nb, 256, 0, st>>>(pv, pst, hi - lo, g0, count, p->low_value, flg);
+  else if (S == 2) k_prologue<2><<<nb, 256, 0, st>>>(pv, pst, hi - lo, g0, count, p->low_value, flg);
+  else k_prologue<0><<<nb, 256, 0, st>>>(pv, pst, hi - lo, g0, count, p->low_value, flg);
+}
+
 // Network inputs of the warm start from the prologue's fitting grids.
 n4_status_t enqueue_pool(n4_context *ctx, const Prepared &P, const DescBuf &B, __nv_bfloat16 *d_x, cudaStream_t st) {
   const long long cells = (long long)P.n * kPoolCells;
@@ -839,8 +862,6 @@ n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepa
   const int n = P.n;
   const long long *pst = B.hp<long long>(P.o_pst), *tst = B.hp<long long>(P.o_tst);
   int launches = 0;
-  // full grids for the prologues and corrections too: limited to the SMs the
-  // clusters leave free they fall behind the N4 launches (measured)
   k_axis_tables<<<3 * n, 256, 0, side>>>(B.dp<TableJob>(P.o_tab));
   CK(cudaGetLastError());
   CK(cudaEventRecord(ev[1], side));
@@ -850,8 +871,7 @@ n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepa
     const int lo = P.sub_lo[k], hi = P.sub_lo[k + 1], nk = hi - lo;
     const long long g0 = pst[lo], g1 = hi < n ? pst[hi] : P.fit_total;
     const int blocks = (int)std::min<long long>((g1 - g0 + 255) / 256, (long long)ctx->nsm * 16);
-    k_prologue<<<std::max(blocks, 1), 256, 0, side>>>(B.dp<PrologueVol>(P.o_pro) + lo, B.dp<long long>(P.o_pst) + lo,
-                                                       nk, g0, g1 - g0, p->low_value, B.dp<int>(P.o_flg) + lo);
+    launch_prologue(p, P, B, lo, hi, g0, g1 - g0, blocks, side);
     CK(cudaGetLastError());
     ++launches;
     if (p->ShrinkFactor > 1 && (p->flags & N4_FLAG_INPLACE_THRESH)) {
@@ -892,7 +912,7 @@ n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepa
     const long long t0 = tst[lo], t1 = hi < n ? tst[hi] : P.tiles;
     CK(cudaStreamWaitEvent(corr, ev[6 + k], 0));
     k_correct<<<(unsigned)(t1 - t0), 256, 0, corr>>>(B.dp<CorrectVol>(P.o_cor) + lo, B.dp<long long>(P.o_tst) + lo,
-                                                 hi - lo, t0, t1 - t0, p->low_value);
+                                                 hi - lo, t0, p->low_value);
     CK(cudaGetLastError());
     ++launches;
   }
@@ -917,8 +937,7 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
   {
     ++launches;
     const int blocks = (int)std::min<long long>((P.fit_total + 255) / 256, (long long)ctx->nsm * 16);
-    k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(B.dp<PrologueVol>(P.o_pro), B.dp<long long>(P.o_pst), n,
-                                                     0, P.fit_total, p->low_value, B.dp<int>(P.o_flg));
+    launch_prologue(p, P, B, 0, n, 0, P.fit_total, blocks, st);
     CK(cudaGetLastError());
     if (p->ShrinkFactor > 1 && (p->flags & N4_FLAG_INPLACE_THRESH)) {
       for (int i = 0; i < n; ++i) {
@@ -957,7 +976,7 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
   k_axis_tables<<<3 * n, 256, 0, st>>>(B.dp<TableJob>(P.o_tab));
   CK(cudaGetLastError());
   if (profile) TRY(prof_mark(ctx, 3, st));
-  k_correct<<<(unsigned)P.tiles, 256, 0, st>>>(B.dp<CorrectVol>(P.o_cor), B.dp<long long>(P.o_tst), n, 0, P.tiles,
+  k_correct<<<(unsigned)P.tiles, 256, 0, st>>>(B.dp<CorrectVol>(P.o_cor), B.dp<long long>(P.o_tst), n, 0,
                                                p->low_value);
   CK(cudaGetLastError());
   if (profile) TRY(prof_mark(ctx, 4, st));
@@ -1227,8 +1246,7 @@ n4_status_t n4_warm_inputs(n4_context_t *ctx, const n4_params_t *p, int n, const
   TRY(begin_run(ctx, st));
   CK(cudaMemcpyAsync(B.d, B.h, P.bytes, cudaMemcpyHostToDevice, st));
   const int blocks = (int)std::min<long long>((fit_total + 255) / 256, (long long)ctx->nsm * 16);
-  k_prologue<<<std::max(blocks, 1), 256, 0, st>>>(B.dp<PrologueVol>(P.o_pro), B.dp<long long>(P.o_pst), n, 0,
-                                                   fit_total, p->low_value, B.dp<int>(P.o_flg));
+  launch_prologue(p, P, B, 0, n, 0, fit_total, blocks, st);
   CK(cudaGetLastError());
   TRY(enqueue_pool(ctx, P, B, (__nv_bfloat16 *)d_x, st));
   u.slot->nrep = 0;
@@ -1638,7 +1656,7 @@ n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice, uns
   const size_t so = align_up(sizeof(cv), 16);
   const bool prof = ctx->profiling != 0;
   if (prof) TRY(prof_mark(ctx, 1, st));
-  k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0, tiles, 0.0f);
+  k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0, 0.0f);
   CK(cudaGetLastError());
   if (prof) { TRY(prof_mark(ctx, 2, st)); TRY(prof_mark(ctx, 3, st)); TRY(prof_mark(ctx, 4, st)); }
   ctx->prof_launches = 2;

@@ -47,43 +47,114 @@ __device__ __forceinline__ int find_volume(const long long *starts, int n, long 
   return lo;
 }
 
+// Rows of S consecutive voxels loaded as one vector: S floats, or S mask bytes.
+template <int S> struct VecF;
+template <> struct VecF<2> { using T = float2; };
+template <> struct VecF<4> { using T = float4; };
+template <int S> struct VecB;
+template <> struct VecB<2> { using T = uchar2; };
+template <> struct VecB<4> { using T = uchar4; };
+__device__ __forceinline__ float vget(const float2 &v, int i) { return i == 0 ? v.x : v.y; }
+__device__ __forceinline__ float vget(const float4 &v, int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
+__device__ __forceinline__ unsigned char vget(const uchar2 &v, int i) { return i == 0 ? v.x : v.y; }
+__device__ __forceinline__ unsigned char vget(const uchar4 &v, int i) {
+  return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+
 // Fitting voxels g0 .. g0 + total - 1 of a batch (numbered as in
 // PrologueVol::start) of the volumes vols[0 .. nvol); a non-finite voxel inside
-// the mask sets flag_nonfinite[v] of its volume v.
-__global__ void __launch_bounds__(256, 6) k_prologue(const PrologueVol *vols, const long long *starts, int nvol,
-                                                     long long g0, long long total, float low,
-                                                     int *flag_nonfinite) {
+// the mask sets flag_nonfinite[v] of its volume v.  S = 0: any shrink factor,
+// scalar loads.  S = 2 or 4: that shrink factor, every volume with fewer than
+// 2^31 fitting voxels and its rows of S voxels aligned to S floats (S bytes for
+// a byte mask): the block's S*S rows are read as one vector load per row and
+// array, all requested before they are summed, in the scalar path's order
+// (the same sums, bitwise).
+template <int S>
+__global__ void __launch_bounds__(256, S == 0 ? 6 : 4) k_prologue(const PrologueVol *vols, const long long *starts,
+                                                                  int nvol, long long g0, long long total, float low,
+                                                                  int *flag_nonfinite) {
   const long long end = g0 + total;
   for (long long gi = g0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; gi < end;
        gi += (long long)gridDim.x * blockDim.x) {
     const int v = find_volume(starts, nvol, gi);
     const PrologueVol &P = vols[v];
-    const long long li = gi - P.start;
-    const int z = (int)(li % P.Z), y = (int)((li / P.Z) % P.Y), x = (int)(li / ((long long)P.Z * P.Y));
-    const int s = P.s;
     float out;
-    if (s == 1) {
-      const float val = P.im[li];
-      const bool m = (P.mask ? mask_on(P.mask, P.mask_u8, li) : true) && val > low;
-      if (m && !isfinite(val)) atomicExch(flag_nonfinite + v, 1);
-      out = m ? logf(val) : __int_as_float(0x7fc00000);
-      if (P.im_w && !(val > low)) { P.im_w[li] = 0.0f; if (P.mask_w) mask_clear(P.mask_w, P.mask_u8, li); }
+    if constexpr (S == 0) {
+      const long long li = gi - P.start;
+      const int z = (int)(li % P.Z), y = (int)((li / P.Z) % P.Y), x = (int)(li / ((long long)P.Z * P.Y));
+      const int s = P.s;
+      if (s == 1) {
+        const float val = P.im[li];
+        const bool m = (P.mask ? mask_on(P.mask, P.mask_u8, li) : true) && val > low;
+        if (m && !isfinite(val)) atomicExch(flag_nonfinite + v, 1);
+        out = m ? logf(val) : __int_as_float(0x7fc00000);
+        if (P.im_w && !(val > low)) { P.im_w[li] = 0.0f; if (P.mask_w) mask_clear(P.mask_w, P.mask_u8, li); }
+      } else {
+        float sum = 0.0f;
+        int cnt = 0;
+        for (int dx = 0; dx < s; ++dx)
+          for (int dy = 0; dy < s; ++dy) {
+            const long long rowb = ((long long)(x * s + dx) * P.FY + (y * s + dy)) * P.FZ + (long long)z * s;
+            for (int dz = 0; dz < s; ++dz) {
+              const float val = P.im[rowb + dz];
+              const bool m = (P.mask ? mask_on(P.mask, P.mask_u8, rowb + dz) : true) && val > low;
+              if (m) { sum += val; ++cnt; if (!isfinite(val)) atomicExch(flag_nonfinite + v, 1); }
+            }
+          }
+        const float mean = cnt ? sum / (float)cnt : 0.0f;
+        out = (2 * cnt > s * s * s && mean > low) ? logf(mean) : __int_as_float(0x7fc00000);
+      }
+      P.imlog[li] = out;
     } else {
+      using VF = typename VecF<S>::T;
+      using VB = typename VecB<S>::T;
+      const unsigned li = (unsigned)(gi - P.start);
+      const unsigned Z = (unsigned)P.Z, Y = (unsigned)P.Y;
+      const unsigned q = li / Z, z = li - q * Z, x = q / Y, y = q - x * Y;
+      const size_t FY = (size_t)P.FY, FZ = (size_t)P.FZ;
+      // rows in batches of kB: the batch's loads are all requested before its
+      // values are summed; the mask becomes one bit per voxel on arrival
+      constexpr int kB = 4;
       float sum = 0.0f;
       int cnt = 0;
-      for (int dx = 0; dx < s; ++dx)
-        for (int dy = 0; dy < s; ++dy) {
-          const long long rowb = ((long long)(x * s + dx) * P.FY + (y * s + dy)) * P.FZ + (long long)z * s;
-          for (int dz = 0; dz < s; ++dz) {
-            const float val = P.im[rowb + dz];
-            const bool m = (P.mask ? mask_on(P.mask, P.mask_u8, rowb + dz) : true) && val > low;
-            if (m) { sum += val; ++cnt; if (!isfinite(val)) atomicExch(flag_nonfinite + v, 1); }
+      bool bad = false;
+#pragma unroll
+      for (int r0 = 0; r0 < S * S; r0 += kB) {
+        VF iv[kB];
+        unsigned bits = 0;
+#pragma unroll
+        for (int j = 0; j < kB; ++j) {
+          const int r = r0 + j;
+          const size_t rowb = ((size_t)(x * S + r / S) * FY + (y * S + r % S)) * FZ + (size_t)z * S;
+          iv[j] = *(const VF *)(P.im + rowb);
+          unsigned mb = (1u << S) - 1u;
+          if (P.mask && P.mask_u8) {
+            const VB m = *(const VB *)((const unsigned char *)P.mask + rowb);
+            mb = 0;
+#pragma unroll
+            for (int d = 0; d < S; ++d) mb |= (vget(m, d) != 0 ? 1u : 0u) << d;
+          } else if (P.mask) {
+            const VF m = *(const VF *)((const float *)P.mask + rowb);
+            mb = 0;
+#pragma unroll
+            for (int d = 0; d < S; ++d) mb |= (vget(m, d) != 0.0f ? 1u : 0u) << d;
           }
+          bits |= mb << (S * j);
         }
+#pragma unroll
+        for (int j = 0; j < kB; ++j)
+#pragma unroll
+          for (int d = 0; d < S; ++d) {
+            const float val = vget(iv[j], d);
+            const bool m = ((bits >> (S * j + d)) & 1u) && val > low;
+            if (m) { sum += val; ++cnt; bad |= !isfinite(val); }
+          }
+      }
+      if (bad) atomicExch(flag_nonfinite + v, 1);
       const float mean = cnt ? sum / (float)cnt : 0.0f;
-      out = (2 * cnt > s * s * s && mean > low) ? logf(mean) : __int_as_float(0x7fc00000);
+      out = (2 * cnt > S * S * S && mean > low) ? logf(mean) : __int_as_float(0x7fc00000);
+      P.imlog[li] = out;
     }
-    P.imlog[li] = out;
   }
 }
 
@@ -492,16 +563,13 @@ __device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long 
   }
 }
 
-// Tiles t0 .. t0 + ntiles - 1 of a batch, grid-stride (a grid of one CTA per
-// tile runs each CTA once).
+// Tile t0 + blockIdx.x of a batch (numbered as in CorrectVol::tile0) of the
+// volumes vols[0 .. nvol).
 __global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, const long long *tile_starts,
-                                                    int nvol, long long t0, long long ntiles, float low) {
+                                                    int nvol, long long t0, float low) {
   __shared__ float Gs[kRowsPerTile * kMaxNcz];
   __shared__ float Lx[2 * kLxMax];
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    if (t != blockIdx.x) __syncthreads();   // every thread is done with the previous tile's Gs
-    correct_tile(vols, tile_starts, nvol, t0 + t, low, Gs, Lx);
-  }
+  correct_tile(vols, tile_starts, nvol, t0 + blockIdx.x, low, Gs, Lx);
 }
 
 // ------------------------------------------------------------------ standalone fit

@@ -254,6 +254,39 @@ def test_nonfinite_input_is_reported(cuda):
         n4b200.N4(cuda.tensor(im, device="cuda"), cuda.tensor(ph.mask, device="cuda"), param(1, [2], 0.0))
 
 
+@pytest.mark.parametrize("shrink", [2, 4])
+@pytest.mark.parametrize("u8", [False, True])
+def test_vector_prologue_matches_scalar(cuda, shrink, u8):
+    """Shrink 2 and 4 read each block's rows with one vector load per row when
+    the image and mask are aligned for it, else with scalar loads; the same
+    volume at an aligned address and 4 bytes (1 byte for a byte mask) further
+    on corrects bitwise alike, and a non-finite voxel inside the mask is
+    reported by both."""
+    import n4b200
+    ph = make_phantom((64, 64, 48), seed=21)
+    n = ph.im.size
+    mask = (ph.mask.ravel() != 0).astype(np.uint8) if u8 else ph.mask.ravel().astype(np.float32)
+    res = []
+    for bad in (False, True):
+        for off in (0, 1):
+            ib = cuda.zeros(n + 8, device="cuda")
+            ib[off:off + n] = cuda.tensor(ph.im.ravel(), device="cuda")
+            mb = cuda.zeros(n + 8, dtype=cuda.uint8 if u8 else cuda.float32, device="cuda")
+            mb[off:off + n] = cuda.tensor(mask, device="cuda")
+            im, mk = ib[off:off + n].view(ph.im.shape), mb[off:off + n].view(ph.im.shape)
+            p = param(2, [6, 6], 0.0, ShrinkFactor=shrink)
+            if bad:
+                idx = tuple(int(i) for i in np.argwhere(ph.mask != 0)[len(np.argwhere(ph.mask != 0)) // 2])
+                im[idx] = float("inf")
+                with pytest.raises(n4b200.N4Error, match="NONFINITE"):
+                    n4b200.N4(im, mk, p)
+            else:
+                res.append(n4b200.N4(im, mk, p))
+    assert res[0].report["status"] == "N4_OK"
+    assert cuda.equal(res[0].lattice, res[1].lattice)
+    assert cuda.equal(res[0].im_normalized, res[1].im_normalized)
+
+
 def test_batch_graph_replays(cuda):
     """The graph-recorded batch equals N4Batch, and a launch after refilling
     an input in place corrects the new data."""
