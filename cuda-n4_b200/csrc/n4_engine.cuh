@@ -402,18 +402,39 @@ struct Engine {
   __device__ bool pass_a(bool need_cv, double st[4]) {
     float vmin = INFINITY, vmax = -INFINITY;
     double sy = 0.0, syy = 0.0;
-    const int n = nrow * Z;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const float v = imlog[i];
-      if (isnan(v)) continue;   // outside the mask
-      const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
-      const float lu = __fsub_rn(v, eval(G, rl, vz));
-      vmin = fminf(vmin, lu);
-      vmax = fmaxf(vmax, lu);
-      if (need_cv) {
-        const float y = expm1f(-eval(Gd, rl, vz));
-        sy += (double)y;
-        syy += (double)y * (double)y;
+    const int per = (int)blockDim.x / Z;   // whole rows per sweep: each thread keeps one z
+    if (per > 0) {
+      const int rs = (int)threadIdx.x / Z, vz = (int)threadIdx.x - rs * Z;
+      if (rs < per) {
+        const float4 w = az.w[vz];
+        const int sz = az.s[vz];
+        for (int rl = rs; rl < nrow; rl += per) {
+          const float v = imlog[rl * Z + vz];
+          if (isnan(v)) continue;   // outside the mask
+          const float lu = __fsub_rn(v, dot4(w, G + rl * ncz + sz));
+          vmin = fminf(vmin, lu);
+          vmax = fmaxf(vmax, lu);
+          if (need_cv) {
+            const float y = expm1f(-dot4(w, Gd + rl * ncz + sz));
+            sy += (double)y;
+            syy += (double)y * (double)y;
+          }
+        }
+      }
+    } else {
+      const int n = nrow * Z;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float v = imlog[i];
+        if (isnan(v)) continue;
+        const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
+        const float lu = __fsub_rn(v, eval(G, rl, vz));
+        vmin = fminf(vmin, lu);
+        vmax = fmaxf(vmax, lu);
+        if (need_cv) {
+          const float y = expm1f(-eval(Gd, rl, vz));
+          sy += (double)y;
+          syy += (double)y * (double)y;
+        }
       }
     }
     double loc[4];
@@ -436,22 +457,46 @@ struct Engine {
     __syncthreads();
     N4_MARK(PH_B_ZERO);
     unsigned *hc = hist + ((threadIdx.x >> 5) % kHistCopies) * bins;
-    const int n = nrow * Z;
-    for (int base = 0; base < n; base += blockDim.x) {
-      const int i = base + threadIdx.x;
-      int key = -1;
-      unsigned qlo = 0, qhi = 0;
-      if (i < n) {
-        const float v = imlog[i];
-        if (!isnan(v)) {
-          const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
-          const float lu = __fsub_rn(v, eval(G, rl, vz));
-          key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
+    const int per = (int)blockDim.x / Z;   // whole rows per sweep, as in pass A
+    if (per > 0) {
+      const int rs = (int)threadIdx.x / Z, vz = (int)threadIdx.x - rs * Z;
+      const float4 w = rs < per ? az.w[vz] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const int sz = rs < per ? az.s[vz] : 0;
+      const int sweeps = (nrow + per - 1) / per;
+      for (int k = 0; k < sweeps; ++k) {
+        const int rl = rs + k * per;
+        int key = -1;
+        unsigned qlo = 0, qhi = 0;
+        if (rs < per && rl < nrow) {
+          const float v = imlog[rl * Z + vz];
+          if (!isnan(v)) {
+            const float lu = __fsub_rn(v, dot4(w, G + rl * ncz + sz));
+            key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
+          }
+        }
+        if (key >= 0) {
+          atomicAdd(&hc[key], qlo);
+          if (qhi) atomicAdd(&hc[key + 1], qhi);
         }
       }
-      if (key >= 0) {
-        atomicAdd(&hc[key], qlo);
-        if (qhi) atomicAdd(&hc[key + 1], qhi);
+    } else {
+      const int n = nrow * Z;
+      for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        int key = -1;
+        unsigned qlo = 0, qhi = 0;
+        if (i < n) {
+          const float v = imlog[i];
+          if (!isnan(v)) {
+            const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
+            const float lu = __fsub_rn(v, eval(G, rl, vz));
+            key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
+          }
+        }
+        if (key >= 0) {
+          atomicAdd(&hc[key], qlo);
+          if (qhi) atomicAdd(&hc[key + 1], qhi);
+        }
       }
     }
     __syncthreads();
