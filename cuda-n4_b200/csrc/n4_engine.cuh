@@ -212,6 +212,36 @@ struct Engine {
     }
   }
 
+  // rowtab(la, Ga) and rowtab(lb, Gb) in one sweep (the same operations per
+  // entry; the row's spans and weights are read once for both)
+  __device__ void rowtab2(const float *la, float *Ga, const float *lb, float *Gb) {
+    const int ntask = nrow * ncz;
+    for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
+      const int rl = t / ncz, cz = t - rl * ncz;
+      int vx, vy;
+      row_xy(rl, vx, vy);
+      const int sx = ax.s[vx], sy = ay.s[vy];
+      const float4 wx = ax.w[vx], wy = ay.w[vy];
+      const float wxa[4] = {wx.x, wx.y, wx.z, wx.w};
+      const float wya[4] = {wy.x, wy.y, wy.z, wy.w};
+      float acca = 0.0f, accb = 0.0f;
+#pragma unroll
+      for (int jx = 0; jx < 4; ++jx) {
+        const int o = ((sx + jx) * ncy + sy) * ncz + cz;
+        float sa = 0.0f, sb = 0.0f;
+#pragma unroll
+        for (int jy = 0; jy < 4; ++jy) {
+          sa = __fmaf_rn(wya[jy], la[o + jy * ncz], sa);
+          sb = __fmaf_rn(wya[jy], lb[o + jy * ncz], sb);
+        }
+        acca = __fmaf_rn(wxa[jx], sa, acca);
+        accb = __fmaf_rn(wxa[jx], sb, accb);
+      }
+      Ga[t] = acca;
+      Gb[t] = accb;
+    }
+  }
+
   __device__ __forceinline__ float eval(const float *Gt, int rl, int vz) const {
     return dot4(az.w[vz], Gt + rl * ncz + az.s[vz]);
   }
@@ -241,12 +271,25 @@ struct Engine {
   }
 
   // Sum of every CTA's `mine[0..n)` into `out` (shared), identical in all
-  // CTAs: each CTA reduces one slice over all peers (fixed order), then every
-  // CTA gathers the slices.  Slices live in a buffer of their own, so a CTA
-  // may modify `out` while slower peers are still gathering.
+  // CTAs, each entry summed over the CTAs in rank order.  Cluster: after one
+  // barrier every CTA reads all K partials through DSMEM (a partial is written
+  // again only after later barriers of the iteration, by which time every
+  // peer has read it).  Grid: each CTA reduces one slice over all peers, then
+  // every CTA gathers the slices; slices live in a buffer of their own, so a
+  // CTA may modify `out` while slower peers are still gathering.
   template <class T>
   __device__ bool allreduce(const T *mine, T *out, int n) {
     if (!g.sync()) return false;
+    if (!Group::kGrid) {
+      for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        T acc = 0;
+#pragma unroll 4
+        for (int k = 0; k < K; ++k) acc += *(g.peer(mine, k) + c);
+        out[c] = acc;
+      }
+      __syncthreads();
+      return true;
+    }
     const int per = (n + K - 1) / K;
     const int c0 = rank * per, c1 = min(n, c0 + per);
     T *slice = Group::kGrid ? (T *)red_global : (T *)(big + pl.b_slice);
@@ -645,8 +688,7 @@ struct Engine {
         if (use_warm) {
           for (int c = threadIdx.x; c < nlat; c += blockDim.x) { L[c] = aux[c]; D[c] = tmp[c]; }
           __syncthreads();
-          rowtab(L, G);
-          rowtab(D, Gd);
+          rowtab2(L, G, D, Gd);
           __syncthreads();
         }
         cv = use_warm ? cvs[0] : cvs[1];
@@ -666,8 +708,7 @@ struct Engine {
         if (!fit_step(st)) goto timeout;
         for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] += D[c];
         __syncthreads();
-        rowtab(D, Gd);
-        rowtab(L, G);
+        rowtab2(L, G, D, Gd);
         __syncthreads();
         N4_MARK(PH_UPDATE);
         ++it;
