@@ -7,10 +7,11 @@ One step = one batch of B synthetic 256x256x176 phantoms (shrink 4, 4 levels,
 <= 50 iterations per level, convergence 0.001, 200 bins, FWHM 0.15, Wiener
 0.01) bias-corrected to convergence: the masked log volumes are pooled to
 32x32x24, the learned encoder predicts every volume's first-level lattice,
-and the batch runs in one persistent launch with those warm lattices,
-recorded once as a CUDA graph (``n4_batch_graph_*``) and replayed.  The
-cluster size of the batch is chosen by the autotuner (``n4_autotune``,
-untimed, before the warm-up).  ``value`` is whole-job volumes/s of that
+and the batch runs as persistent cluster launches with those warm lattices
+(overlapped sub-batches: each sub-batch's prologue, warm start and correction
+run beside the other sub-batches' N4 launches), recorded once as a CUDA graph
+(``n4_batch_graph_*``) and replayed.  The cluster size of the batch is chosen
+by the autotuner (``n4_autotune``, untimed, before the warm-up).  ``value`` is whole-job volumes/s of that
 batched + warm-started path with the inputs resident in HBM.  Beside it:
 ``batched_plain`` (the same graph without warm start), ``batched_without_graph``
 (``n4_run_batched`` at every step), ``plain`` (``n4_run``, one volume per
