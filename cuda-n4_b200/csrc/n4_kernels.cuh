@@ -372,7 +372,7 @@ struct CorrectVol {
   int vec4;              // FZ % 4 == 0 and every pointer 16-byte aligned
 };
 
-constexpr int kRowsPerTile = 64;
+constexpr int kRowsPerTile = 128;
 constexpr int kMaxNcz = 64;
 constexpr int kLxMax = 2048;    // x-contracted lattice slice ncy*ncz held per x-plane
 
