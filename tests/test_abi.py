@@ -96,3 +96,22 @@ def test_create_reports_missing_device():
     h = C.c_void_p()
     assert lib.n4_create(C.byref(h), 0) == 9   # N4_ERR_NO_DEVICE
     assert lib.n4_destroy(None) == 0
+
+
+def test_python_flags_match_the_header():
+    """Every N4_FLAG_* constant of the Python binding has the header's value
+    (the parametrised ones for every argument)."""
+    from n4b200 import _lib
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    consts = dict(re.findall(r"#define\s+N4_FLAG_([A-Z0-9_]+)\s+(0x[0-9a-fA-F]+)u", src))
+    assert consts, "no flag constants found"
+    for name, value in consts.items():
+        assert getattr(_lib, "FLAG_" + name) == int(value, 16), name
+    pattern = r"#define\s+N4_FLAG_([A-Z0-9_]+)\(k\)\s+\(\(\(unsigned int\)\(k\) & (\d+)u\) << (\d+)\)"
+    shifts = {name: (int(mask), int(shift)) for name, mask, shift in re.findall(pattern, src)}
+    assert "SUB_BATCHES" in shifts and "CLUSTER_SIZE" in shifts
+    import n4b200
+    for k in range(8):
+        assert _lib.FLAG_SUB_BATCHES(k) == (k & shifts["SUB_BATCHES"][0]) << shifts["SUB_BATCHES"][1]
+    for k in range(17):
+        assert n4b200.cluster_size_flag(k) == (k & shifts["CLUSTER_SIZE"][0]) << shifts["CLUSTER_SIZE"][1]
