@@ -846,11 +846,13 @@ n4_status_t ensure_pipe(n4_context *ctx) {
 
 // A cluster-path batch as P.nsub sub-batches (descriptors already on the
 // device; capturable).  Sub-batch k's N4 launch waits only for its own
-// prologue and warm start, and runs on high-priority stream pipe[k % 2], so
-// that it takes the SMs the previous launch frees; the prologues, pooling and
-// encoder calls run in order on pipe[2] and the corrections on pipe[3], at
-// low priority, on the SMs the clusters leave free.  Every kernel reads and
-// writes only its own volumes' buffers; st waits for all four streams.
+// prologue and warm start, and runs on stream pipe[k % 2], so that it can
+// start on the SMs the previous launch frees while that launch's last volumes
+// finish; the prologues, pooling and encoder calls run in order on pipe[2]
+// and the corrections on pipe[3], on the SMs the clusters leave free (the N4
+// streams have the higher priority; measured, it makes no difference).
+// Every kernel reads and writes only its own volumes' buffers; st waits for
+// all four streams.
 n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepared &P, const DescBuf &B,
                               cudaStream_t st) {
   TRY(ensure_pipe(ctx));
