@@ -192,6 +192,8 @@ n4_status_t make_dims(const n4_params_t *p, unsigned fx, unsigned fy, unsigned f
   if (fx == 0 || fy == 0 || fz == 0) return fail(N4_ERR_INVALID_ARG, "empty volume");
   if (fx % s || fy % s || fz % s) return fail(N4_ERR_INVALID_ARG, "dimensions must be multiples of ShrinkFactor");
   if ((unsigned long long)fx * fy * fz >= (1ull << 40)) return fail(N4_ERR_TOO_LARGE, "volume too large");
+  // the correction indexes full-resolution rows (fx * fy of them) in 32 bits
+  if ((unsigned long long)fx * fy >= (1ull << 32)) return fail(N4_ERR_TOO_LARGE, "more than 2^32 - 1 rows (fx * fy)");
   d.FX = (int)fx; d.FY = (int)fy; d.FZ = (int)fz;
   d.X = (int)(fx / s); d.Y = (int)(fy / s); d.Z = (int)(fz / s);
   if (d.Z > 1024) return fail(N4_ERR_TOO_LARGE, "fitting grid rows longer than 1024 voxels (raise ShrinkFactor)");
@@ -1068,6 +1070,15 @@ n4_status_t n4_lattice_dims(const n4_params_t *p, unsigned int dims[3], size_t *
   return N4_OK;
 }
 
+n4_status_t n4_fitting_dims(const n4_params_t *p, unsigned int fx, unsigned int fy, unsigned int fz,
+                            unsigned int dims[3]) {
+  TRY(check_params(p));
+  Dims d;
+  TRY(make_dims(p, fx, fy, fz, d));
+  if (dims) { dims[0] = (unsigned)d.X; dims[1] = (unsigned)d.Y; dims[2] = (unsigned)d.Z; }
+  return N4_OK;
+}
+
 const char *n4_status_string(int s) {
   switch (s) {
     case N4_OK: return "ok";
@@ -1582,6 +1593,20 @@ static void launch_fit_rows(const float *field, const float *mask, long long row
                                                                                    t1d);
 }
 
+// Sizes a standalone fit accepts: every extent below 2^31 (the kernels take
+// them as int), at most 2^36 field voxels and 4096 control points per axis,
+// so that the row and plane sums (fx*fy*ncpt_z, fx*ncpt_y*ncpt_z floats)
+// cannot wrap.
+static n4_status_t check_fit_sizes(unsigned ncpt_x, unsigned ncpt_y, unsigned ncpt_z, unsigned fx, unsigned fy,
+                                   unsigned fz) {
+  if (ncpt_x < 4 || ncpt_y < 4 || ncpt_z < 4 || !fx || !fy || !fz) return fail(N4_ERR_INVALID_ARG, "bad sizes");
+  if (fx > 0x7fffffffu || fy > 0x7fffffffu || fz > 0x7fffffffu) return fail(N4_ERR_TOO_LARGE, "extent >= 2^31");
+  if ((unsigned long long)fx * fy * fz >= (1ull << 36)) return fail(N4_ERR_TOO_LARGE, "field too large");
+  if (ncpt_x > 4096 || ncpt_y > 4096 || ncpt_z > 4096)
+    return fail(N4_ERR_TOO_LARGE, "more than 4096 control points along an axis");
+  return N4_OK;
+}
+
 static n4_status_t component_tables(n4_context_t *ctx, unsigned fx, unsigned fy, unsigned fz, unsigned nx, unsigned ny,
                                     unsigned nz, cudaStream_t st, Axis &ax, Axis &ay, Axis &az) {
   const size_t bx = align_up(axis_bytes(fx, nx - 3), 256), by = align_up(axis_bytes(fy, ny - 3), 256),
@@ -1608,8 +1633,7 @@ n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const floa
                              unsigned int ncpt_y, unsigned int ncpt_z, unsigned int fx, unsigned int fy,
                              unsigned int fz, float eps, int zero_den, float *d_lattice, void *stream) {
   if (!ctx || !d_field || !d_lattice) return fail(N4_ERR_INVALID_ARG, "NULL pointer");
-  if (ncpt_x < 4 || ncpt_y < 4 || ncpt_z < 4 || !fx || !fy || !fz) return fail(N4_ERR_INVALID_ARG, "bad sizes");
-  if ((unsigned long long)fx * fy * fz >= (1ull << 36)) return fail(N4_ERR_TOO_LARGE, "field too large");
+  TRY(check_fit_sizes(ncpt_x, ncpt_y, ncpt_z, fx, fy, fz));
   cudaStream_t st = (cudaStream_t)stream;
   Axis ax, ay, az;
   TRY(component_tables(ctx, fx, fy, fz, ncpt_x, ncpt_y, ncpt_z, st, ax, ay, az));
@@ -1750,8 +1774,40 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = 8u << 20;   // 8 MiB per device
 static __device__ __align__(256) unsigned char g_fit_scratch[kNoAllocScratchBytes];
 
+// The array's device address, looked up once per CUDA context: a context
+// made after cudaDeviceReset loads the module again, possibly elsewhere, so
+// the cached address is keyed by the context's process-unique id as well as
+// the device ordinal.
 constexpr int kMaxDevices = 64;
-std::atomic<void *> g_fit_scratch_ptr[kMaxDevices];
+struct ScratchAddr {
+  unsigned long long ctx_id = 0;   // 0: not looked up yet
+  void *ptr = nullptr;
+};
+ScratchAddr g_fit_scratch_addr[kMaxDevices];
+std::mutex g_fit_scratch_mu;
+
+// Unique id of the current CUDA context (cuCtxGetCurrent + cuCtxGetId through
+// the runtime's driver entry points, so the library needs no -lcuda).
+n4_status_t current_context_id(unsigned long long *id) {
+  using GetCurrent = int (*)(void **);
+  using GetId = int (*)(void *, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    void *a = nullptr, *b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+        qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess)
+      return fail(N4_ERR_CUDA, "cuCtxGetCurrent/cuCtxGetId not available from the driver");
+    get_current = (GetCurrent)a;
+    get_id = (GetId)b;
+  }
+  void *ctx = nullptr;
+  if (get_current(&ctx) != 0 || !ctx) return fail(N4_ERR_CUDA, "no current CUDA context");
+  if (get_id(ctx, id) != 0) return fail(N4_ERR_CUDA, "cuCtxGetId failed");
+  return N4_OK;
+}
 
 // The three tables of one call, passed by value (no descriptor upload).
 __global__ void k_axis_tables_by_value(TableJob jx, TableJob jy, TableJob jz) {
@@ -1767,7 +1823,7 @@ n4_status_t n4_fit_bspline3d_noalloc(const float *d_field, const float *d_mask, 
                                      unsigned int ncpt_y, unsigned int ncpt_z, unsigned int fx, unsigned int fy,
                                      unsigned int fz, float eps, int zero_den, float *d_lattice, void *stream) {
   if (!d_field || !d_lattice) return fail(N4_ERR_INVALID_ARG, "NULL pointer");
-  if (ncpt_x < 4 || ncpt_y < 4 || ncpt_z < 4 || !fx || !fy || !fz) return fail(N4_ERR_INVALID_ARG, "bad sizes");
+  TRY(check_fit_sizes(ncpt_x, ncpt_y, ncpt_z, fx, fy, fz));
   const size_t bx = align_up(axis_bytes(fx, ncpt_x - 3), 256), by = align_up(axis_bytes(fy, ncpt_y - 3), 256),
                bz = align_up(axis_bytes(fz, ncpt_z - 3), 256);
   const size_t t1 = (size_t)fx * fy * ncpt_z, t2 = (size_t)fx * ncpt_y * ncpt_z;
@@ -1782,12 +1838,20 @@ n4_status_t n4_fit_bspline3d_noalloc(const float *d_field, const float *d_mask, 
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return fail(N4_ERR_INVALID_ARG, "device ordinal out of range");
-  char *base = (char *)g_fit_scratch_ptr[dev].load(std::memory_order_acquire);
-  if (!base) {   // once per device: the scratch's device address
-    void *p = nullptr;
-    CK(cudaGetSymbolAddress(&p, g_fit_scratch));
-    g_fit_scratch_ptr[dev].store(p, std::memory_order_release);
-    base = (char *)p;
+  CK(cudaSetDevice(dev));   // makes the device's primary context current (CUDA 12 initialises it here)
+  unsigned long long cid = 0;
+  TRY(current_context_id(&cid));
+  char *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_fit_scratch_mu);
+    ScratchAddr &a = g_fit_scratch_addr[dev];
+    if (a.ctx_id != cid) {   // once per device and context: the scratch's device address
+      void *p = nullptr;
+      CK(cudaGetSymbolAddress(&p, g_fit_scratch));
+      a.ptr = p;
+      a.ctx_id = cid;
+    }
+    base = (char *)a.ptr;
   }
   cudaStream_t st = (cudaStream_t)stream;
   const TableJob jx{base, (int)fx, (int)ncpt_x}, jy{base + bx, (int)fy, (int)ncpt_y},

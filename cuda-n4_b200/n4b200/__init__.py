@@ -122,6 +122,17 @@ def lattice_dims(param: N4Param):
     return tuple(int(d) for d in dims)
 
 
+def fitting_dims(param: N4Param, shape):
+    """Fitting-grid dimensions of a volume of ``shape`` (full size divided by
+    the shrink factor), after the same size checks ``N4`` makes; raises
+    ``N4Error`` for a volume ``N4`` would reject.  Needs no GPU."""
+    dims = (C.c_uint * 3)()
+    c = param.to_c()
+    fx, fy, fz = (int(d) for d in shape)
+    check(_lib.load().n4_fitting_dims(C.byref(c), fx, fy, fz, dims))
+    return tuple(int(d) for d in dims)
+
+
 # ---------------------------------------------------------------- context
 class Context:
     """Owns the device workspaces of n4b200 (``n4_create`` / ``n4_destroy``)."""

@@ -100,6 +100,7 @@ _U = C.c_uint
 SIGNATURES = [
     ("n4_params_default", None, [C.POINTER(n4_params_t)]),
     ("n4_lattice_dims", C.c_int, [C.POINTER(n4_params_t), C.POINTER(C.c_uint), C.POINTER(C.c_size_t)]),
+    ("n4_fitting_dims", C.c_int, [C.POINTER(n4_params_t), C.c_uint, C.c_uint, C.c_uint, C.POINTER(C.c_uint)]),
     ("n4_status_string", C.c_char_p, [C.c_int]),
     ("n4_last_error_string", C.c_char_p, []),
     ("n4_version", C.c_char_p, []),

@@ -114,6 +114,13 @@ void n4_params_default(n4_params_t *p);
  * (cudaN4.h:359, main.cpp:87-92). */
 n4_status_t n4_lattice_dims(const n4_params_t *p, unsigned int dims[3], size_t *count);
 
+/* No counterpart in the reference (it has no shrink factor).  Checks a
+ * volume of fx*fy*fz voxels against the parameters exactly as n4_run does
+ * before it touches the GPU (shrink divisibility, size limits) and returns
+ * the fitting-grid dimensions (fx, fy, fz) / ShrinkFactor.  Needs no GPU. */
+n4_status_t n4_fitting_dims(const n4_params_t *p, unsigned int fx, unsigned int fy, unsigned int fz,
+                            unsigned int dims[3]);
+
 const char *n4_status_string(int status);
 /* Message of the last failed call on this thread. */
 const char *n4_last_error_string(void);
@@ -231,8 +238,11 @@ n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const floa
  * 8 MiB device array per device, which holds the axis tables plus
  * fx*fy*ncpt_z*8 + fx*ncpt_y*ncpt_z*8 bytes (e.g. 256x256 rows with up to
  * 15 control points along z); larger fits return N4_ERR_TOO_LARGE and need
- * n4_fit_bspline3d.  The first call on a device looks up the array's address
- * (make it before any stream capture).  Calls on one device share the
+ * n4_fit_bspline3d.  The first call on a device (and again the first one in
+ * a context made after cudaDeviceReset) looks up the array's address; make
+ * it before any stream capture.  That first call may also be the one that
+ * loads the library's device code (lazy module loading), which is when the
+ * 8 MiB are reserved; later calls reserve nothing.  Calls on one device share the
  * scratch: two calls that may overlap in time (different streams or host
  * threads) race and must be ordered by the caller.  Runs on the current
  * device, asynchronously on `stream`. */

@@ -136,9 +136,12 @@ def n4_c1(ref) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("N4_REFERENCE_DIR"),
+                    help="checkout of JiancongWang/CUDA-N4 holding N4.py (or set N4_REFERENCE_DIR)")
     ap.add_argument("--c1", action="store_true")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give --reference <checkout of the reference> or set N4_REFERENCE_DIR")
     ref = load_reference(a.reference)
     if a.c1:
         np.savez_compressed(os.path.join(HERE, "n4_c1.npz"), **n4_c1(ref))

@@ -79,6 +79,46 @@ def test_validation_without_a_gpu():
         n4b200.N4Param(NotAField=1)
 
 
+def test_volume_size_checks_without_a_gpu():
+    """The size checks of a run (shrink divisibility, voxel and row limits)
+    happen on the host before any device work."""
+    import n4b200
+    from n4b200 import N4Error
+    p = n4b200.N4Param(ShrinkFactor=4)
+    assert n4b200.fitting_dims(p, (256, 256, 176)) == (64, 64, 44)
+    assert n4b200.fitting_dims(n4b200.N4Param(ShrinkFactor=2), (512, 512, 320)) == (256, 256, 160)
+    with pytest.raises(N4Error, match="INVALID_ARG"):
+        n4b200.fitting_dims(p, (256, 256, 174))          # not a multiple of the shrink factor
+    with pytest.raises(N4Error, match="INVALID_ARG"):
+        n4b200.fitting_dims(p, (0, 256, 176))
+    # 65536 x 65536 x 8 (2^35 voxels, 34 GB): fewer than 2^40 voxels, but
+    # 2^32 rows, which the full-resolution correction cannot index
+    with pytest.raises(N4Error, match="TOO_LARGE"):
+        n4b200.fitting_dims(p, (65536, 65536, 8))
+    assert n4b200.fitting_dims(p, (65532, 65536, 8)) == (16383, 16384, 2)
+    with pytest.raises(N4Error, match="TOO_LARGE"):
+        n4b200.fitting_dims(n4b200.N4Param(ShrinkFactor=1), (64, 64, 2048))   # fitting rows > 1024
+
+
+def test_fit_size_checks_precede_device_work():
+    """Both standalone fits reject extents of 2^31 or more, more than 2^36
+    field voxels and more than 4096 control points along an axis before any
+    CUDA call (the pointers below are never dereferenced)."""
+    import n4b200
+    from n4b200 import _lib
+    lib = n4b200.library()
+    fake = C.c_void_p(256)
+    cases = [((4, 4, 4), (1 << 31, 1, 1)),          # extent above INT_MAX
+             ((4, 4, 4), (1 << 20, 1 << 16, 1)),    # 2^36 voxels
+             ((4, 4, 5000), (64, 64, 64))]          # control points per axis
+    for nc, dims in cases:
+        st = lib.n4_fit_bspline3d_noalloc(fake, None, *nc, *dims, 1e-3, 0, fake, None)
+        assert _lib.STATUS[st] == "N4_ERR_TOO_LARGE", (nc, dims)
+        # the allocating fit checks sizes before it touches its (here fake) context
+        st = lib.n4_fit_bspline3d(fake, fake, None, *nc, *dims, 1e-3, 0, fake, None)
+        assert _lib.STATUS[st] == "N4_ERR_TOO_LARGE", (nc, dims)
+
+
 def test_status_strings():
     import n4b200
     lib = n4b200.library()

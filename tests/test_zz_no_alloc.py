@@ -78,3 +78,41 @@ def test_largest_fit_the_scratch_holds(cuda):
         ref = n4b200.FitBspline3D(f, m, nc)
         cuda.cuda.synchronize()
         assert cuda.equal(got, ref)
+
+
+@pytest.mark.gpu
+def test_calls_after_the_first_reserve_no_device_memory(cuda):
+    """The point of the entry point: once the library's device code is loaded
+    (the first call of each kernel variant may load it, and with it the fixed
+    scratch array), further calls of any size leave the device's free memory
+    unchanged.  Inputs and outputs are allocated before the first sample."""
+    rng = np.random.default_rng(33)
+    cases = [((64, 64, 44), (11, 11, 11), True), ((96, 80, 60), (7, 5, 9), False), ((40, 48, 36), (4, 6, 5), True)]
+    bufs = []
+    for shape, nc, with_mask in cases:
+        f = cuda.tensor(rng.normal(0.0, 0.3, size=shape).astype(np.float32), device="cuda")
+        m = cuda.tensor((rng.random(shape) < 0.7).astype(np.float32), device="cuda") if with_mask else None
+        out = cuda.empty(nc, dtype=cuda.float32, device="cuda")
+        bufs.append((f, m, nc, out))
+    L = _lib()
+    lib = L.load()
+
+    def call(f, m, nc, out):
+        X, Y, Z = f.shape
+        L.check(lib.n4_fit_bspline3d_noalloc(f.data_ptr(), None if m is None else m.data_ptr(), *nc, X, Y, Z,
+                                             1e-3, 0, out.data_ptr(),
+                                             cuda.cuda.current_stream(f.device).cuda_stream))
+
+    for b in bufs:            # warm-up: every kernel variant the later calls use
+        call(*b)
+    cuda.cuda.synchronize()
+    free0, _ = cuda.cuda.mem_get_info()
+    firsts = [b[3].clone() for b in bufs]
+    for _ in range(3):
+        for b in bufs:
+            call(*b)
+    cuda.cuda.synchronize()
+    free1, _ = cuda.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    for b, first in zip(bufs, firsts):
+        assert cuda.equal(b[3], first)
