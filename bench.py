@@ -16,9 +16,11 @@ batched + warm-started path with the inputs resident in HBM.  Beside it:
 ``batched_plain`` (the same graph without warm start), ``batched_without_graph``
 (``n4_run_batched`` at every step), ``plain`` (``n4_run``, one volume per
 call: the single-volume path the batched one is compared with), and ``e2e``
-(the headline path through the public API with the inputs copied from pinned
-host memory and the corrected volumes and lattices copied back inside the
-timed region).
+(the same warm-started batched correction through ``n4_run_batched_host``:
+images and float masks in pinned host memory, corrected volumes and lattices
+back into pinned host memory, the library overlapping the uploads, runs and
+downloads of sub-batches of 8 volumes; its device time runs from the first
+upload to the last download of every step).
 
 Multi-GPU: one process per GPU (torchrun); volumes are independent, so each
 rank corrects its own batch (replicas, weak scaling, no collective on the data
@@ -261,11 +263,41 @@ def measure_c3(dev, ctx, reps=2):
             "path": res.report["path"], "ctas": res.report["cluster_size"]}
 
 
+def schedule_summary(reports, fit_voxels):
+    """How a batched run used its clusters, from the per-volume device
+    timestamps of the reports: a persistent cluster keeps its SMs, so the SM
+    of a volume's leading CTA names its cluster.  makespan = first begin to
+    last end; per cluster, busy = sum of its volumes' times; tail = makespan
+    minus the mean cluster finish (the time clusters sit idle at the end on
+    average); ns_per_voxel_iteration relates each volume's time to its work."""
+    import numpy as np
+    rs = [r for r in reports if r.get("device_end_ns")]
+    if not rs:
+        return {}
+    t0 = min(r["device_begin_ns"] for r in rs)
+    t1 = max(r["device_end_ns"] for r in rs)
+    by = {}
+    for r in rs:
+        by.setdefault(r["sm"], []).append(r)
+    fin = [max(r["device_end_ns"] for r in v) - t0 for v in by.values()]
+    busy = [sum(r["device_end_ns"] - r["device_begin_ns"] for r in v) for v in by.values()]
+    work = np.array([fv * sum(r["iterations"][:r["levels"]]) for r, fv in zip(reports, fit_voxels)
+                     if r.get("device_end_ns")], dtype=np.float64)
+    dur = np.array([r["device_end_ns"] - r["device_begin_ns"] for r in rs], dtype=np.float64)
+    return {"clusters": len(by), "makespan_ms": (t1 - t0) / 1e6, "mean_cluster_finish_ms": float(np.mean(fin)) / 1e6,
+            "mean_cluster_busy_ms": float(np.mean(busy)) / 1e6, "max_cluster_busy_ms": float(np.max(busy)) / 1e6,
+            "tail_ms": ((t1 - t0) - float(np.mean(fin))) / 1e6,
+            "volume_ms_min_median_max": [float(np.min(dur)) / 1e6, float(np.median(dur)) / 1e6,
+                                         float(np.max(dur)) / 1e6],
+            "ns_per_voxel_iteration_median": float(np.median(dur / np.maximum(work, 1.0)))}
+
+
 def measure_c4(dev, enc, n=48, reps=5):
     """48 phantoms with every axis drawn from 96, 104, ..., 288 (4^3-grid bias
     N(0, 0.15^2), Rician 0.03), shrink 4, 4 levels, <= 50 iterations,
     convergence 0.001: one batched run each, with and without the learned
     warm start, after autotuning the batch."""
+    import numpy as np
     import torch
     import n4b200
     from n4b200.phantom import batch_dims
@@ -293,9 +325,11 @@ def measure_c4(dev, enc, n=48, reps=5):
             torch.cuda.synchronize(dev)
             times.append(e0.elapsed_time(e1))
         ms = sorted(times)[len(times) // 2]
+        fv = [int(np.prod(n4b200.fitting_dims(p, tuple(im.shape)))) for im, _ in vols]
         out[name] = {"volumes_per_s": n * 1000.0 / ms, "ms_per_batch_median": ms, "ms_per_batch_all": times,
                      "iterations_per_volume": sum(sum(r.report["iterations"][:r.report["levels"]]) for r in res) / n,
-                     "paths": {k: sum(1 for r in res if r.report["path"] == k) for k in ("cluster", "grid")}}
+                     "paths": {k: sum(1 for r in res if r.report["path"] == k) for k in ("cluster", "grid")},
+                     "schedule": schedule_summary([r.report for r in res], fv)}
     ctx.close()
     return out
 
@@ -380,14 +414,16 @@ def run_ours(args, rank, world, local_rank):
     graph.sync()
     ms_gplain = max_over_ranks(e0.elapsed_time(e1))
     # warm-started vs plain: log-bias difference at full resolution over the
-    # mask, without its mean (a constant log bias is a global intensity scale
-    # that the convergence measure std/mean of exp(change) does not see)
+    # mask, as it is (raw) and without its mean (a constant log bias is a
+    # global intensity scale that the convergence measure std/mean of
+    # exp(change) does not see, so N4 never corrects it)
     dims = n4b200.lattice_dims(p)
-    dmax = 0.0
+    draw, dcent = [], []
     for i, r in enumerate(res):
         d = n4b200.EvaluateBspline3D(lat_w[i] - r.lattice, dims, SHAPE, ctx=ctx)
         inside = d[vols_dev[i][1] != 0]
-        dmax = max(dmax, float((inside - inside.double().mean().float()).abs().max()))
+        draw.append(float(inside.abs().max()))
+        dcent.append(float((inside - inside.double().mean().float()).abs().max()))
     graph.close()
     warm.close()
 
@@ -435,59 +471,34 @@ def run_ours(args, rank, world, local_rank):
     ms_plain = max_over_ranks(e0.elapsed_time(e1))
     plain = world * B * args.steps / (ms_plain / 1000.0)
 
-    # ---- end to end: pinned host inputs -> device -> batched N4 -> host outputs,
-    # pipelined in sub-batches over 3 streams (one context each) so that the
-    # host<->device copies of one sub-batch overlap the kernels of another
-    nsub = 4 if B % 4 == 0 else 1
-    per = B // nsub
-    streams = [torch.cuda.Stream(dev) for _ in range(3)]
-    ctxs = [n4b200.Context(local_rank) for _ in range(3)]
-    dev_in = [(torch.empty_like(a, device=dev), torch.empty_like(b, device=dev)) for a, b in vols_host]
-    out_h = [torch.empty_like(a).pin_memory() for a, _ in vols_host]
+    # ---- end to end through n4_run_batched_host: pinned host inputs ->
+    # staging -> batched N4 (warm start) -> pinned host outputs, uploads,
+    # runs and downloads of its sub-batches overlapped by the library; the
+    # device time of each call runs from its first upload to its last download
+    out_h = [torch.empty(a.shape, dtype=torch.float32).pin_memory() for a, _ in vols_host]
     lat_h = [torch.empty(n4b200.lattice_dims(p), dtype=torch.float32).pin_memory() for _ in vols_host]
+    hctx = n4b200.Context(local_rank)
+    henc = load_encoder(max_batch=16)
 
-    for (ih, mh), (idv, mdv) in zip(vols_host, dev_in):
-        idv.copy_(ih)
-        mdv.copy_(mh)
-    for c2 in ctxs:
-        n4b200.autotune(dev_in[:per], p, ctx=c2)
-    encs = [load_encoder(max_batch=per) for _ in range(3)]      # one per stream: an encoder serves one run at a time
-
-    def step_e2e(host, dev_vols):
-        for k in range(nsub):
-            st = streams[k % 3]
-            sl = slice(k * per, (k + 1) * per)
-            with torch.cuda.stream(st):
-                for (ih, mh), (idv, mdv) in zip(host[sl], dev_vols[sl]):
-                    idv.copy_(ih, non_blocking=True)
-                    mdv.copy_(mh, non_blocking=True)
-                rs = n4b200.N4Batch(dev_vols[sl], p, ctx=ctxs[k % 3], synchronous=False, encoder=encs[k % 3])
-                for r, o, l in zip(rs, out_h[sl], lat_h[sl]):
-                    o.copy_(r.im_normalized, non_blocking=True)
-                    l.copy_(r.lattice, non_blocking=True)
-
-    def time_e2e(host, dev_vols):
+    def time_e2e(host):
+        outs = list(zip(out_h, lat_h))
         for _ in range(min(args.warmup, 2)):
-            step_e2e(host, dev_vols)
+            n4b200.N4BatchHost(host, p, encoder=henc, outputs=outs, ctx=hctx, device=local_rank)
         barrier()
-        e0.record(stream)
-        for s2 in streams:
-            s2.wait_event(e0)
+        tot = 0.0
+        w0 = time.perf_counter()
         for _ in range(args.steps):
-            step_e2e(host, dev_vols)
-        for s2 in streams:
-            ev = torch.cuda.Event()
-            ev.record(s2)
-            stream.wait_event(ev)
-        e1.record(stream)
+            res_h, dms = n4b200.N4BatchHost(host, p, encoder=henc, outputs=outs, ctx=hctx, device=local_rank)
+            tot += dms
+        wall = (time.perf_counter() - w0) * 1000.0
+        assert all(r.report["status"] == "N4_OK" for r in res_h)
         barrier()
-        return max_over_ranks(e0.elapsed_time(e1))
+        return max_over_ranks(tot), wall
 
-    ms_e2e = time_e2e(vols_host, dev_in)
+    ms_e2e, wall_e2e = time_e2e(vols_host)
     # the same with byte masks (N4_FLAG_MASK_U8): 1 B instead of 4 B per mask voxel over PCIe
     host_u8 = [(ih, (mh != 0).to(torch.uint8).pin_memory()) for ih, mh in vols_host]
-    dev_u8 = [(idv, torch.empty(mh.shape, dtype=torch.uint8, device=dev)) for (idv, _), (_, mh) in zip(dev_in, host_u8)]
-    ms_e2e_u8 = time_e2e(host_u8, dev_u8)
+    ms_e2e_u8, wall_e2e_u8 = time_e2e(host_u8)
     h2d_u8 = sum(a.numel() * 4 + b.numel() for a, b in host_u8)
     h2d = sum(a.numel() * 4 + b.numel() * 4 for a, b in vols_host)
     d2h = sum(o.numel() * 4 for o in out_h) + sum(l.numel() * 4 for l in lat_h)
@@ -512,10 +523,13 @@ def run_ours(args, rank, world, local_rank):
                      f"peak {peak_kind}",
         },
         "e2e": {"value": world * B * args.steps / (ms_e2e / 1000.0), "unit": "volumes/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "n4_run_batched_host (float masks, warm start, sub-batches of 8 over 3 staging slots)",
+                "wall_ms_per_step": wall_e2e / args.steps},
         "e2e_byte_masks": {"value": world * B * args.steps / (ms_e2e_u8 / 1000.0), "unit": "volumes/s",
                            "h2d_bytes_per_step": h2d_u8, "d2h_bytes_per_step": d2h,
-                           "path": "same as e2e with uint8 masks (N4_FLAG_MASK_U8)"},
+                           "path": "same as e2e with uint8 masks (N4_FLAG_MASK_U8)",
+                           "wall_ms_per_step": wall_e2e_u8 / args.steps},
         "gpu_launches": warm.kernel_launches * args.steps,
         "sub_batches": warm.sub_batches,
         "clocks": clk,
@@ -525,8 +539,12 @@ def run_ours(args, rank, world, local_rank):
                           "ms_per_step": ms_gplain / args.steps, "path": "batch graph without warm start"},
         "warm_start": {"iterations_per_volume_warm": sum(iters_w) / B,
                        "iterations_per_volume_plain": sum(iters) / B, "kept": kept,
-                       "max_abs_log_bias_diff_vs_plain": dmax,
-                       "diff_basis": "full-resolution log bias over the mask, mean removed"},
+                       "max_abs_log_bias_diff_vs_plain_raw": max(draw),
+                       "median_abs_log_bias_diff_vs_plain_raw": float(np.median(draw)),
+                       "share_of_volumes_raw_within_0_01": float(np.mean(np.asarray(draw) <= 0.01)),
+                       "max_abs_log_bias_diff_vs_plain_mean_removed": max(dcent),
+                       "diff_basis": "per volume, max over the mask of |log bias (warm) - log bias (plain)| "
+                                     "at full resolution; raw, and after removing its mean over the mask"},
         "autotune": {"cluster_sizes_ms": tune["candidates"], "chosen_cluster_size": tune["chosen"]},
         "batched_without_graph": {"value": world * B * args.steps / (ms_nograph / 1000.0), "unit": "volumes/s",
                                   "ms_per_step": ms_nograph / args.steps},

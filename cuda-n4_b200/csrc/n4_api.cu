@@ -104,6 +104,7 @@ struct TuneVal {
   int grid;   // 1 = whole-GPU path
   int K;      // CTAs per cluster
   int nt;     // threads per CTA
+  int corr;   // correction tile shape (index into kCorrectShape)
 };
 
 constexpr int kStaticSmemReserve = 1024;
@@ -120,12 +121,21 @@ struct n4_context {
   DevBuf s1, s2, s3, s4, s5;   // component scratch
   DevBuf warm_x, warm_lat;     // learned warm start: network inputs, predicted lattices
   DevBuf h_im, h_mask, h_out, h_lat, h_bias, h_warm;   // host-run staging
+  // pipelined host batches: device staging slots and the upload, run and
+  // download streams with one event of each kind per slot
+  DevBuf hb;
+  cudaStream_t hst[3] = {};
+  cudaEvent_t hev[3 * 4] = {};
+  cudaEvent_t hclock[2] = {};
   Slot slots[kSlots];
   int next_slot = 0;
   int last_slot = -1;
   cudaStream_t last_stream = nullptr;
   cudaEvent_t last_done = nullptr;
   std::map<TuneKey, TuneVal> tune;
+  // standalone components: (fx, fy, fz, ncpt, field alignment) -> fit shape,
+  // (fx, fy, fz, ncpt) -> evaluation (correction) tile shape
+  std::map<std::vector<int>, int> fit_tune, eval_tune;
   // max co-resident clusters per (threads, cluster size, shared bytes)
   std::map<std::tuple<int, int, int>, int> cluster_cap;
   // sub-batch pipeline: N4 launches on two high-priority streams, prologues
@@ -137,6 +147,7 @@ struct n4_context {
   cudaEvent_t ev[5] = {};
   int prof_launches = 0;
   long long prof_fit = 0, prof_full = 0;
+  int prof_fit_shape = -1, prof_corr_shape = -1;   // shapes of the last profiled call
   bool prof_valid = false;
 };
 
@@ -294,9 +305,6 @@ Plan make_plan(const n4_params_t *p, int K, const std::vector<Dims> &vols, bool 
   pl.b_slotC = take((size_t)pl.NLAT * 4);
   pl.b_slice = take(std::max((size_t)(pl.NLAT + K - 1) / K * 4, (size_t)(pl.bins + K - 1) / K * 8));
   pl.big_bytes = (int)align_up(o, 128);
-  // a histogram copy (one per 8th warp) receives at most n/8 + NT/8 of a
-  // CTA's n voxels (NT <= 1024 threads); its 32-bit bins must not overflow
-  pl.hist_shift = hist_shift_for(((long long)rows_max * pl.Zmax + 7) / 8 + 160);
   return pl;
 }
 
@@ -349,7 +357,8 @@ n4_status_t capacity(n4_context *ctx, int nt, int K, int smem, int *n) {
   const auto key = std::make_tuple(nt, K, smem);
   auto it = ctx->cluster_cap.find(key);
   if (it != ctx->cluster_cap.end()) { *n = it->second; return N4_OK; }
-  TRY(nt == 1024 ? cluster_capacity<1024>(ctx, K, smem, n) : cluster_capacity<512>(ctx, K, smem, n));
+  TRY(nt == 1024 ? cluster_capacity<1024>(ctx, K, smem, n)
+                  : nt == 768 ? cluster_capacity<768>(ctx, K, smem, n) : cluster_capacity<512>(ctx, K, smem, n));
   ctx->cluster_cap[key] = *n;
   return N4_OK;
 }
@@ -470,6 +479,18 @@ n4_status_t ensure_grid_workspace(n4_context *ctx, const n4_params_t *p, const D
   return N4_OK;
 }
 
+// Cooperative launch of the whole-GPU N4 kernel with NT threads per CTA.
+template <int NT>
+n4_status_t launch_grid_kernel(GridArgs &a, int nblk, int smem, cudaStream_t st) {
+  CK(cudaFuncSetAttribute(k_n4_grid<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_n4_grid<NT>, NT, smem));
+  if (occ < 1) return fail(N4_ERR_TOO_LARGE, "grid kernel does not fit on an SM");
+  void *args[] = {&a};
+  CK(cudaLaunchCooperativeKernel((void *)k_n4_grid<NT>, dim3(nblk), dim3(NT), args, smem, st));
+  return N4_OK;
+}
+
 n4_status_t launch_grid_path(n4_context *ctx, const n4_params_t *p, const Params &pr, const RunVol &rv,
                              const VolJob &job0, int nt, cudaStream_t st) {
   std::vector<Dims> one{rv.d};
@@ -495,21 +516,9 @@ n4_status_t launch_grid_path(n4_context *ctx, const n4_params_t *p, const Params
   a.bar.nblocks = nblk;
   a.red_global = ctx->red.as<float>();
   const int smem = pl.sm_bytes;
-  void *args[] = {&a};
-  if (nt == 1024) {
-    CK(cudaFuncSetAttribute(k_n4_grid<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    int occ = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_n4_grid<1024>, 1024, smem));
-    if (occ < 1) return fail(N4_ERR_TOO_LARGE, "grid kernel does not fit on an SM");
-    CK(cudaLaunchCooperativeKernel((void *)k_n4_grid<1024>, dim3(nblk), dim3(1024), args, smem, st));
-  } else {
-    CK(cudaFuncSetAttribute(k_n4_grid<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    int occ = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_n4_grid<512>, 512, smem));
-    if (occ < 1) return fail(N4_ERR_TOO_LARGE, "grid kernel does not fit on an SM");
-    CK(cudaLaunchCooperativeKernel((void *)k_n4_grid<512>, dim3(nblk), dim3(512), args, smem, st));
-  }
-  return N4_OK;
+  if (nt == 1024) return launch_grid_kernel<1024>(a, nblk, smem, st);
+  if (nt == 768) return launch_grid_kernel<768>(a, nblk, smem, st);
+  return launch_grid_kernel<512>(a, nblk, smem, st);
 }
 
 template <int NT>
@@ -536,11 +545,15 @@ n4_status_t launch_cluster_kernel(n4_context *ctx, const ClusterArgs &a, int K, 
 struct Choice {
   bool grid;
   int K, nt;
+  int corr = -1;   // correction tile shape; -1: the recorded or default one
 };
 
+// Autotuner key: first-level lattice, levels, bins, shrink factor and the
+// fitting-grid size of every volume (with the shrink factor, the
+// full-resolution size the correction runs over).
 TuneKey tune_key(const n4_params_t *p, const std::vector<Dims> &vols) {
   TuneKey k{(int)p->NumberOfControlPoints_x, (int)p->NumberOfControlPoints_y, (int)p->NumberOfControlPoints_z,
-            (int)p->NumberOfFittingLevels, (int)p->NumberOfHistogramBins, (int)vols.size()};
+            (int)p->NumberOfFittingLevels, (int)p->NumberOfHistogramBins, (int)p->ShrinkFactor, (int)vols.size()};
   for (const Dims &d : vols) { k.push_back(d.X); k.push_back(d.Y); k.push_back(d.Z); }
   return k;
 }
@@ -568,6 +581,7 @@ n4_status_t choose_path(n4_context *ctx, const n4_params_t *p, const std::vector
     if (it != ctx->tune.end()) {
       c.grid = it->second.grid != 0;
       c.K = it->second.K;
+      c.corr = it->second.corr;
       if (!(p->flags & N4_FLAG_CTA_512)) c.nt = it->second.nt;
       return N4_OK;
     }
@@ -597,6 +611,7 @@ struct Prepared {
   n4_encoder_t *enc = nullptr;   // learned warm start run inside the batch
   int enc_batch = 0;             // predictions per encoder call
   long long fit_total = 0, tiles = 0;
+  int corr = kCorrectDefault;    // correction tile shape
   int nsub = 1;                  // sub-batches (volume ranges sub_lo[k] .. sub_lo[k + 1])
   std::vector<int> sub_lo;
 };
@@ -670,6 +685,7 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
     for (int i : rest) P.in_grid.push_back(i);
   }
   P.ch = ch;
+  P.corr = (ch.corr >= 0 && ch.corr < kCorrectShapes) ? ch.corr : kCorrectDefault;
   for (int i : P.in_grid) TRY(ensure_grid_workspace(ctx, p, dims[i]));
   P.path.assign(n, 0);
   P.csize.assign(n, 0);
@@ -756,7 +772,8 @@ void fill_descriptors(n4_context *ctx, const n4_params_t *p, Prepared &P, const 
     cv[i] = CorrectVol{r.im, r.out, r.bias, r.lat, tx, ty, tz, d.FX, d.FY, d.FZ, P.NCX, P.NCY, P.NCZ, tiles,
                        vec4_ok(d.FZ, r.im, r.out, r.bias)};
     tst[i] = tiles;
-    tiles += ((long long)d.FX * d.FY + kRowsPerTile - 1) / kRowsPerTile;
+    const long long rt = kCorrectShape[P.corr].rows;
+    tiles += ((long long)d.FX * d.FY + rt - 1) / rt;
     std::memset(&rep[i], 0, sizeof(n4_report_t));
     rep[i].status = -1;
   }
@@ -832,6 +849,7 @@ n4_status_t launch_engine(n4_context *ctx, const n4_params_t *p, const Prepared 
   a.use_tma = 1;
   const int ncl = std::min<int>(cap, njobs);
   if (P.ch.nt == 1024) TRY(launch_cluster_kernel<1024>(ctx, a, P.ch.K, ncl, smem, st));
+  else if (P.ch.nt == 768) TRY(launch_cluster_kernel<768>(ctx, a, P.ch.K, ncl, smem, st));
   else TRY(launch_cluster_kernel<512>(ctx, a, P.ch.K, ncl, smem, st));
   return N4_OK;
 }
@@ -855,6 +873,20 @@ n4_status_t ensure_pipe(n4_context *ctx) {
 // streams have the higher priority; measured, it makes no difference).
 // Every kernel reads and writes only its own volumes' buffers; st waits for
 // all four streams.
+// k_correct over `tiles` tiles from t0 with tile shape `shape`.
+n4_status_t launch_correct(int shape, long long tiles, int ncz, cudaStream_t st, const CorrectVol *vols,
+                           const long long *tile_starts, int nvol, long long t0, float low) {
+  if (tiles <= 0) return N4_OK;
+  const CorrectShape cs = kCorrectShape[shape];
+  const size_t smem = correct_smem_bytes(cs.rows, ncz);
+  if (cs.threads == 512)
+    k_correct<512><<<(unsigned)tiles, 512, smem, st>>>(vols, tile_starts, nvol, t0, low, cs.rows);
+  else
+    k_correct<256><<<(unsigned)tiles, 256, smem, st>>>(vols, tile_starts, nvol, t0, low, cs.rows);
+  CK(cudaGetLastError());
+  return N4_OK;
+}
+
 n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepared &P, const DescBuf &B,
                               cudaStream_t st) {
   TRY(ensure_pipe(ctx));
@@ -915,9 +947,8 @@ n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepa
     const int lo = P.sub_lo[k], hi = P.sub_lo[k + 1];
     const long long t0 = tst[lo], t1 = hi < n ? tst[hi] : P.tiles;
     CK(cudaStreamWaitEvent(corr, ev[6 + k], 0));
-    k_correct<<<(unsigned)(t1 - t0), 256, 0, corr>>>(B.dp<CorrectVol>(P.o_cor) + lo, B.dp<long long>(P.o_tst) + lo,
-                                                 hi - lo, t0, p->low_value);
-    CK(cudaGetLastError());
+    TRY(launch_correct(P.corr, t1 - t0, P.NCZ, corr, B.dp<CorrectVol>(P.o_cor) + lo, B.dp<long long>(P.o_tst) + lo,
+                       hi - lo, t0, p->low_value));
     ++launches;
   }
   for (int i = 0; i < 4; ++i) {
@@ -928,6 +959,8 @@ n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepa
   ctx->prof_fit = P.fit_total;
   ctx->prof_full = 0;
   for (const Dims &d : P.dims) ctx->prof_full += (long long)d.FX * d.FY * d.FZ;
+  ctx->prof_fit_shape = -1;
+  ctx->prof_corr_shape = P.corr;
   return N4_OK;
 }
 
@@ -980,15 +1013,16 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
   k_axis_tables<<<3 * n, 256, 0, st>>>(B.dp<TableJob>(P.o_tab));
   CK(cudaGetLastError());
   if (profile) TRY(prof_mark(ctx, 3, st));
-  k_correct<<<(unsigned)P.tiles, 256, 0, st>>>(B.dp<CorrectVol>(P.o_cor), B.dp<long long>(P.o_tst), n, 0,
-                                               p->low_value);
-  CK(cudaGetLastError());
+  TRY(launch_correct(P.corr, P.tiles, P.NCZ, st, B.dp<CorrectVol>(P.o_cor), B.dp<long long>(P.o_tst), n, 0,
+                     p->low_value));
   if (profile) TRY(prof_mark(ctx, 4, st));
   launches += 2;
   ctx->prof_launches = launches;
   ctx->prof_fit = P.fit_total;
   ctx->prof_full = 0;
   for (const Dims &d : P.dims) ctx->prof_full += (long long)d.FX * d.FY * d.FZ;
+  ctx->prof_fit_shape = -1;
+  ctx->prof_corr_shape = P.corr;
   return N4_OK;
 }
 
@@ -1017,9 +1051,16 @@ n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector
   return end_run(ctx, st, u);
 }
 
+// The reports of the run that used descriptor slot `slot` (waits for it).
+n4_status_t collect_slot(n4_context *ctx, int slot, n4_report_t *out, int n);
+
 n4_status_t collect(n4_context *ctx, n4_report_t *out, int n) {
   if (ctx->last_slot < 0) return fail(N4_ERR_INVALID_ARG, "no run to synchronise with");
-  Slot &s = ctx->slots[ctx->last_slot];
+  return collect_slot(ctx, ctx->last_slot, out, n);
+}
+
+n4_status_t collect_slot(n4_context *ctx, int slot, n4_report_t *out, int n) {
+  Slot &s = ctx->slots[slot];
   CK(cudaEventSynchronize(s.ev));
   s.pending = false;
   const n4_report_t *rep = (const n4_report_t *)(s.h + s.off_rep);
@@ -1115,6 +1156,14 @@ n4_status_t n4_create(n4_context_t **out, int device) {
   c->device = device;
   CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
   CK(cudaDeviceGetAttribute(&c->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  // the largest correction tile: 512 rows of kMaxNcz z control points
+  const int corr_smem = (int)correct_smem_bytes(512, kMaxNcz);
+  if (cudaFuncSetAttribute(k_correct<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, corr_smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_correct<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, corr_smem) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return fail(N4_ERR_CUDA, "cannot raise the correction kernel's shared-memory limit");
+  }
   *out = c;
   return N4_OK;
 }
@@ -1125,8 +1174,14 @@ n4_status_t n4_destroy(n4_context_t *c) {
   cudaDeviceSynchronize();
   for (DevBuf *b : {&c->imlog, &c->tables, &c->big, &c->red, &c->bar, &c->s1, &c->s2, &c->s3, &c->s4,
                     &c->s5, &c->h_im, &c->h_mask, &c->h_out, &c->h_lat, &c->h_bias, &c->h_warm, &c->warm_x,
-                    &c->warm_lat})
+                    &c->warm_lat, &c->hb})
     b->release();
+  for (cudaEvent_t e : c->hev)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : c->hclock)
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t s : c->hst)
+    if (s) cudaStreamDestroy(s);
   for (Slot &s : c->slots) {
     if (s.h) cudaFreeHost(s.h);
     s.d.release();
@@ -1309,7 +1364,7 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
     std::vector<Dims> sub;
     for (int i : fit) sub.push_back(dims[i]);
     Plan pl = make_plan(p, K, sub, false);
-    for (int nt : {1024, 512}) {
+    for (int nt : {1024, 768, 512}) {
       int cap = 0;
       TRY(capacity(ctx, nt, K, pl.sm_bytes + pl.big_bytes, &cap));
       if (cap > 0) cand.push_back(Choice{false, K, nt});
@@ -1317,6 +1372,7 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
   }
   if (n == 1) {
     cand.push_back(Choice{true, 0, 1024});
+    cand.push_back(Choice{true, 0, 768});
     cand.push_back(Choice{true, 0, 512});
   }
   if ((int)cand.size() > N4_TUNE_MAX) cand.resize(N4_TUNE_MAX);
@@ -1365,7 +1421,32 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
   if (best < 0) return fail(N4_ERR_TOO_LARGE, "no execution path fits these volumes");
   rep.chosen = best;
   const int K = rep.cluster_size[best];
-  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, rep.threads[best]};
+  // correction tile shapes on the chosen path: the correction stage's device
+  // time (profiling events around it) of one run per shape, the fastest of
+  // two runs each
+  Choice ch{K == 0, K, rep.threads[best]};
+  ctx->profiling = 1;
+  for (int k = 0; k < kCorrectShapes && status == N4_OK; ++k) {
+    ch.corr = k;
+    float ms = 0.0f;
+    for (int r = 0; r < 2 && status == N4_OK; ++r) {
+      status = run_volumes(ctx, p, v, st, &ch);
+      if (status == N4_OK) status = collect(ctx, reps.data(), n);
+      n4_timings_t t{};
+      if (status == N4_OK) status = n4_last_timings(ctx, &t);
+      if (status == N4_OK && (r == 0 || t.stage_ms[3] < ms)) ms = t.stage_ms[3];
+    }
+    if (status != N4_OK) break;
+    rep.corr_rows[k] = kCorrectShape[k].rows;
+    rep.corr_threads[k] = kCorrectShape[k].threads;
+    rep.corr_ms[k] = ms;
+    rep.corr_candidates = k + 1;
+    if (k == 0 || ms < rep.corr_ms[rep.corr_chosen]) rep.corr_chosen = k;
+  }
+  ctx->profiling = saved_prof;
+  ctx->prof_valid = false;
+  if (status != N4_OK) return status;
+  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, rep.threads[best], rep.corr_chosen};
   if (report) *report = rep;
   return N4_OK;
 }
@@ -1385,6 +1466,11 @@ n4_status_t n4_last_timings(n4_context_t *ctx, n4_timings_t *t) {
   t->launches = ctx->prof_launches;
   t->fit_voxels = ctx->prof_fit;
   t->full_voxels = ctx->prof_full;
+  const int fs = ctx->prof_fit_shape, cs = ctx->prof_corr_shape;
+  t->fit_rows = fs >= 0 ? kFitShape[fs].rows : -1;
+  t->fit_step = fs >= 0 ? kFitShape[fs].step : -1;
+  t->correct_rows = cs >= 0 ? kCorrectShape[cs].rows : -1;
+  t->correct_threads = cs >= 0 ? kCorrectShape[cs].threads : -1;
   return N4_OK;
 }
 
@@ -1428,6 +1514,119 @@ n4_status_t n4_run_host(n4_context_t *ctx, const n4_params_t *p, const float *h_
   if (h_bias_field) CK(cudaMemcpyAsync(h_bias_field, ctx->h_bias.p, nv * 4, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return s;
+}
+
+n4_status_t n4_run_batched_host(n4_context_t *ctx, const n4_params_t *p, int n, const n4_volume_t *vols, int per,
+                                n4_encoder_t *enc, n4_report_t *reports, float *device_ms) {
+  if (!ctx || !vols || n < 1 || per < 0) return fail(N4_ERR_INVALID_ARG, "bad batch");
+  TRY(check_params(p));
+  CK(cudaSetDevice(ctx->device));
+  size_t nlat = 0;
+  TRY(n4_lattice_dims(p, nullptr, &nlat));
+  const size_t nwarm = (size_t)p->NumberOfControlPoints_x * p->NumberOfControlPoints_y * p->NumberOfControlPoints_z;
+  const size_t mask_b = (p->flags & N4_FLAG_MASK_U8) ? 1 : 4;
+  size_t vmax = 0;
+  bool any_mask = false, any_bias = false, any_warm = false;
+  for (int i = 0; i < n; ++i) {
+    const n4_volume_t &q = vols[i];
+    if (!q.im || !q.im_normalized || !q.lattice) return fail(N4_ERR_INVALID_ARG, "NULL pointer in batch");
+    Dims d;
+    TRY(make_dims(p, q.fx, q.fy, q.fz, d));
+    vmax = std::max(vmax, (size_t)q.fx * q.fy * q.fz);
+    any_mask |= q.mask != nullptr;
+    any_bias |= q.bias_field != nullptr;
+    any_warm |= q.warm_lattice != nullptr;
+  }
+  if (enc && any_warm) return fail(N4_ERR_INVALID_ARG, "warm lattices are predicted by the encoder: pass none");
+  if (per == 0) per = std::min(n, 8);
+  per = std::min(per, n);
+  // one staging slot: per volumes of input, mask, output, bias, lattice, warm lattice
+  auto al = [](size_t b) { return align_up(b, 256); };
+  const size_t vin = al(vmax * 4), vmask = any_mask ? al(vmax * mask_b) : 0, vout = al(vmax * 4),
+               vbias = any_bias ? al(vmax * 4) : 0, vlat = al(nlat * 4), vwarm = any_warm ? al(nwarm * 4) : 0;
+  const size_t per_vol = vin + vmask + vout + vbias + vlat + vwarm;
+  constexpr int D = 3;   // staging slots: upload k + 2 while k + 1 runs and k downloads
+  TRY(ctx->hb.ensure((size_t)D * per * per_vol, "host-batch staging"));
+  for (cudaStream_t &s2 : ctx->hst)
+    if (!s2) CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+  for (cudaEvent_t &e : ctx->hev)
+    if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (cudaEvent_t &e : ctx->hclock)
+    if (!e) CK(cudaEventCreate(&e));
+  cudaStream_t up = ctx->hst[0], run = ctx->hst[1], down = ctx->hst[2];
+  auto ev_up = [&](int d) { return ctx->hev[d]; };
+  auto ev_run = [&](int d) { return ctx->hev[4 + d]; };
+  auto ev_down = [&](int d) { return ctx->hev[8 + d]; };
+  // the previous work of this context (any stream) comes first
+  if (ctx->last_done && ctx->last_slot >= 0) CK(cudaStreamWaitEvent(up, ctx->last_done, 0));
+  CK(cudaEventRecord(ctx->hclock[0], up));
+  const int nsb = (n + per - 1) / per;
+  std::vector<int> run_slot(nsb, -1);
+  n4_status_t worst = N4_OK;
+  auto harvest = [&](int k) -> n4_status_t {
+    if (k < 0 || run_slot[k] < 0) return N4_OK;
+    const int lo = k * per, cnt = std::min(per, n - lo);
+    n4_status_t st = collect_slot(ctx, run_slot[k], reports ? reports + lo : nullptr, cnt);
+    run_slot[k] = -1;
+    if (st == N4_ERR_CUDA || st == N4_ERR_TIMEOUT) return st;
+    if (st != N4_OK && worst == N4_OK) worst = st;
+    return N4_OK;
+  };
+  for (int k = 0; k < nsb; ++k) {
+    const int d = k % D, lo = k * per, cnt = std::min(per, n - lo);
+    char *base = (char *)ctx->hb.p + (size_t)d * per * per_vol;
+    auto vol_at = [&](int j) { return base + (size_t)j * per_vol; };
+    // upload: after the download that last used this staging slot
+    if (k >= D) CK(cudaStreamWaitEvent(up, ev_down(d), 0));
+    std::vector<RunVol> rvs(cnt);
+    for (int j = 0; j < cnt; ++j) {
+      const n4_volume_t &q = vols[lo + j];
+      const size_t nv = (size_t)q.fx * q.fy * q.fz;
+      char *v = vol_at(j);
+      float *im = (float *)v, *mk = (float *)(v + vin), *out = (float *)(v + vin + vmask),
+            *bias = (float *)(v + vin + vmask + vout), *lat = (float *)(v + vin + vmask + vout + vbias),
+            *warm = (float *)(v + vin + vmask + vout + vbias + vlat);
+      CK(cudaMemcpyAsync(im, q.im, nv * 4, cudaMemcpyHostToDevice, up));
+      if (q.mask) CK(cudaMemcpyAsync(mk, q.mask, nv * mask_b, cudaMemcpyHostToDevice, up));
+      if (q.warm_lattice) CK(cudaMemcpyAsync(warm, q.warm_lattice, nwarm * 4, cudaMemcpyHostToDevice, up));
+      RunVol &r = rvs[j];
+      TRY(make_dims(p, q.fx, q.fy, q.fz, r.d));
+      r.im = im;
+      r.mask = q.mask ? mk : nullptr;
+      r.out = out;
+      r.lat = lat;
+      r.bias = q.bias_field ? bias : nullptr;
+      r.warm = q.warm_lattice ? warm : nullptr;
+    }
+    CK(cudaEventRecord(ev_up(d), up));
+    // the run: its descriptor slot is the one run k - 4 used; take that run's
+    // reports before the slot is reused
+    TRY(harvest(k - kSlots));
+    CK(cudaStreamWaitEvent(run, ev_up(d), 0));
+    TRY(run_volumes(ctx, p, rvs, run, nullptr, enc));
+    run_slot[k] = ctx->last_slot;
+    CK(cudaEventRecord(ev_run(d), run));
+    // download
+    CK(cudaStreamWaitEvent(down, ev_run(d), 0));
+    for (int j = 0; j < cnt; ++j) {
+      const n4_volume_t &q = vols[lo + j];
+      const size_t nv = (size_t)q.fx * q.fy * q.fz;
+      const RunVol &r = rvs[j];
+      CK(cudaMemcpyAsync(q.im_normalized, r.out, nv * 4, cudaMemcpyDeviceToHost, down));
+      CK(cudaMemcpyAsync(q.lattice, r.lat, nlat * 4, cudaMemcpyDeviceToHost, down));
+      if (q.bias_field) CK(cudaMemcpyAsync(q.bias_field, r.bias, nv * 4, cudaMemcpyDeviceToHost, down));
+    }
+    CK(cudaEventRecord(ev_down(d), down));
+  }
+  CK(cudaEventRecord(ctx->hclock[1], down));
+  // later work of this context waits for the downloads
+  CK(cudaEventRecord(ctx->last_done, down));
+  ctx->last_stream = down;
+  for (int k = std::max(0, nsb - kSlots); k < nsb; ++k) TRY(harvest(k));
+  CK(cudaEventSynchronize(ctx->hclock[1]));
+  if (device_ms) CK(cudaEventElapsedTime(device_ms, ctx->hclock[0], ctx->hclock[1]));
+  if (worst != N4_OK) return fail(worst, std::string("volume failed: ") + n4_status_string(worst));
+  return N4_OK;
 }
 
 }  // extern "C"
@@ -1574,24 +1773,65 @@ n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *g) {
 }
 
 // ---------------------------------------------------------------- components
-// z contraction of a standalone fit: rows read in 8-voxel (32-byte) register
-// steps when Z % 8 == 0 and field and mask start on 32-byte boundaries, in
-// 4-voxel (16-byte) steps when Z % 4 == 0 and they start on 16-byte
-// boundaries, both while the z table fits the default 48 KB of shared memory
-// (Z <= 1024); the scalar kernel otherwise.  Same arithmetic, bitwise the
-// same sums.
-static void launch_fit_rows(const float *field, const float *mask, long long rows, int Z, const Axis &az,
-                            float *t1n, float *t1d, cudaStream_t st) {
+// Whether fit shape `k` can run on this field: 8-voxel (32-byte) register
+// steps need Z % 8 == 0 and field and mask on 32-byte boundaries, 4-voxel
+// (16-byte) steps Z % 4 == 0 and 16-byte boundaries, both a z table within
+// the default 48 KB of shared memory (Z <= 1024); the scalar kernel runs on
+// anything.  Every shape computes the same sums in the same order (bitwise).
+static bool fit_shape_ok(int k, const float *field, const float *mask, int Z) {
   const uintptr_t al = (uintptr_t)field | (uintptr_t)mask;
-  const unsigned grid = (unsigned)((rows + kFitRowsD - 1) / kFitRowsD);
-  if (Z % 8 == 0 && Z <= kFitZMaxD && (al & 31u) == 0)
-    k_fit_rows_v5<8, 3><<<grid, kFitRowsD, kFitTableBytes(Z), st>>>(field, mask, rows, Z, az, t1n, t1d);
-  else if (Z % 4 == 0 && Z <= kFitZMaxD && (al & 15u) == 0)
-    k_fit_rows_v5<4, 6><<<grid, kFitRowsD, kFitTableBytes(Z), st>>>(field, mask, rows, Z, az, t1n, t1d);
-  else
-    k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(field, mask, rows, Z, az, t1n,
-                                                                                   t1d);
+  const FitShape f = kFitShape[k];
+  if (f.step == 8) return Z % 8 == 0 && Z <= kFitZMaxD && (al & 31u) == 0;
+  if (f.step == 4) return Z % 4 == 0 && Z <= kFitZMaxD && (al & 15u) == 0;
+  return true;
 }
+
+static int fit_default_shape(const float *field, const float *mask, int Z) {
+  if (fit_shape_ok(kFitDefault8, field, mask, Z)) return kFitDefault8;
+  if (fit_shape_ok(kFitDefault4, field, mask, Z)) return kFitDefault4;
+  return kFitScalar;
+}
+
+// Component autotuner keys: field and lattice sizes (and, for the fit, the
+// alignment class of field and mask, which decides the shapes that can run).
+static std::vector<int> fit_key(unsigned fx, unsigned fy, unsigned fz, unsigned nx, unsigned ny, unsigned nz,
+                                const float *field, const float *mask) {
+  const uintptr_t al = (uintptr_t)field | (uintptr_t)mask;
+  const int cls = (al & 31u) == 0 ? 32 : ((al & 15u) == 0 ? 16 : 4);
+  return {(int)fx, (int)fy, (int)fz, (int)nx, (int)ny, (int)nz, cls};
+}
+static std::vector<int> eval_key(unsigned fx, unsigned fy, unsigned fz, unsigned nx, unsigned ny, unsigned nz) {
+  return {(int)fx, (int)fy, (int)fz, (int)nx, (int)ny, (int)nz};
+}
+
+extern "C++" {
+template <int S, int D, int R>
+static void fit_rows_as(const float *field, const float *mask, long long rows, int Z, const Axis &az, float *t1n,
+                        float *t1d, cudaStream_t st) {
+  k_fit_rows_v5<S, D, R><<<(unsigned)((rows + R - 1) / R), R, kFitTableBytes(Z), st>>>(field, mask, rows, Z, az, t1n,
+                                                                                      t1d);
+}
+}  // extern "C++"
+
+// z contraction of a standalone fit with shape `k` (fit_shape_ok must hold).
+static void launch_fit_rows(int k, const float *field, const float *mask, long long rows, int Z, const Axis &az,
+                            float *t1n, float *t1d, cudaStream_t st) {
+  switch (k) {
+    case 0: fit_rows_as<8, 3, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 1: fit_rows_as<8, 2, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 2: fit_rows_as<8, 4, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 3: fit_rows_as<8, 3, 32>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 4: fit_rows_as<8, 3, 128>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 5: fit_rows_as<8, 2, 128>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 6: fit_rows_as<4, 6, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 7: fit_rows_as<4, 4, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 8: fit_rows_as<4, 6, 128>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    default:
+      k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(field, mask, rows, Z, az, t1n,
+                                                                                     t1d);
+  }
+}
+static_assert(kFitShapes == 10, "launch_fit_rows covers every fit shape");
 
 // Sizes a standalone fit accepts: every extent below 2^31 (the kernels take
 // them as int), at most 2^36 field voxels and 4096 control points per axis,
@@ -1644,8 +1884,11 @@ n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const floa
   const int gb = ctx->nsm * 8;
   const long long rows = (long long)fx * fy;
   const bool prof = ctx->profiling != 0;
+  int shape = fit_default_shape(d_field, d_mask, (int)fz);
+  auto it = ctx->fit_tune.find(fit_key(fx, fy, fz, ncpt_x, ncpt_y, ncpt_z, d_field, d_mask));
+  if (it != ctx->fit_tune.end() && fit_shape_ok(it->second, d_field, d_mask, (int)fz)) shape = it->second;
   if (prof) TRY(prof_mark(ctx, 0, st));
-  launch_fit_rows(d_field, d_mask, rows, fz, az, t1n, t1d, st);
+  launch_fit_rows(shape, d_field, d_mask, rows, fz, az, t1n, t1d, st);
   if (prof) TRY(prof_mark(ctx, 1, st));
   k_fit_planes<<<(int)std::min<size_t>((t2 + 255) / 256, gb), 256, 0, st>>>(t1n, t1d, fx, fy, ay, ncpt_z, t2n, t2d);
   if (prof) TRY(prof_mark(ctx, 2, st));
@@ -1656,6 +1899,8 @@ n4_status_t n4_fit_bspline3d(n4_context_t *ctx, const float *d_field, const floa
   ctx->prof_launches = 4;
   ctx->prof_fit = (long long)fx * fy * fz;
   ctx->prof_full = 0;
+  ctx->prof_fit_shape = shape;
+  ctx->prof_corr_shape = -1;
   ctx->prof_valid = prof;
   return N4_OK;
 }
@@ -1673,7 +1918,11 @@ n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice, uns
   CorrectVol cv{nullptr, d_fitted, nullptr, d_lattice, (char *)ax.s, (char *)ay.s, (char *)az.s,
                 (int)fx, (int)fy, (int)fz, (int)ncpt_x, (int)ncpt_y, (int)ncpt_z, 0,
                 vec4_ok((int)fz, nullptr, d_fitted, nullptr)};
-  const long long tiles = ((long long)fx * fy + kRowsPerTile - 1) / kRowsPerTile;
+  int shape = kCorrectDefault;
+  auto it = ctx->eval_tune.find(eval_key(fx, fy, fz, ncpt_x, ncpt_y, ncpt_z));
+  if (it != ctx->eval_tune.end()) shape = it->second;
+  const long long rt = kCorrectShape[shape].rows;
+  const long long tiles = ((long long)fx * fy + rt - 1) / rt;
   Upload u;
   TRY(acquire_slot(ctx, sizeof(cv) + 16, u));
   std::memcpy(u.h(), &cv, sizeof(cv));
@@ -1682,15 +1931,117 @@ n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice, uns
   const size_t so = align_up(sizeof(cv), 16);
   const bool prof = ctx->profiling != 0;
   if (prof) TRY(prof_mark(ctx, 1, st));
-  k_correct<<<(unsigned)tiles, 256, 0, st>>>(u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0, 0.0f);
-  CK(cudaGetLastError());
+  TRY(launch_correct(shape, tiles, (int)ncpt_z, st, u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0, 0.0f));
   if (prof) { TRY(prof_mark(ctx, 2, st)); TRY(prof_mark(ctx, 3, st)); TRY(prof_mark(ctx, 4, st)); }
   ctx->prof_launches = 2;
   ctx->prof_fit = 0;
   ctx->prof_full = (long long)fx * fy * fz;
+  ctx->prof_fit_shape = -1;
+  ctx->prof_corr_shape = shape;
   ctx->prof_valid = prof;
   u.slot->nrep = 0;
   return end_run(ctx, st, u);
+}
+
+n4_status_t n4_autotune_components(n4_context_t *ctx, const float *d_field, const float *d_mask, unsigned int ncpt_x,
+                                   unsigned int ncpt_y, unsigned int ncpt_z, unsigned int fx, unsigned int fy,
+                                   unsigned int fz, float *d_lattice, float *d_out, void *stream,
+                                   n4_component_tune_t *report) {
+  if (!ctx || !d_field || !d_lattice || !d_out) return fail(N4_ERR_INVALID_ARG, "NULL pointer");
+  TRY(check_fit_sizes(ncpt_x, ncpt_y, ncpt_z, fx, fy, fz));
+  if (ncpt_z > (unsigned)kMaxNcz) return fail(N4_ERR_TOO_LARGE, "at most 64 control points along z");
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  Axis ax, ay, az;
+  TRY(component_tables(ctx, fx, fy, fz, ncpt_x, ncpt_y, ncpt_z, st, ax, ay, az));
+  const size_t t1 = (size_t)fx * fy * ncpt_z;
+  TRY(ctx->s1.ensure(t1 * 8, "fit rows"));
+  float *t1n = ctx->s1.as<float>(), *t1d = t1n + t1;
+  // a 256 MiB buffer read before every timed launch evicts its inputs from L2
+  const size_t evict_bytes = 256u << 20;
+  TRY(ctx->s4.ensure(evict_bytes + 256, "L2 eviction buffer"));
+  CK(cudaMemsetAsync(ctx->s4.p, 0, evict_bytes + 256, st));
+  const float4 *ev_buf = (const float4 *)ctx->s4.p;
+  float *sink = (float *)((char *)ctx->s4.p + evict_bytes);
+  const long long rows = (long long)fx * fy;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    return fail(N4_ERR_CUDA, "cudaEventCreate failed");
+  }
+  // time `launch` three times after an eviction each; the fastest in ms
+  auto timed = [&](auto &&launch, float *ms) -> n4_status_t {
+    launch();   // warm-up (and the first launch of the kernel)
+    float best = 0.0f;
+    for (int r = 0; r < 3; ++r) {
+      k_read_evict<<<ctx->nsm * 4, 512, 0, st>>>(ev_buf, (long long)(evict_bytes / 16), sink);
+      CK(cudaEventRecord(e0, st));
+      launch();
+      CK(cudaEventRecord(e1, st));
+      CK(cudaGetLastError());
+      CK(cudaEventSynchronize(e1));
+      float t = 0.0f;
+      CK(cudaEventElapsedTime(&t, e0, e1));
+      if (r == 0 || t < best) best = t;
+    }
+    *ms = best;
+    return N4_OK;
+  };
+  n4_component_tune_t rep{};
+  n4_status_t status = N4_OK;
+  for (int k = 0; k < kFitShapes && status == N4_OK && rep.fit_candidates < N4_TUNE_MAX; ++k) {
+    if (!fit_shape_ok(k, d_field, d_mask, (int)fz)) continue;
+    float ms = 0.0f;
+    status = timed([&] { launch_fit_rows(k, d_field, d_mask, rows, (int)fz, az, t1n, t1d, st); }, &ms);
+    if (status != N4_OK) break;
+    const int c = rep.fit_candidates++;
+    rep.fit_step[c] = kFitShape[k].step;
+    rep.fit_depth[c] = kFitShape[k].depth;
+    rep.fit_rows[c] = kFitShape[k].rows;
+    rep.fit_ms[c] = ms;
+    if (c == 0 || ms < rep.fit_ms[rep.fit_chosen]) { rep.fit_chosen = c; rep.fit_shape = k; }
+  }
+  // the evaluation candidates write d_out from the lattice the fit produces
+  if (status == N4_OK)
+    status = n4_fit_bspline3d(ctx, d_field, d_mask, ncpt_x, ncpt_y, ncpt_z, fx, fy, fz, 1e-3f, 0, d_lattice, stream);
+  Upload u;
+  if (status == N4_OK) status = acquire_slot(ctx, sizeof(CorrectVol) + 16, u);
+  if (status == N4_OK) {
+    CorrectVol cv{nullptr, d_out, nullptr, d_lattice, (char *)ax.s, (char *)ay.s, (char *)az.s,
+                  (int)fx, (int)fy, (int)fz, (int)ncpt_x, (int)ncpt_y, (int)ncpt_z, 0,
+                  vec4_ok((int)fz, nullptr, d_out, nullptr)};
+    std::memcpy(u.h(), &cv, sizeof(cv));
+    status = begin_run(ctx, st);
+    if (status == N4_OK && cudaMemcpyAsync(u.slot->d.p, u.slot->h, sizeof(cv) + 16, cudaMemcpyHostToDevice, st) !=
+                               cudaSuccess)
+      status = fail(N4_ERR_CUDA, "descriptor upload failed");
+    const size_t so = align_up(sizeof(cv), 16);
+    for (int k = 0; k < kCorrectShapes && status == N4_OK; ++k) {
+      const long long rt = kCorrectShape[k].rows;
+      const long long tiles = ((long long)fx * fy + rt - 1) / rt;
+      float ms = 0.0f;
+      n4_status_t ls = N4_OK;
+      status = timed([&] { ls = launch_correct(k, tiles, (int)ncpt_z, st, u.dp<CorrectVol>(0),
+                                               u.dp<long long>(so), 1, 0, 0.0f); }, &ms);
+      if (status == N4_OK) status = ls;
+      if (status != N4_OK) break;
+      const int c = rep.eval_candidates++;
+      rep.eval_rows[c] = kCorrectShape[k].rows;
+      rep.eval_threads[c] = kCorrectShape[k].threads;
+      rep.eval_ms[c] = ms;
+      if (c == 0 || ms < rep.eval_ms[rep.eval_chosen]) { rep.eval_chosen = c; rep.eval_shape = k; }
+    }
+    u.slot->nrep = 0;
+    if (status == N4_OK) status = end_run(ctx, st, u);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (status != N4_OK) return status;
+  ctx->fit_tune[fit_key(fx, fy, fz, ncpt_x, ncpt_y, ncpt_z, d_field, d_mask)] = rep.fit_shape;
+  ctx->eval_tune[eval_key(fx, fy, fz, ncpt_x, ncpt_y, ncpt_z)] = rep.eval_shape;
+  if (report) *report = rep;
+  return N4_OK;
 }
 
 n4_status_t n4_upsample_lattice3d(n4_context_t *ctx, const float *d_lattice, unsigned int ncpt_x, unsigned int ncpt_y,
@@ -1861,7 +2212,7 @@ n4_status_t n4_fit_bspline3d_noalloc(const float *d_field, const float *d_mask, 
   float *t1n = (float *)(base + bx + by + bz), *t1d = t1n + t1;
   float *t2n = (float *)(base + bx + by + bz + align_up(t1 * 8, 256)), *t2d = t2n + t2;
   const long long rows = (long long)fx * fy;
-  launch_fit_rows(d_field, d_mask, rows, fz, az, t1n, t1d, st);
+  launch_fit_rows(fit_default_shape(d_field, d_mask, (int)fz), d_field, d_mask, rows, fz, az, t1n, t1d, st);
   k_fit_planes<<<(int)std::min<size_t>((t2 + 255) / 256, 148 * 8), 256, 0, st>>>(t1n, t1d, fx, fy, ay, ncpt_z, t2n,
                                                                                    t2d);
   const int nlat = ncpt_x * ncpt_y * ncpt_z;

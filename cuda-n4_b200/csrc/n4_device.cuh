@@ -126,6 +126,18 @@ struct FastDiv {
   __device__ __forceinline__ unsigned div(unsigned i) const { return d == 1 ? i : __umulhi(i, m); }
 };
 
+// GPU global timer (ns) and the SM this thread runs on.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ int sm_id() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+  return (int)r;
+}
+
 // ---------------------------------------------------------------- reductions
 __device__ __forceinline__ float warp_min(float v) {
   for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(kFull, v, o));
@@ -143,6 +155,30 @@ __device__ __forceinline__ float warp_sumf(float v) {
   for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
   return v;
 }
+
+// Kahan-compensated FP32 sum (Kahan, CACM 8(1), 1965): `s` is the running
+// sum and `c` the part of the last addition that `s` could not hold, fed
+// back into the next term.  The error of a compensated sum of n terms is
+// bounded by ~2u sum|x_i| independently of n (u = 2^-24), instead of the
+// ~n u sum|x_i| of a plain recursive sum.  The intrinsics keep the compiler
+// from contracting or reassociating the steps.
+struct KahanSum {
+  float s = 0.0f, c = 0.0f;
+  __device__ __forceinline__ void add(float x) {
+    const float y = __fsub_rn(x, c);
+    const float t = __fadd_rn(s, y);
+    c = __fsub_rn(__fsub_rn(t, s), y);
+    s = t;
+  }
+  // adds w * x (the product rounded once, inside the first step)
+  __device__ __forceinline__ void add_prod(float w, float x) {
+    const float y = __fmaf_rn(w, x, -c);
+    const float t = __fadd_rn(s, y);
+    c = __fsub_rn(__fsub_rn(t, s), y);
+    s = t;
+  }
+  __device__ __forceinline__ float value() const { return __fsub_rn(s, c); }
+};
 
 // CTA-wide reduction of four values (min, max, sum, sum) into out[0..3] of
 // thread 0; `scratch` holds 4 * 32 doubles.  Deterministic order.

@@ -19,12 +19,24 @@
 //   update  D = num / (den + eps), L += D, G = rows(L), Gd = rows(D)
 #pragma once
 #include <cooperative_groups.h>
+#include <type_traits>
 
 #include "n4_device.cuh"
 
 namespace cg = cooperative_groups;
 
 namespace n4 {
+
+// Fixed-point scale 2^shift of one volume's histogram: the largest shift
+// (<= 24) for which no 32-bit bin of a histogram copy can overflow.  A copy
+// (one per 8th warp) receives at most an 8th of a CTA's voxels plus 160.  It
+// depends on the volume and the group size alone (not on the other volumes of
+// a batch), so a volume gets bitwise the same result in any batch.
+__host__ __device__ inline int volume_hist_shift(int X, int Y, int Z, int K, bool grid) {
+  const long long rows = (long long)X * Y;
+  const long long rpc = grid ? (rows + K - 1) / K : ((long long)X + K - 1) / K * Y;
+  return hist_shift_for((rpc * Z + 7) / 8 + 160);
+}
 
 // ------------------------------------------------------------------ layout
 // Byte offsets of one CTA's workspace.  "sm" offsets are always in shared
@@ -34,7 +46,7 @@ struct Plan {
   // limits
   int levels, nc0x, nc0y, nc0z, NCX, NCY, NCZ, NLAT;
   int Xmax, Ymax, Zmax, slab_floats, rows_max, nvxl;
-  int bins, npad, hoff, hist_shift;
+  int bins, npad, hoff;
   // shared
   int o_ax, o_ay, o_az, o_L, o_D, o_den, o_tmp, o_aux, o_hist, o_H64, o_H, o_E;
   int o_fa, o_fb, o_tw, o_ff, o_red, o_misc;
@@ -128,6 +140,7 @@ struct Engine {
   // rows of this CTA: grid path, contiguous rows r0 + rl; cluster path,
   // whole x-planes vx = rank + m * K (m = rl / Y), interleaved over the group
   int r0, nplane;
+  int hshift;   // fixed-point scale of this volume's histogram
   FastDiv divZ;
   const float *imlog;
   // level
@@ -277,15 +290,24 @@ struct Engine {
   // peer has read it).  Grid: each CTA reduces one slice over all peers, then
   // every CTA gathers the slices; slices live in a buffer of their own, so a
   // CTA may modify `out` while slower peers are still gathering.
+  // Sum over the group's K partials of entry c, in rank order: exact for the
+  // integer histogram, Kahan-compensated for the fit's float partials.
+  struct Acc64 {
+    unsigned long long s = 0;
+    __device__ __forceinline__ void add(unsigned long long x) { s += x; }
+    __device__ __forceinline__ unsigned long long value() const { return s; }
+  };
+  template <class T> using AccOf = typename std::conditional<std::is_same<T, float>::value, KahanSum, Acc64>::type;
+
   template <class T>
   __device__ bool allreduce(const T *mine, T *out, int n) {
     if (!g.sync()) return false;
     if (!Group::kGrid) {
       for (int c = threadIdx.x; c < n; c += blockDim.x) {
-        T acc = 0;
+        AccOf<T> acc;
 #pragma unroll 4
-        for (int k = 0; k < K; ++k) acc += *(g.peer(mine, k) + c);
-        out[c] = acc;
+        for (int k = 0; k < K; ++k) acc.add(*(g.peer(mine, k) + c));
+        out[c] = acc.value();
       }
       __syncthreads();
       return true;
@@ -294,10 +316,10 @@ struct Engine {
     const int c0 = rank * per, c1 = min(n, c0 + per);
     T *slice = Group::kGrid ? (T *)red_global : (T *)(big + pl.b_slice);
     for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-      T acc = 0;
+      AccOf<T> acc;
 #pragma unroll 4
-      for (int k = 0; k < K; ++k) acc += g.load(g.peer(mine, k) + c);
-      slice[Group::kGrid ? c : c - c0] = acc;
+      for (int k = 0; k < K; ++k) acc.add(g.load(g.peer(mine, k) + c));
+      slice[Group::kGrid ? c : c - c0] = acc.value();
     }
     if (!g.sync()) return false;
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
@@ -321,6 +343,10 @@ struct Engine {
   //                 a fixed order
   //   T2[vx][cy][cz] y contraction over the CTA's rows of each x-plane
   //   slotC[c]       x contraction (the CTA's partial lattice)
+  // then the group all-reduce of the partial lattices.  The sums across rows
+  // (y, x and over the CTAs) are Kahan-compensated: a control point of the
+  // 256x256x160 grid gathers ~5e5 voxels through them.  The sum within a row
+  // covers one span (at most Z / spans voxels, fixed order) and is plain FP32.
   __device__ void contract(bool num_mode, const BinMap *bm = nullptr, bool degenerate = false) {
     float *T1 = Gd;   // Gd is dead between pass A and the next update
     const int nt1 = nrow * ncz;
@@ -378,31 +404,30 @@ struct Engine {
       for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
         const int cz = t % ncz, cy = (t / ncz) % ncy, xl = t / (ncz * ncy);
         const int rb = (vx0 + xl) * Y - r0;   // local row of (vx, 0)
-        float acc = 0.0f;
+        KahanSum acc;
         for (int j = 0; j < 4; ++j) {
           const int sp = cy - j;
           if (sp < 0 || sp >= ay.nsp) continue;
           const int lo = max(ay.lo[sp], -rb), hi = min(ay.hi[sp], nrow - rb);
           const float *wy = PY + j * Y;
 #pragma unroll 4
-          for (int vy = lo; vy < hi; ++vy) acc = __fmaf_rn(wy[vy], T1[(rb + vy) * ncz + cz], acc);
+          for (int vy = lo; vy < hi; ++vy) acc.add_prod(wy[vy], T1[(rb + vy) * ncz + cz]);
         }
-        T2[t] = acc;
+        T2[t] = acc.value();
       }
       __syncthreads();
       N4_MARK(PH_F_T2);
       for (int c = threadIdx.x; c < nlat; c += blockDim.x) {
         const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
-        float acc = 0.0f;
+        KahanSum acc;
         for (int j = 0; j < 4; ++j) {
           const int sp = cx - j;
           if (sp < 0 || sp >= ax.nsp) continue;
           const int lo = max(ax.lo[sp], vx0), hi = min(ax.hi[sp], vx1 + 1);
           const float *wx = PX + j * X;
-          for (int vx = lo; vx < hi; ++vx)
-            acc = __fmaf_rn(wx[vx], T2[((vx - vx0) * ncy + cy) * ncz + cz], acc);
+          for (int vx = lo; vx < hi; ++vx) acc.add_prod(wx[vx], T2[((vx - vx0) * ncy + cy) * ncz + cz]);
         }
-        slotC[c] = acc;
+        slotC[c] = acc.value();
       }
       return;
     }
@@ -411,21 +436,21 @@ struct Engine {
     for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
       const int cz = t % ncz, cy = (t / ncz) % ncy, m = t / (ncz * ncy);
       const float *t1 = T1 + (size_t)m * Y * ncz + cz;
-      float acc = 0.0f;
+      KahanSum acc;
       for (int j = 0; j < 4; ++j) {
         const int sp = cy - j;
         if (sp < 0 || sp >= ay.nsp) continue;
         const float *wy = PY + j * Y;
 #pragma unroll 4
-        for (int vy = ay.lo[sp]; vy < ay.hi[sp]; ++vy) acc = __fmaf_rn(wy[vy], t1[vy * ncz], acc);
+        for (int vy = ay.lo[sp]; vy < ay.hi[sp]; ++vy) acc.add_prod(wy[vy], t1[vy * ncz]);
       }
-      T2[t] = acc;
+      T2[t] = acc.value();
     }
     __syncthreads();
     N4_MARK(PH_F_T2);
     for (int c = threadIdx.x; c < nlat; c += blockDim.x) {
       const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
-      float acc = 0.0f;
+      KahanSum acc;
       for (int j = 0; j < 4; ++j) {
         const int sp = cx - j;
         if (sp < 0 || sp >= ax.nsp) continue;
@@ -433,10 +458,9 @@ struct Engine {
         // local planes inside [lo, hi): vx = rank + m*K
         const int lo = ax.lo[sp], hi = ax.hi[sp];
         int m = lo <= rank ? 0 : (lo - rank + K - 1) / K;
-        for (int vx = rank + m * K; vx < hi; vx += K, ++m)
-          acc = __fmaf_rn(wx[vx], T2[(m * ncy + cy) * ncz + cz], acc);
+        for (int vx = rank + m * K; vx < hi; vx += K, ++m) acc.add_prod(wx[vx], T2[(m * ncy + cy) * ncz + cz]);
       }
-      slotC[c] = acc;
+      slotC[c] = acc.value();
     }
   }
 
@@ -494,7 +518,7 @@ struct Engine {
 
   // ---- pass B + sharpening: histogram of logU over the group, then E
   __device__ bool pass_b(const BinMap &bm) {
-    const int bins = pr.bins, shift = pl.hist_shift;
+    const int bins = pr.bins, shift = hshift;
     const double scale = ldexp(1.0, shift);
     for (int i = threadIdx.x; i < kHistCopies * bins; i += blockDim.x) hist[i] = 0u;
     __syncthreads();
@@ -596,10 +620,9 @@ struct Engine {
   __device__ void run(const VolJob &job, const float *imlog_in) {
     X = job.X; Y = job.Y; Z = job.Z;
     rank = g.rank(); K = g.size();
-    const int rows = X * Y;
-    if (Group::kGrid) {            // contiguous rows: the volume lives in global memory
-      r0 = (int)((long long)rows * rank / K);
-      nrow = (int)((long long)rows * (rank + 1) / K) - r0;
+    if constexpr (Group::kGrid) {  // contiguous rows: the volume lives in global memory
+      r0 = (int)((long long)X * Y * rank / K);
+      nrow = (int)((long long)X * Y * (rank + 1) / K) - r0;
       nplane = 0;
     } else {                       // interleaved planes: every CTA samples the whole volume
       r0 = 0;
@@ -607,9 +630,11 @@ struct Engine {
       nrow = nplane * Y;
     }
     divZ = FastDiv((unsigned)Z);
+    hshift = volume_hist_shift(X, Y, Z, K, Group::kGrid);
     imlog = imlog_in;
     const bool lead = (rank == 0 && threadIdx.x == 0);
     n4_report_t *rep = job.report;
+    if (lead) { rep->device_begin_ns = global_ns(); rep->device_end_ns = 0; rep->sm = sm_id(); }
 
 #ifdef N4_PHASE_TIMERS
     if (threadIdx.x == 0) ph_last = clock64();
@@ -717,7 +742,7 @@ struct Engine {
     }
     if (rank == 0) {
       for (int c = threadIdx.x; c < nlat; c += blockDim.x) job.lattice_out[c] = L[c];
-      if (threadIdx.x == 0) rep->status = N4_OK;
+      if (threadIdx.x == 0) { rep->status = N4_OK; rep->device_end_ns = global_ns(); }
     }
 #ifdef N4_PHASE_TIMERS
     if (lead)

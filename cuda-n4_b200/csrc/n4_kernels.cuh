@@ -203,11 +203,6 @@ __global__ void k_pool_fitgrid(const PoolJob *jobs, int nvol, __nv_bfloat16 *out
 }
 
 // ------------------------------------------------------------------ N4 kernels
-__device__ __forceinline__ void row_range(int rows, int rank, int K, int &r0, int &r1) {
-  r0 = (int)((long long)rows * rank / K);
-  r1 = (int)((long long)rows * (rank + 1) / K);
-}
-
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
 }
@@ -343,8 +338,7 @@ __global__ void __launch_bounds__(NT, 1) k_n4_grid(const __grid_constant__ GridA
   __syncthreads();
   GridGroup g{a.bar, a.big_base, a.big_stride};
   char *big = a.big_base + (size_t)blockIdx.x * a.big_stride;
-  int r0, r1;
-  row_range(a.job.X * a.job.Y, g.rank(), g.size(), r0, r1);
+  const int r0 = (int)((long long)a.job.X * a.job.Y * g.rank() / g.size());
   Engine<GridGroup> e(g, s_pl, s_pr, smem, big, a.red_global);
   e.run(a.job, a.job.imlog + (size_t)r0 * a.job.Z);
 }
@@ -372,11 +366,26 @@ struct CorrectVol {
   int vec4;              // FZ % 4 == 0 and every pointer 16-byte aligned
 };
 
-constexpr int kRowsPerTile = 128;
 constexpr int kMaxNcz = 64;
 constexpr int kLxMax = 2048;    // x-contracted lattice slice ncy*ncz held per x-plane
 
-// One CTA per tile of kRowsPerTile full-resolution rows (vy fastest within
+// Tile shapes of the correction: full-resolution rows per tile and threads
+// per CTA.  The autotuner times them per workload; kCorrectDefault is used
+// when nothing is recorded.
+struct CorrectShape {
+  int rows, threads;
+};
+constexpr int kCorrectShapes = 6;
+constexpr CorrectShape kCorrectShape[kCorrectShapes] = {{128, 256}, {64, 256}, {256, 256},
+                                                         {512, 256}, {256, 512}, {512, 512}};
+constexpr int kCorrectDefault = 0;
+// Dynamic shared memory of a correction CTA: the two x-contracted planes and
+// the tile's row contractions [rows][ncz].
+__host__ __device__ inline size_t correct_smem_bytes(int rows, int ncz) {
+  return (size_t)(2 * kLxMax + rows * ncz) * sizeof(float);
+}
+
+// One CTA per tile of `rt` full-resolution rows (vy fastest within
 // an x-plane).  Contraction of the lattice for the tile's rows into shared
 // memory, separable: per x-plane the tile touches, Lx[cy][cz] =
 // sum_jx wx L[sx+jx][cy][cz]; per row, G[r][cz] = sum_jy wy Lx[sy+jy][cz]
@@ -388,13 +397,13 @@ constexpr int kCorrectPre = 4;   // input float4 loads a thread keeps in flight
 // Tile `tile` of a batch (numbered as in CorrectVol::tile0) of the volumes
 // vols[0 .. nvol); Gs and Lx in shared memory.
 __device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long long *tile_starts, int nvol,
-                                             long long tile, float low, float *Gs, float *Lx) {
+                                             long long tile, float low, int rt, float *Gs, float *Lx) {
   const int v = find_volume(tile_starts, nvol, tile);
   const CorrectVol &C = vols[v];
   const Axis ax = axis_at(C.tx, C.FX, C.ncx), ay = axis_at(C.ty, C.FY, C.ncy), az = axis_at(C.tz, C.FZ, C.ncz);
   const long long rows = (long long)C.FX * C.FY;
-  const long long row0 = (tile - C.tile0) * (long long)kRowsPerTile;
-  const int nr = (int)min((long long)kRowsPerTile, rows - row0);
+  const long long row0 = (tile - C.tile0) * (long long)rt;
+  const int nr = (int)min((long long)rt, rows - row0);
   const int ncz = C.ncz, ncy = C.ncy;
   const int FZ = C.FZ;
   const long long base = row0 * FZ;
@@ -563,13 +572,15 @@ __device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long 
   }
 }
 
-// Tile t0 + blockIdx.x of a batch (numbered as in CorrectVol::tile0) of the
-// volumes vols[0 .. nvol).
-__global__ void __launch_bounds__(256, 3) k_correct(const CorrectVol *vols, const long long *tile_starts,
-                                                    int nvol, long long t0, float low) {
-  __shared__ float Gs[kRowsPerTile * kMaxNcz];
-  __shared__ float Lx[2 * kLxMax];
-  correct_tile(vols, tile_starts, nvol, t0 + blockIdx.x, low, Gs, Lx);
+// Tile t0 + blockIdx.x of a batch (numbered as in CorrectVol::tile0, tiles of
+// `rt` rows) of the volumes vols[0 .. nvol); dynamic shared memory
+// correct_smem_bytes(rt, ncz).
+template <int NT>
+__global__ void __launch_bounds__(NT, NT <= 256 ? 3 : 1) k_correct(const CorrectVol *vols,
+                                                                   const long long *tile_starts, int nvol,
+                                                                   long long t0, float low, int rt) {
+  extern __shared__ __align__(16) float correct_sm[];
+  correct_tile(vols, tile_starts, nvol, t0 + blockIdx.x, low, rt, correct_sm + 2 * kLxMax, correct_sm);
 }
 
 // ------------------------------------------------------------------ standalone fit
@@ -644,11 +655,22 @@ __global__ void __launch_bounds__(kFitRows) k_fit_rows(const float *field, const
 // overlap the arithmetic of others instead of the whole grid alternating
 // between loading and walking.  S = 8 (Z % 8 == 0, 32-byte aligned rows):
 // one 32-byte load per array and step, exactly one sector, not kept in L1;
-// S = 4: 16-byte loads, the sector's other half served by L1.  Dynamic
-// shared memory: kFitTableBytes(Z) (the z table: numerator and denominator
-// weights and the span of every voxel).
-constexpr int kFitRowsD = 64;     // rows (threads) per CTA
+// S = 4: 16-byte loads, the sector's other half served by L1.  R rows
+// (threads) per CTA.  Dynamic shared memory: kFitTableBytes(Z) (the z table:
+// numerator and denominator weights and the span of every voxel).
 constexpr int kFitZMaxD = 1024;
+
+// Shapes of the fit's z contraction: voxels per load step (8: 32-byte steps,
+// 4: 16-byte steps, 0: the shared-memory staged kernel k_fit_rows), steps in
+// flight per thread and rows per CTA.  The autotuner times the ones the
+// field's alignment allows; kFitDefault8 / kFitDefault4 are used otherwise.
+struct FitShape {
+  int step, depth, rows;
+};
+constexpr int kFitShapes = 10;
+constexpr FitShape kFitShape[kFitShapes] = {{8, 3, 64}, {8, 2, 64}, {8, 4, 64}, {8, 3, 32}, {8, 3, 128},
+                                            {8, 2, 128}, {4, 6, 64}, {4, 4, 64}, {4, 6, 128}, {0, 0, kFitRows}};
+constexpr int kFitDefault8 = 0, kFitDefault4 = 6, kFitScalar = 9;
 __host__ __device__ inline size_t kFitTableBytes(int Z) { return (size_t)Z * 36; }
 
 template <int S> struct FitStep { float v[S]; };
@@ -728,15 +750,15 @@ __device__ __forceinline__ void fit_table(const Axis &az, int Z, char *tab) {
   }
 }
 
-template <int S, int D>
-__global__ void __launch_bounds__(kFitRowsD, 8) k_fit_rows_v5(const float *__restrict__ field,
+template <int S, int D, int R>
+__global__ void __launch_bounds__(R, 512 / R) k_fit_rows_v5(const float *__restrict__ field,
                                                               const float *__restrict__ mask, long long rows, int Z,
                                                               Axis az, float *__restrict__ t1n,
                                                               float *__restrict__ t1d) {
   extern __shared__ __align__(16) char fit_tab[];
   const float4 *sp4 = (const float4 *)fit_tab, *sq4 = sp4 + Z;
   const int *ss = (const int *)(sq4 + Z);
-  const long long row = (long long)blockIdx.x * kFitRowsD + threadIdx.x;
+  const long long row = (long long)blockIdx.x * R + threadIdx.x;
   const bool live = row < rows;
   const int nq = Z / S;                             // steps per row
   const float *fp = field + (live ? row : 0) * Z;
@@ -789,18 +811,18 @@ __global__ void k_fit_planes(const float *t1n, const float *t1d, int X, int Y, A
        t += (long long)gridDim.x * blockDim.x) {
     const int cz = (int)(t % ncz), cy = (int)((t / ncz) % ncy);
     const long long vx = t / ((long long)ncz * ncy);
-    float an = 0.0f, ad = 0.0f;
+    KahanSum an, ad;
     for (int j = 0; j < 4; ++j) {
       const int sp = cy - j;
       if (sp < 0 || sp >= ay.nsp) continue;
       for (int vy = ay.lo[sp]; vy < ay.hi[sp]; ++vy) {
         const long long i = (vx * Y + vy) * ncz + cz;
-        an = __fmaf_rn(ay.p[j * Y + vy], t1n[i], an);
-        ad = __fmaf_rn(ay.q[j * Y + vy], t1d[i], ad);
+        an.add_prod(ay.p[j * Y + vy], t1n[i]);
+        ad.add_prod(ay.q[j * Y + vy], t1d[i]);
       }
     }
-    t2n[t] = an;
-    t2d[t] = ad;
+    t2n[t] = an.value();
+    t2d[t] = ad.value();
   }
 }
 
@@ -810,16 +832,17 @@ __global__ void k_fit_final(const float *t2n, const float *t2d, int X, Axis ax, 
   const int nlat = ncx * ncy * ncz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nlat; c += gridDim.x * blockDim.x) {
     const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
-    float an = 0.0f, ad = 0.0f;
+    KahanSum sn, sd;
     for (int j = 0; j < 4; ++j) {
       const int sp = cx - j;
       if (sp < 0 || sp >= ax.nsp) continue;
       for (int vx = ax.lo[sp]; vx < ax.hi[sp]; ++vx) {
         const long long i = ((long long)vx * ncy + cy) * ncz + cz;
-        an = __fmaf_rn(ax.p[j * X + vx], t2n[i], an);
-        ad = __fmaf_rn(ax.q[j * X + vx], t2d[i], ad);
+        sn.add_prod(ax.p[j * X + vx], t2n[i]);
+        sd.add_prod(ax.q[j * X + vx], t2d[i]);
       }
     }
+    const float an = sn.value(), ad = sd.value();
     lattice[c] = zero_den ? (ad != 0.0f ? an / ad : 0.0f) : an / (ad + eps);
   }
 }
@@ -905,6 +928,19 @@ __global__ void k_remap(const float *x, const float *mask, long long n, const do
     if (mask && mask[i] == 0.0f) { out[i] = 0.0f; continue; }
     out[i] = inv > 0.0 ? (float)sharpened_value(bm.coord(x[i]), E, bins) : x[i];
   }
+}
+
+// ------------------------------------------------------------------ autotuner helper
+// Reads n float4s (and writes one value that depends on them, so the reads
+// stay): run before a timed kernel to evict its inputs from L2 with clean
+// lines, so that the timed kernel reads from HBM and no write-back lands in it.
+__global__ void k_read_evict(const float4 *p, long long n, float *sink) {
+  float acc = 0.0f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float4 v = __ldcs(p + i);
+    acc += v.x + v.y + v.z + v.w;
+  }
+  if (acc == 1.2345678f) *sink = acc;   // practically never true; keeps the loads
 }
 
 // ------------------------------------------------------------------ standalone convergence

@@ -39,7 +39,7 @@ __all__ = [
     "N4Param", "N4", "N4Batch", "N4BatchGraph", "N4Result", "Context", "FitBspline3D",
     "EvaluateBspline3D", "UpsampleLattice3D", "upsampleLattice3D", "sharpenImage",
     "CalculateConvergenceMeasurement", "calculateConvergenceMeasurement", "N4Error",
-    "lattice_dims", "library", "autotune", "cluster_size_flag", "warm_inputs",
+    "lattice_dims", "library", "autotune", "autotune_components", "cluster_size_flag", "warm_inputs", "N4BatchHost",
 ]
 
 
@@ -166,7 +166,8 @@ class Context:
         t = _lib.n4_timings_t()
         check(_lib.load().n4_last_timings(self._h, C.byref(t)))
         return dict(stage_ms=list(t.stage_ms), launches=t.launches, fit_voxels=t.fit_voxels,
-                    full_voxels=t.full_voxels)
+                    full_voxels=t.full_voxels, fit_rows=t.fit_rows, fit_step=t.fit_step,
+                    correct_rows=t.correct_rows, correct_threads=t.correct_threads)
 
     @classmethod
     def default(cls, device: int = 0) -> "Context":
@@ -254,7 +255,8 @@ def _report_dict(r: n4_report_t) -> dict:
                 iterations=list(r.iterations[:lv]), final_cv=list(r.final_cv[:lv]),
                 warm_start_used=bool(r.warm_start_used), first_cv_warm=r.first_cv_warm,
                 first_cv_plain=r.first_cv_plain, foreground=r.foreground,
-                path={1: "cluster", 2: "grid"}.get(r.path, r.path), cluster_size=r.cluster_size)
+                path={1: "cluster", 2: "grid"}.get(r.path, r.path), cluster_size=r.cluster_size,
+                device_begin_ns=int(r.device_begin_ns), device_end_ns=int(r.device_end_ns), sm=int(r.sm))
 
 
 def N4(im, mask=None, param: Optional[N4Param] = None, warm_lattice=None, return_bias=False,
@@ -350,6 +352,58 @@ def N4Batch(volumes: Sequence, param: Optional[N4Param] = None, warm_lattices=No
     return results
 
 
+def N4BatchHost(volumes: Sequence, param: Optional[N4Param] = None, per: int = 0, encoder=None,
+                return_bias: bool = False, outputs=None, ctx: Optional[Context] = None, device: int = 0):
+    """Bias-correct volumes held in host memory (``n4_run_batched_host``):
+    uploads, batched runs and downloads overlap over sub-batches of ``per``
+    volumes.  ``volumes``: sequence of ``(im, mask)`` CPU tensors (page-locked
+    for overlapped copies; float32 images, float32 or uint8 masks, or None).
+    ``outputs``: optional preallocated ``(im_normalized, lattice)`` CPU
+    tensors per volume.  Returns ``(results, device_ms)``: a list of
+    ``N4Result`` with host tensors, and the GPU time from the first upload to
+    the last download."""
+    torch = _torch()
+    param = param or N4Param()
+    cpar = param.to_c()
+    dims = lattice_dims(param)
+    n = len(volumes)
+    arr = (n4_volume_t * n)()
+    keep, results, kinds = [], [], []
+    for i, (im, mask) in enumerate(volumes):
+        imt = torch.as_tensor(im)
+        if imt.is_cuda or imt.dtype != torch.float32 or not imt.is_contiguous():
+            raise ValueError("N4BatchHost takes contiguous float32 CPU images")
+        mk = None
+        if mask is not None:
+            mk = torch.as_tensor(mask)
+            if mk.is_cuda or mk.dtype not in (torch.float32, torch.uint8) or not mk.is_contiguous():
+                raise ValueError("masks must be contiguous float32 or uint8 CPU tensors")
+            kinds.append(mk.dtype == torch.uint8)
+        if outputs is not None:
+            out, lat = outputs[i]
+        else:
+            out = torch.empty(imt.shape, dtype=torch.float32, pin_memory=True)
+            lat = torch.empty(dims, dtype=torch.float32, pin_memory=True)
+        bias = torch.empty(imt.shape, dtype=torch.float32, pin_memory=True) if return_bias else None
+        keep += [imt, mk, out, lat, bias]
+        fx, fy, fz = (int(d) for d in imt.shape)
+        arr[i] = n4_volume_t(imt.data_ptr(), None if mk is None else mk.data_ptr(), fx, fy, fz, out.data_ptr(),
+                             lat.data_ptr(), None if bias is None else bias.data_ptr(), None)
+        results.append(N4Result(out, lat, bias, {}))
+    if kinds and len(set(kinds)) > 1:
+        raise ValueError("all masks of a batch must have one type")
+    if kinds and kinds[0]:
+        cpar.flags |= _lib.FLAG_MASK_U8
+    reps = (n4_report_t * n)()
+    ms = C.c_float()
+    c = ctx or Context.default(device)
+    check(_lib.load().n4_run_batched_host(c.handle, C.byref(cpar), n, arr, int(per),
+                                          None if encoder is None else encoder.h, reps, C.byref(ms)))
+    for r, rep in zip(results, reps):
+        r.report = _report_dict(rep)
+    return results, float(ms.value)
+
+
 def warm_inputs(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[Context] = None):
     """Network inputs of the learned warm start (``n4_warm_inputs``): every
     volume's masked log fitting grid pooled to 32x32x24, CUDA BF16
@@ -387,7 +441,9 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     (``n4_autotune``) and record the fastest in the context for later runs
     of volumes of the same sizes with the same lattice, levels and bins.
     Returns ``{"candidates": [(cluster_size, threads, ms), ...], "chosen":
-    cluster_size, "chosen_threads": threads}`` (cluster size 0 = whole-GPU
+    cluster_size, "chosen_threads": threads, "correction": [(rows, threads,
+    ms), ...], "correction_chosen": (rows, threads)}`` (cluster size 0 =
+    whole-GPU path; the correction tile shapes are timed on the chosen
     path)."""
     torch = _torch()
     param = param or N4Param()
@@ -413,7 +469,34 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     rep = _lib.n4_tune_report_t()
     check(_lib.load().n4_autotune(c.handle, C.byref(cpar), n, arr, _stream(dev), C.byref(rep)))
     cands = [(int(rep.cluster_size[k]), int(rep.threads[k]), float(rep.ms[k])) for k in range(rep.candidates)]
-    return {"candidates": cands, "chosen": cands[rep.chosen][0], "chosen_threads": cands[rep.chosen][1]}
+    corr = [(int(rep.corr_rows[k]), int(rep.corr_threads[k]), float(rep.corr_ms[k]))
+            for k in range(rep.corr_candidates)]
+    return {"candidates": cands, "chosen": cands[rep.chosen][0], "chosen_threads": cands[rep.chosen][1],
+            "correction": corr, "correction_chosen": corr[rep.corr_chosen][:2] if corr else None}
+
+
+def autotune_components(field, mask, numberOfControlPoints, ctx: Optional[Context] = None) -> dict:
+    """Time the tile shapes of the standalone fit (``FitBspline3D``) and of
+    the dense evaluation (``EvaluateBspline3D``) on this field and lattice
+    size (``n4_autotune_components``) and record the fastest of each in the
+    context; later calls with the same sizes use them.  Returns the timed
+    candidates and the chosen shapes."""
+    torch = _torch()
+    f = _dev_f32(field)
+    m = None if mask is None else _dev_f32(mask, f.device)
+    nc = tuple(int(c) for c in numberOfControlPoints)
+    lat = torch.empty(nc, dtype=torch.float32, device=f.device)
+    out = torch.empty_like(f)
+    c = ctx or Context.default(f.device.index or 0)
+    rep = _lib.n4_component_tune_t()
+    X, Y, Z = (int(d) for d in f.shape)
+    check(_lib.load().n4_autotune_components(c.handle, _ptr(f), _ptr(m), *nc, X, Y, Z, _ptr(lat), _ptr(out),
+                                             _stream(f.device), C.byref(rep)))
+    fit = [(int(rep.fit_step[k]), int(rep.fit_depth[k]), int(rep.fit_rows[k]), float(rep.fit_ms[k]))
+           for k in range(rep.fit_candidates)]
+    ev = [(int(rep.eval_rows[k]), int(rep.eval_threads[k]), float(rep.eval_ms[k])) for k in range(rep.eval_candidates)]
+    return {"fit": fit, "fit_chosen": fit[rep.fit_chosen][:3], "evaluate": ev,
+            "evaluate_chosen": ev[rep.eval_chosen][:2]}
 
 
 class N4BatchGraph:

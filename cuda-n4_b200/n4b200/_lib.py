@@ -62,6 +62,10 @@ class n4_report_t(C.Structure):
         ("foreground", C.c_longlong),
         ("path", C.c_int),
         ("cluster_size", C.c_int),
+        ("device_begin_ns", C.c_ulonglong),
+        ("device_end_ns", C.c_ulonglong),
+        ("sm", C.c_int),
+        ("reserved", C.c_int),
     ]
 
 
@@ -74,7 +78,7 @@ class n4_volume_t(C.Structure):
     ]
 
 
-N4_TUNE_MAX = 16
+N4_TUNE_MAX = 24
 
 
 class n4_tune_report_t(C.Structure):
@@ -82,6 +86,18 @@ class n4_tune_report_t(C.Structure):
         ("candidates", C.c_int), ("cluster_size", C.c_int * N4_TUNE_MAX), ("threads", C.c_int * N4_TUNE_MAX),
         ("ms", C.c_float * N4_TUNE_MAX),
         ("chosen", C.c_int),
+        ("corr_candidates", C.c_int), ("corr_rows", C.c_int * N4_TUNE_MAX),
+        ("corr_threads", C.c_int * N4_TUNE_MAX), ("corr_ms", C.c_float * N4_TUNE_MAX), ("corr_chosen", C.c_int),
+    ]
+
+
+class n4_component_tune_t(C.Structure):
+    _fields_ = [
+        ("fit_candidates", C.c_int), ("fit_step", C.c_int * N4_TUNE_MAX), ("fit_depth", C.c_int * N4_TUNE_MAX),
+        ("fit_rows", C.c_int * N4_TUNE_MAX), ("fit_ms", C.c_float * N4_TUNE_MAX), ("fit_chosen", C.c_int),
+        ("fit_shape", C.c_int),
+        ("eval_candidates", C.c_int), ("eval_rows", C.c_int * N4_TUNE_MAX), ("eval_threads", C.c_int * N4_TUNE_MAX),
+        ("eval_ms", C.c_float * N4_TUNE_MAX), ("eval_chosen", C.c_int), ("eval_shape", C.c_int),
     ]
 
 
@@ -89,6 +105,7 @@ class n4_timings_t(C.Structure):
     _fields_ = [
         ("stage_ms", C.c_float * 4), ("launches", C.c_int), ("fit_voxels", C.c_longlong),
         ("full_voxels", C.c_longlong),
+        ("fit_rows", C.c_int), ("fit_step", C.c_int), ("correct_rows", C.c_int), ("correct_threads", C.c_int),
     ]
 
 
@@ -122,6 +139,9 @@ SIGNATURES = [
     ("n4_set_profiling", C.c_int, [_P, C.c_int]),
     ("n4_last_timings", C.c_int, [_P, C.POINTER(n4_timings_t)]),
     ("n4_autotune", C.c_int, [_P, _P, C.c_int, _P, _P, _P]),
+    ("n4_run_batched_host", C.c_int, [_P, _P, C.c_int, _P, C.c_int, _P, _P, C.POINTER(C.c_float)]),
+    ("n4_autotune_components", C.c_int, [_P, _P, _P, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint,
+                                         _P, _P, _P, _P]),
     ("n4_warm_inputs", C.c_int, [_P, _P, C.c_int, _P, _P, _P]),
     ("n4_run_batched_warm", C.c_int, [_P, _P, C.c_int, _P, _P, _P, _P]),
     ("n4_batch_graph_create_warm", C.c_int, [_P, _P, C.c_int, _P, _P, _P]),

@@ -6,13 +6,28 @@
   volumes differ from the numpy ones with the same seed).
 * ``make_dataset`` — network inputs and labels: the input of a phantom is its
   masked log fitting grid pooled to 32x32x24 (``n4b200.warm_inputs``, the
-  same pooling a warm-started run does internally); its label is the
-  first-level 4x4x4 lattice of the plain GPU N4 run to convergence with one
-  fitting level at the run's shrink factor.
-* ``train_encoder`` — Adam on MSE with the tensor-core encoder.
+  same pooling a warm-started run does internally); its label comes from the
+  plain GPU N4 with one fitting level at the run's shrink factor, either the
+  lattice it converges to (``label="end"``) or the lattice it holds one
+  iteration before it stops (``label="pre"``, the default).  A warm start
+  always runs at least one iteration, so from a perfect "pre" prediction the
+  warm run repeats the plain run's last first-level iteration and continues
+  exactly as the plain run does; from an "end" prediction it runs one
+  iteration more than the plain run.
+* ``train_encoder`` — Adam on MSE with the tensor-core encoder, optionally
+  with the constant mode of the lattice weighted up (``gauge_weight``).
 * ``evaluate`` — held-out phantoms corrected batched with and without the
   learned warm start (``N4Batch(..., encoder=...)``): iterations,
   volumes/s, warm starts kept, and the log-bias difference between the runs.
+
+Why the constant mode matters.  The N4 residual ``logU - E(logU)`` is
+unchanged when a constant is added to ``logU`` (the histogram, its bin range
+and the sharpened map all shift with it), and so is every later update and
+convergence value.  The constant of the log-bias lattice is therefore never
+corrected: whatever constant the warm start hands over stays in the result,
+plus the drift ``mean(residual)`` that every iteration adds.  Its error is
+the whole raw log-bias difference between a warm and a plain run beyond the
+(small) difference of their non-constant parts.
 
 Command line (GPU)::
 
@@ -74,7 +89,36 @@ def eval_param(shrink=4, levels=4):
                    low_value=0.0, ShrinkFactor=shrink)
 
 
-def make_dataset(n, shape, seed, shrink=4, chunk=256, **gen):
+def level1_labels(vols, shrink=4, label="pre"):
+    """First-level 4x4x4 lattices [n,4,4,4] of the plain GPU N4 on ``vols``.
+
+    ``label="end"``: the lattice one fitting level converges to (CV < 0.001,
+    at most 50 iterations).  ``label="pre"``: the lattice one iteration
+    before that (zero when the plain run stops after its first iteration);
+    the volumes are rerun in groups of equal iteration count with that count
+    minus one and no convergence test, which repeats the same iterations
+    (the engine is deterministic)."""
+    import torch
+    res = N4Batch(vols, label_param(shrink))
+    lat = torch.stack([r.lattice for r in res])
+    if label == "end":
+        return lat
+    if label != "pre":
+        raise ValueError(f"unknown label kind {label!r}")
+    its = [int(r.report["iterations"][0]) for r in res]
+    for n_it in sorted(set(its)):
+        idx = [i for i, k in enumerate(its) if k == n_it]
+        if n_it <= 1:
+            lat[idx] = 0.0
+            continue
+        p = N4Param(NumberOfFittingLevels=1, MaximumNumberOfIterations=n_it - 1, ConvergenceThreshold=0.0,
+                    low_value=0.0, ShrinkFactor=shrink)
+        r2 = N4Batch([vols[i] for i in idx], p)
+        lat[idx] = torch.stack([r.lattice for r in r2])
+    return lat
+
+
+def make_dataset(n, shape, seed, shrink=4, chunk=256, label="pre", **gen):
     """(x [n,32,32,24] bf16, y [n,4,4,4] float) on the GPU."""
     import torch
     xs, ys = [], []
@@ -82,31 +126,71 @@ def make_dataset(n, shape, seed, shrink=4, chunk=256, **gen):
         m = min(chunk, n - c0)
         im, mask = phantoms_gpu(m, shape, seed + c0, **gen)
         vols = [(im[i], mask[i]) for i in range(m)]
-        res = N4Batch(vols, label_param(shrink))
-        ys.append(torch.stack([r.lattice for r in res]))
+        ys.append(level1_labels(vols, shrink, label))
         xs.append(warm_inputs(vols, label_param(shrink)))
-        del im, mask, res, vols
+        del im, mask, vols
     return torch.cat(xs), torch.cat(ys)
 
 
-def train_encoder(n_train=4096, n_val=256, shape=(128, 128, 96), epochs=20, batch=64, lr=1e-3, seed=0,
-                  shrink=4, **gen):
-    """Generate data with the plain GPU N4 and train; returns (encoder, report dict)."""
+def gauge_transform(weight: float) -> np.ndarray:
+    """Symmetric 64x64 map T that multiplies the constant mode of a 4x4x4
+    lattice (the unit vector u = ones / 8) by ``weight`` and leaves the
+    orthogonal modes alone: T = I + (weight - 1) u u^T.  Training on T y
+    weights the constant's squared error by weight^2 in the MSE; the trained
+    head is then composed with T^-1 (``fold_output``) so that the network
+    predicts lattices again."""
+    u = np.full((64, 1), 1.0 / 8.0)
+    return np.eye(64) + (float(weight) - 1.0) * (u @ u.T)
+
+
+def fold_output(params: np.ndarray, T_inv: np.ndarray) -> np.ndarray:
+    """Compose the linear head (the last 64x512 weights and 64 biases of the
+    flat parameter vector) with ``T_inv`` on its output."""
+    p = np.array(params, dtype=np.float64)
+    nw, nb = 64 * 512, 64
+    W = p[-(nw + nb):-nb].reshape(64, 512)
+    b = p[-nb:]
+    p[-(nw + nb):-nb] = (T_inv @ W).ravel()
+    p[-nb:] = T_inv @ b
+    return p.astype(np.float32)
+
+
+def train_encoder(n_train=4096, n_val=256, shape=(256, 256, 176), epochs=20, batch=64, lr=1e-3, seed=0,
+                  shrink=4, label="pre", gauge_weight=1.0, data=None, **gen):
+    """Generate data with the plain GPU N4 and train; returns (encoder, report dict).
+
+    ``data`` = (x, y, x_val, y_val) reuses a dataset from ``make_dataset``.
+    With ``gauge_weight`` w != 1 the targets are T y (``gauge_transform``) and
+    the trained head is folded with T^-1, so the constant mode's squared error
+    counts w^2 times in the loss."""
     import time
     import torch
     gen = {**TRAIN_GEN, **gen}
     t0 = time.time()
-    x, y = make_dataset(n_train, shape, seed, shrink, **gen)
-    xv, yv = make_dataset(n_val, shape, seed + 1_000_000, shrink, **gen)
+    if data is None:
+        x, y = make_dataset(n_train, shape, seed, shrink, label=label, **gen)
+        xv, yv = make_dataset(n_val, shape, seed + 1_000_000, shrink, label=label, **gen)
+    else:
+        x, y, xv, yv = data
     torch.cuda.synchronize()
     t_data = time.time() - t0
+    y = y.reshape(-1, 64)
+    yv = yv.reshape(-1, 64)
+    T = torch.tensor(gauge_transform(gauge_weight), dtype=torch.float32, device=y.device)
     enc = Encoder(max_batch=batch, seed=seed)
-    rep = train(enc, x, y.reshape(-1, 64), epochs=epochs, batch=batch, lr=lr, seed=seed,
-                x_val=xv, y_val=yv.reshape(-1, 64))
-    base = float((yv.reshape(-1, 64) - y.reshape(-1, 64).mean(0)).pow(2).mean())
-    return enc, dict(n_train=n_train, n_val=n_val, epochs=epochs, data_seconds=t_data, train_seconds=rep.seconds,
-                     loss_first_epoch=rep.losses[0], loss_last_epoch=rep.losses[-1], val_mse=rep.val_loss,
-                     val_mse_of_mean_predictor=base)
+    rep = train(enc, x, (y @ T).contiguous(), epochs=epochs, batch=batch, lr=lr, seed=seed)
+    if gauge_weight != 1.0:
+        enc.set_params(fold_output(enc.params(), gauge_transform(1.0 / gauge_weight)))
+    pred = enc.predict(xv).reshape(-1, 64)
+    err = pred - yv
+    base = float((yv - y.mean(0)).pow(2).mean())
+    const_err = err.mean(1)
+    return enc, dict(n_train=int(x.shape[0]), n_val=int(xv.shape[0]), shape=list(shape), label=label,
+                     gauge_weight=gauge_weight, epochs=epochs, data_seconds=t_data, train_seconds=rep.seconds,
+                     loss_first_epoch=rep.losses[0], loss_last_epoch=rep.losses[-1],
+                     val_mse=float(err.pow(2).mean()), val_mse_of_mean_predictor=base,
+                     val_rms_constant_error=float(const_err.pow(2).mean().sqrt()),
+                     val_max_constant_error=float(const_err.abs().max()))
 
 
 def evaluate(enc: Encoder, n_eval=256, shape=(256, 256, 176), seed=5_000_000, chunk=32, param=None, **gen):
@@ -159,6 +243,7 @@ def evaluate(enc: Encoder, n_eval=256, shape=(256, 256, 176), seed=5_000_000, ch
             dfov.append(float(d.abs().max()))
         del im, mask, vols, plain, warm
     n = len(it_plain)
+    q = lambda a, f: float(np.quantile(np.asarray(a), f))
     return dict(n_eval=n, shape=list(shape),
                 iterations_plain=float(np.mean(it_plain)), iterations_warm=float(np.mean(it_warm)),
                 level1_iterations_plain=float(np.mean(lvl1_plain)),
@@ -167,6 +252,10 @@ def evaluate(enc: Encoder, n_eval=256, shape=(256, 256, 176), seed=5_000_000, ch
                 volumes_per_s_plain_batched=n / (ms_plain / 1000.0),
                 volumes_per_s_warm_batched=n / (ms_warm / 1000.0),
                 max_abs_log_bias_diff_mask=float(np.max(dmask)),
+                median_abs_log_bias_diff_mask=q(dmask, 0.5),
+                p90_abs_log_bias_diff_mask=q(dmask, 0.9),
+                p99_abs_log_bias_diff_mask=q(dmask, 0.99),
+                share_within_0_01=float(np.mean(np.asarray(dmask) <= 0.01)),
                 max_abs_log_bias_diff_mask_mean_removed=float(np.max(dcent)),
                 median_abs_log_bias_diff_mask_mean_removed=float(np.median(dcent)),
                 max_abs_log_bias_diff_fov=float(np.max(dfov)))

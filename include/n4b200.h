@@ -92,6 +92,10 @@ typedef struct {
   long long foreground;                          /* masked voxels at fitting resolution*/
   int path;                                      /* 1 = cluster, 2 = whole-GPU grid    */
   int cluster_size;                              /* CTAs per volume                    */
+  unsigned long long device_begin_ns;            /* GPU global timer when the volume's */
+  unsigned long long device_end_ns;              /*   levels began / ended (ns)        */
+  int sm;                                        /* SM of the CTA that led the volume  */
+  int reserved;
 } n4_report_t;
 
 /* One volume of a batch (device pointers). */
@@ -106,6 +110,7 @@ typedef struct {
 } n4_volume_t;
 
 typedef struct n4_context n4_context_t;
+typedef struct n4_encoder n4_encoder_t;   /* the learned warm start, see below */
 
 /* Defaults of N4Param (cudaN4.h:24-94). */
 void n4_params_default(n4_params_t *p);
@@ -150,6 +155,21 @@ n4_status_t n4_run_host(n4_context_t *ctx, const n4_params_t *p,
                         float *h_im_normalized, float *h_lattice, float *h_bias_field,
                         const float *h_warm_lattice, n4_report_t *report);
 
+/* Batched host-pointer twin (testN4, cudaN4.h:367-387, corrects one volume
+ * per call).  vols[i] holds HOST pointers (im, mask, outputs, optional bias
+ * and warm lattice).  The volumes are corrected in sub-batches of `per`
+ * (0: the library's choice, 8) through three device staging slots: the
+ * upload of one sub-batch, the batched run of the previous one and the
+ * download of the one before run on three streams at once, so the host link
+ * and the GPU stay busy together.  Host buffers should be page-locked
+ * (cudaHostAlloc / cudaHostRegister) for the copies to overlap.  enc: the
+ * learned warm start (as n4_run_batched_warm) or NULL.  reports: n entries
+ * or NULL.  device_ms (may be NULL): GPU time from the first upload to the
+ * last download.  Synchronous. */
+n4_status_t n4_run_batched_host(n4_context_t *ctx, const n4_params_t *p, int n,
+                                const n4_volume_t *vols, int per, n4_encoder_t *enc,
+                                n4_report_t *reports, float *device_ms);
+
 /* Many volumes of uneven sizes in one persistent launch (no counterpart in
  * the reference, which corrects one volume per call).  `reports` (n entries)
  * may be NULL for a fully asynchronous call. */
@@ -182,19 +202,29 @@ n4_status_t n4_batch_graph_info(const n4_batch_graph_t *graph, int *kernel_launc
  * fits them: thread-block clusters of 16, 12, 8, 6, 4 and 2 CTAs per volume
  * (a cluster keeps its volume in shared memory; smaller clusters run more
  * volumes side by side) and, for a single volume, the whole-GPU path, each
- * with 1024 and with 512 threads per CTA.  It
- * records the fastest in the context under the key (lattice, levels, bins,
- * fitting-grid size of every volume, in order); later n4_run,
- * n4_run_batched and n4_batch_graph_create calls with the same key use it
- * unless a FORCE flag is set.  The outputs of the volumes are written as by
- * a run.  Synchronous. */
-#define N4_TUNE_MAX 16
+ * with 1024, 768 and 512 threads per CTA; then, on the fastest, every tile
+ * shape of the full-resolution correction (rows per tile x threads per CTA,
+ * timed by the correction stage's own device time).  It records both in the
+ * context under the key (lattice, levels, bins, shrink factor, fitting-grid
+ * size of every volume, in order; with the shrink factor that fixes the
+ * full-resolution sizes); later n4_run, n4_run_batched and
+ * n4_batch_graph_create calls with the same key use them unless a FORCE flag
+ * is set.  The reference's tiles are fixed (6x6x6 span blocks,
+ * cudaN4.cu:1190-1215, 1300-1330).  The outputs of the volumes are written as
+ * by a run.  Synchronous. */
+#define N4_TUNE_MAX 24
 typedef struct {
   int candidates;                  /* configurations timed                   */
   int cluster_size[N4_TUNE_MAX];   /* CTAs per volume; 0 = whole-GPU path    */
   int threads[N4_TUNE_MAX];        /* threads per CTA                        */
   float ms[N4_TUNE_MAX];           /* device time of one run of the volumes  */
   int chosen;                      /* index of the configuration recorded    */
+  /* tile shapes of the full-resolution correction on the chosen path */
+  int corr_candidates;
+  int corr_rows[N4_TUNE_MAX];      /* full-resolution rows per tile          */
+  int corr_threads[N4_TUNE_MAX];   /* threads per CTA                        */
+  float corr_ms[N4_TUNE_MAX];      /* device time of the correction stage    */
+  int corr_chosen;
 } n4_tune_report_t;
 
 n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *params, int n,
@@ -214,6 +244,8 @@ typedef struct {
   int launches;            /* kernels launched by the call                */
   long long fit_voxels;    /* fitting-grid voxels of the call             */
   long long full_voxels;   /* full-resolution voxels of the call          */
+  int fit_rows, fit_step;  /* z-contraction shape of a fit call (-1: none) */
+  int correct_rows, correct_threads;   /* correction tile (-1: none)      */
 } n4_timings_t;
 
 n4_status_t n4_set_profiling(n4_context_t *ctx, int enable);
@@ -251,6 +283,36 @@ n4_status_t n4_fit_bspline3d_noalloc(const float *d_field, const float *d_mask,
                                      unsigned int fx, unsigned int fy, unsigned int fz,
                                      float eps, int zero_den, float *d_lattice, void *stream);
 
+/* No counterpart in the reference (its fit and evaluation tiles are fixed:
+ * 6x6x6 span blocks, cudaN4.cu:1190-1215, 1300-1330).  Times every shape of
+ * n4_fit_bspline3d's z contraction that the field's alignment allows
+ * (voxels per load step, steps in flight, rows per CTA) and every tile shape
+ * of n4_evaluate_bspline3d (rows per tile, threads per CTA) on an fx*fy*fz
+ * field with an ncpt lattice, each launch after L2 has been evicted, and
+ * records the fastest of each in the context under (fx, fy, fz, ncpt and,
+ * for the fit, the alignment class of field and mask): later calls of those
+ * two entry points with that key use them.  d_field/d_mask: a field to fit;
+ * d_lattice: ncpt floats, receives the fit; d_out: fx*fy*fz floats, written
+ * by the evaluation candidates.  Synchronous. */
+typedef struct {
+  int fit_candidates;
+  int fit_step[N4_TUNE_MAX];       /* voxels per load step (0: staged kernel) */
+  int fit_depth[N4_TUNE_MAX];      /* load steps in flight per thread         */
+  int fit_rows[N4_TUNE_MAX];       /* field rows per CTA                      */
+  float fit_ms[N4_TUNE_MAX];       /* z contraction, L2 evicted               */
+  int fit_chosen, fit_shape;       /* candidate index, library shape index    */
+  int eval_candidates;
+  int eval_rows[N4_TUNE_MAX];      /* field rows per tile                     */
+  int eval_threads[N4_TUNE_MAX];   /* threads per CTA                         */
+  float eval_ms[N4_TUNE_MAX];      /* dense evaluation, L2 evicted            */
+  int eval_chosen, eval_shape;
+} n4_component_tune_t;
+n4_status_t n4_autotune_components(n4_context_t *ctx, const float *d_field, const float *d_mask,
+                                   unsigned int ncpt_x, unsigned int ncpt_y, unsigned int ncpt_z,
+                                   unsigned int fx, unsigned int fy, unsigned int fz,
+                                   float *d_lattice, float *d_out, void *stream,
+                                   n4_component_tune_t *report);
+
 /* Replaces EvaluateBspline3D (cudaN4.h:288-298). */
 n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice,
                                   unsigned int ncpt_x, unsigned int ncpt_y, unsigned int ncpt_z,
@@ -284,7 +346,6 @@ n4_status_t n4_convergence(n4_context_t *ctx, const float *d_field1, const float
  * moments.  Inputs are device arrays of batch x 32 x 32 x 24 BF16 values
  * (n4_warm_inputs writes them); outputs batch x 64 floats, first-level
  * lattices (n4_run_batched_warm uses them as warm starts). */
-typedef struct n4_encoder n4_encoder_t;
 
 size_t n4_encoder_num_params(void);
 n4_status_t n4_encoder_create(n4_encoder_t **enc, int device, int max_batch);

@@ -147,3 +147,41 @@ def test_convergence(cuda, golden_components):
     cv1 = n4b200.CalculateConvergenceMeasurement(g["cv_f1"], g["cv_f2"], g["cv_mask"], ddof=1)
     ref1 = O.CalculateConvergenceMeasurement(g["cv_f1"], g["cv_f2"], g["cv_mask"], ddof=1)
     assert cv1 == pytest.approx(ref1, rel=1e-4)
+
+
+def test_component_autotuner_records_and_reuses_tile_shapes(cuda):
+    """n4_autotune_components times the fit's z-contraction shapes and the
+    evaluation's tile shapes on one field and lattice size and records the
+    fastest of each; later FitBspline3D / EvaluateBspline3D calls with that
+    key run them (n4_last_timings reports the shape a call used), with
+    bitwise the results of the default shapes, and another size keeps the
+    defaults."""
+    import n4b200
+    rng = np.random.default_rng(41)
+    shape, nc = (64, 72, 160), (8, 7, 11)
+    f = cuda.tensor(rng.normal(0.0, 0.3, size=shape).astype(np.float32), device="cuda")
+    m = cuda.tensor((rng.random(shape) < 0.6).astype(np.float32), device="cuda")
+    ctx = n4b200.Context()
+    lat0 = n4b200.FitBspline3D(f, m, nc, ctx=ctx)
+    ev0 = n4b200.EvaluateBspline3D(lat0, nc, shape, ctx=ctx)
+    t = n4b200.autotune_components(f, m, nc, ctx=ctx)
+    assert len(t["fit"]) >= 8 and len(t["evaluate"]) >= 4
+    assert all(ms > 0 for *_, ms in t["fit"]) and all(ms > 0 for *_, ms in t["evaluate"])
+    assert t["fit_chosen"] == min(t["fit"], key=lambda c: c[3])[:3]
+    assert t["evaluate_chosen"] == min(t["evaluate"], key=lambda c: c[2])[:2]
+    ctx.set_profiling(True)
+    lat1 = n4b200.FitBspline3D(f, m, nc, ctx=ctx)
+    tf = ctx.last_timings()
+    ev1 = n4b200.EvaluateBspline3D(lat1, nc, shape, ctx=ctx)
+    te = ctx.last_timings()
+    assert (tf["fit_step"], tf["fit_rows"]) == (t["fit_chosen"][0], t["fit_chosen"][2])
+    assert (te["correct_rows"], te["correct_threads"]) == t["evaluate_chosen"]
+    assert cuda.equal(lat0, lat1) and cuda.equal(ev0, ev1)
+    # a different field size: the default shapes
+    f2, m2 = f[:, :, :80].contiguous(), m[:, :, :80].contiguous()
+    n4b200.FitBspline3D(f2, m2, nc, ctx=ctx)
+    assert (ctx.last_timings()["fit_step"], ctx.last_timings()["fit_rows"]) == (8, 64)
+    n4b200.EvaluateBspline3D(lat1, nc, (64, 72, 80), ctx=ctx)
+    assert (ctx.last_timings()["correct_rows"], ctx.last_timings()["correct_threads"]) == (128, 256)
+    ctx.set_profiling(False)
+    ctx.close()

@@ -130,6 +130,10 @@ def test_deterministic(cuda):
 
 
 def test_batched_matches_single(cuda):
+    """A volume's result does not depend on the other volumes of its batch:
+    with the same cluster size and threads per CTA, the batched run and the
+    single run do the same arithmetic (the histogram's fixed-point scale is
+    chosen per volume), so they agree bitwise."""
     import n4b200
     shapes = [(40, 48, 32), (64, 56, 40), (24, 32, 48), (56, 56, 56), (32, 24, 40)]
     vols = []
@@ -141,9 +145,9 @@ def test_batched_matches_single(cuda):
     for (im, mk), r in zip(vols, batch):
         s = n4b200.N4(im, mk, p)
         assert r.report["status"] == "N4_OK"
+        assert r.report["cluster_size"] == s.report["cluster_size"]
         assert r.report["iterations"] == s.report["iterations"]
-        assert nrel(r.lattice, s.lattice.cpu().numpy().astype(np.float64)) < 1e-6
-        assert nrel(r.im_normalized, s.im_normalized.cpu().numpy().astype(np.float64)) < 1e-6
+        assert cuda.equal(r.lattice, s.lattice) and cuda.equal(r.im_normalized, s.im_normalized)
 
 
 def test_host_path_matches_device_path(cuda):
@@ -311,9 +315,9 @@ def test_batch_graph_replays(cuda):
     g.launch()
     res = g.sync()
     single = n4b200.N4(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"), p)
-    # the histogram's fixed-point scale follows the batch's largest volume, so
-    # a volume in a batch matches its single run to round-off, not bitwise
-    assert nrel(res[0].lattice, single.lattice.cpu().numpy().astype(np.float64)) < 1e-6
+    # a volume's arithmetic depends on its cluster size, not on its batch
+    assert res[0].report["cluster_size"] == single.report["cluster_size"]
+    assert cuda.equal(res[0].lattice, single.lattice)
     g.close()
 
 
@@ -333,7 +337,7 @@ def test_autotune_records_the_fastest_configuration(cuda):
     t = n4b200.autotune(vols, p, ctx=ctx)
     sizes = [k for k, _, _ in t["candidates"]]
     assert len(sizes) >= 4 and 16 in sizes
-    assert {nt for _, nt, _ in t["candidates"]} == {512, 1024}
+    assert {nt for _, nt, _ in t["candidates"]} == {512, 768, 1024}
     assert all(ms > 0 for _, _, ms in t["candidates"])
     best = min(t["candidates"], key=lambda c: c[2])
     assert (t["chosen"], t["chosen_threads"]) == (best[0], best[1])
@@ -341,6 +345,18 @@ def test_autotune_records_the_fastest_configuration(cuda):
     for r in res:
         assert r.report["status"] == "N4_OK"
         assert r.report["cluster_size"] == t["chosen"]
+    # correction tile shapes: every shape timed on the chosen path, the
+    # fastest recorded and used by later runs of the same key, all bitwise alike
+    corr = t["correction"]
+    assert len(corr) >= 4 and all(ms > 0 for _, _, ms in corr)
+    assert t["correction_chosen"] == min(corr, key=lambda c: c[2])[:2]
+    ctx.set_profiling(True)
+    again = n4b200.N4Batch(vols, p, ctx=ctx)
+    tm = ctx.last_timings()
+    ctx.set_profiling(False)
+    assert (tm["correct_rows"], tm["correct_threads"]) == t["correction_chosen"]
+    for a, b in zip(res, again):
+        assert cuda.equal(a.im_normalized, b.im_normalized)
     # another batch shape is not affected by the record
     other = n4b200.N4Batch(vols[:2], p, ctx=ctx)
     assert all(r.report["cluster_size"] == 16 for r in other)
