@@ -213,6 +213,12 @@ def measure_components(dev, ctx, hbm_peak, reps=10):
     # its own inputs in L2 nor pays for writing back a flush's dirty lines
     flush = torch.zeros(64 << 20, dtype=torch.float32, device=dev)
 
+    # tile shapes chosen by the component autotuner for these two sizes
+    tune_fit = n4b200.autotune_components(field, fmask, (11, 11, 11), ctx=ctx)
+    big = torch.randn(full_shape, device=dev, generator=gen)
+    tune_eval = n4b200.autotune_components(big, None, (11, 11, 11), ctx=ctx)
+    del big
+
     def kernel_ms(fn, stage):
         fn()
         ctx.set_profiling(True)
@@ -221,19 +227,24 @@ def measure_components(dev, ctx, hbm_peak, reps=10):
             flush.sum()
             fn()
             tot += ctx.last_timings()["stage_ms"][stage]
+        tm = ctx.last_timings()
         ctx.set_profiling(False)
-        return tot / reps
-    ms_fit = kernel_ms(lambda: n4b200.FitBspline3D(field, fmask, (11, 11, 11), ctx=ctx), 0)
-    ms_eval = kernel_ms(lambda: n4b200.EvaluateBspline3D(lat11, (11, 11, 11), full_shape, ctx=ctx), 1)
+        return tot / reps, tm
+    ms_fit, tf = kernel_ms(lambda: n4b200.FitBspline3D(field, fmask, (11, 11, 11), ctx=ctx), 0)
+    ms_eval, te = kernel_ms(lambda: n4b200.EvaluateBspline3D(lat11, (11, 11, 11), full_shape, ctx=ctx), 1)
     nfit, nfull = field.numel(), int(np.prod(full_shape))
     del field, fmask, flush
     fit = 8 * nfit / (ms_fit / 1000) / 1e9
     ups = 4 * nfull / (ms_eval / 1000) / 1e9
     return {
         "fit_gbs": {"value": fit, "frac": fit / hbm_peak, "ms": ms_fit,
+                    "shape": {"step_voxels": tf["fit_step"], "rows_per_cta": tf["fit_rows"]},
+                    "tuner_candidates_ms": tune_fit["fit"],
                     "workload": "FitBspline3D z-contraction pass (k_fit_rows_v5) over a 256x256x160 field + "
                                 "float mask, 11^3 lattice (8 B per voxel read; L2 evicted before each call)"},
         "upsample_gbs": {"value": ups, "frac": ups / hbm_peak, "ms": ms_eval,
+                         "shape": {"rows_per_tile": te["correct_rows"], "threads": te["correct_threads"]},
+                         "tuner_candidates_ms": tune_eval["evaluate"],
                          "workload": "EvaluateBspline3D dense evaluation (k_correct) of an 11^3 lattice at "
                                      "512x512x320 (4 B per voxel written)"},
     }
@@ -495,6 +506,34 @@ def run_ours(args, rank, world, local_rank):
         barrier()
         return max_over_ranks(tot), wall
 
+    # the host link on this box: pinned H2D, D2H and both at once (8 volumes each way)
+    def link_gbs():
+        src = [a for a, _ in vols_host[:8]]
+        dst = [torch.empty(a.shape, device=dev) for a in src]
+        back = [torch.empty(a.shape, dtype=torch.float32).pin_memory() for a in src]
+        nbytes = sum(a.numel() * 4 for a in src)
+        s_up, s_dn = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+        def timed(up, down):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            for _ in range(3):
+                if up:
+                    with torch.cuda.stream(s_up):
+                        for a, d in zip(src, dst):
+                            d.copy_(a, non_blocking=True)
+                if down:
+                    with torch.cuda.stream(s_dn):
+                        for d, b in zip(dst, back):
+                            b.copy_(d, non_blocking=True)
+            torch.cuda.synchronize(dev)
+            return 3 * nbytes * (int(up) + int(down)) / (time.perf_counter() - t0) / 1e9
+        timed(True, False)
+        r = {"h2d": timed(True, False), "d2h": timed(False, True), "both_ways": timed(True, True)}
+        del dst, back
+        return r
+
+    link = link_gbs()
     ms_e2e, wall_e2e = time_e2e(vols_host)
     # the same with byte masks (N4_FLAG_MASK_U8): 1 B instead of 4 B per mask voxel over PCIe
     host_u8 = [(ih, (mh != 0).to(torch.uint8).pin_memory()) for ih, mh in vols_host]
@@ -502,6 +541,12 @@ def run_ours(args, rank, world, local_rank):
     h2d_u8 = sum(a.numel() * 4 + b.numel() for a, b in host_u8)
     h2d = sum(a.numel() * 4 + b.numel() * 4 for a, b in vols_host)
     d2h = sum(o.numel() * 4 for o in out_h) + sum(l.numel() * 4 for l in lat_h)
+
+    def link_bound(h2d_bytes):
+        # no schedule moves the step's bytes faster than the link: each
+        # direction at its one-way rate, both together at the both-ways rate
+        t = max(h2d_bytes / link["h2d"], d2h / link["d2h"], (h2d_bytes + d2h) / link["both_ways"]) / 1e9
+        return B / t
 
     comp = measure_components(dev, ctx, peaks()[0])
     c3 = measure_c3(dev, ctx)
@@ -525,11 +570,13 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": world * B * args.steps / (ms_e2e / 1000.0), "unit": "volumes/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "n4_run_batched_host (float masks, warm start, sub-batches of 8 over 3 staging slots)",
-                "wall_ms_per_step": wall_e2e / args.steps},
+                "wall_ms_per_step": wall_e2e / args.steps, "link_gbs": link,
+                "link_bound_volumes_per_s": world * link_bound(h2d)},
         "e2e_byte_masks": {"value": world * B * args.steps / (ms_e2e_u8 / 1000.0), "unit": "volumes/s",
                            "h2d_bytes_per_step": h2d_u8, "d2h_bytes_per_step": d2h,
                            "path": "same as e2e with uint8 masks (N4_FLAG_MASK_U8)",
-                           "wall_ms_per_step": wall_e2e_u8 / args.steps},
+                           "wall_ms_per_step": wall_e2e_u8 / args.steps,
+                           "link_bound_volumes_per_s": world * link_bound(h2d_u8)},
         "gpu_launches": warm.kernel_launches * args.steps,
         "sub_batches": warm.sub_batches,
         "clocks": clk,
@@ -545,7 +592,10 @@ def run_ours(args, rank, world, local_rank):
                        "max_abs_log_bias_diff_vs_plain_mean_removed": max(dcent),
                        "diff_basis": "per volume, max over the mask of |log bias (warm) - log bias (plain)| "
                                      "at full resolution; raw, and after removing its mean over the mask"},
-        "autotune": {"cluster_sizes_ms": tune["candidates"], "chosen_cluster_size": tune["chosen"]},
+        "autotune": {"cluster_sizes_ms": tune["candidates"], "chosen_cluster_size": tune["chosen"],
+                     "chosen_threads": tune["chosen_threads"], "correction_tiles_ms": tune["correction"],
+                     "chosen_correction_tile": tune["correction_chosen"], "sub_batches_ms": tune["sub_batches_ms"],
+                     "chosen_sub_batches": tune["sub_batches_chosen"]},
         "batched_without_graph": {"value": world * B * args.steps / (ms_nograph / 1000.0), "unit": "volumes/s",
                                   "ms_per_step": ms_nograph / args.steps},
         "stages_ms_per_batch": dict(zip(("prologue", "n4_levels_iterations", "tables", "correction"), st_ms)),

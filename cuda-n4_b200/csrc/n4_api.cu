@@ -105,6 +105,7 @@ struct TuneVal {
   int K;      // CTAs per cluster
   int nt;     // threads per CTA
   int corr;   // correction tile shape (index into kCorrectShape)
+  int nsub;   // overlapped sub-batches (0: the default rule)
 };
 
 constexpr int kStaticSmemReserve = 1024;
@@ -317,13 +318,14 @@ bool cluster_fits(const n4_context *ctx, const Plan &pl) {
 // record is process-wide too and the grant only ever grows.
 constexpr int kMaxDev = 64;
 std::mutex g_attr_mu;
-int g_attr_smem[kMaxDev][2];
+int g_attr_smem[kMaxDev][3];   // per thread count: 512, 768, 1024
 
 template <int NT>
 n4_status_t grant_cluster_smem(n4_context *ctx, int smem) {
+  static_assert(NT == 512 || NT == 768 || NT == 1024, "engine thread counts");
   if (ctx->device < 0 || ctx->device >= kMaxDev) return fail(N4_ERR_INVALID_ARG, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_attr_mu);
-  int &granted = g_attr_smem[ctx->device][NT == 1024 ? 1 : 0];
+  int &granted = g_attr_smem[ctx->device][NT == 512 ? 0 : (NT == 768 ? 1 : 2)];
   if (smem > granted) {
     CK(cudaFuncSetAttribute(k_n4_cluster<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     CK(cudaFuncSetAttribute(k_n4_cluster<NT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -546,6 +548,7 @@ struct Choice {
   bool grid;
   int K, nt;
   int corr = -1;   // correction tile shape; -1: the recorded or default one
+  int nsub = 0;    // overlapped sub-batches; 0: the recorded count or the default rule
 };
 
 // Autotuner key: first-level lattice, levels, bins, shrink factor and the
@@ -582,6 +585,7 @@ n4_status_t choose_path(n4_context *ctx, const n4_params_t *p, const std::vector
       c.grid = it->second.grid != 0;
       c.K = it->second.K;
       c.corr = it->second.corr;
+      c.nsub = it->second.nsub;
       if (!(p->flags & N4_FLAG_CTA_512)) c.nt = it->second.nt;
       return N4_OK;
     }
@@ -696,7 +700,7 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
   P.nsub = 1;
   const int want_sub = (int)((p->flags >> 16) & 7u);
   if (P.in_grid.empty() && n > 1 && want_sub != 1) {
-    int S = want_sub;
+    int S = want_sub ? want_sub : ch.nsub;
     if (S == 0) {
       const Plan pl = make_plan(p, ch.K, dims, false);
       int cap = 0;
@@ -1443,10 +1447,44 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
     rep.corr_candidates = k + 1;
     if (k == 0 || ms < rep.corr_ms[rep.corr_chosen]) rep.corr_chosen = k;
   }
+  ctx->profiling = 0;
+  // overlapped sub-batches (cluster path, batches of two or more): 1 to 4,
+  // each timed over two runs on the chosen configuration and tile
+  int best_sub = 0;
+  if (status == N4_OK && K > 0 && n > 1) {
+    ch.corr = rep.corr_chosen;
+    float best_sub_ms = 0.0f;
+    for (int S = 1; S <= std::min(kMaxSub, n) && status == N4_OK; ++S) {
+      ch.nsub = S;
+      status = run_volumes(ctx, p, v, st, &ch);   // untimed
+      if (status == N4_OK) status = collect(ctx, reps.data(), n);
+      if (status != N4_OK) break;
+      if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        status = fail(N4_ERR_CUDA, "cudaEventCreate failed");
+        break;
+      }
+      if (cudaEventRecord(e0, st) != cudaSuccess) status = fail(N4_ERR_CUDA, "cudaEventRecord failed");
+      for (int r = 0; r < 2 && status == N4_OK; ++r) status = run_volumes(ctx, p, v, st, &ch);
+      if (status == N4_OK && cudaEventRecord(e1, st) != cudaSuccess) status = fail(N4_ERR_CUDA, "cudaEventRecord failed");
+      if (status == N4_OK) status = collect(ctx, reps.data(), n);
+      float ms = 0.0f;
+      if (status == N4_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        status = fail(N4_ERR_CUDA, "event timing failed");
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      e0 = e1 = nullptr;
+      if (status != N4_OK) break;
+      rep.sub_ms[S - 1] = ms / 2;
+      rep.sub_candidates = S;
+      if (S == 1 || ms / 2 < best_sub_ms) { best_sub = S; best_sub_ms = ms / 2; }
+    }
+    rep.sub_chosen = best_sub;
+  }
   ctx->profiling = saved_prof;
   ctx->prof_valid = false;
   if (status != N4_OK) return status;
-  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, rep.threads[best], rep.corr_chosen};
+  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, rep.threads[best], rep.corr_chosen, best_sub};
   if (report) *report = rep;
   return N4_OK;
 }
@@ -1781,6 +1819,7 @@ n4_status_t n4_batch_graph_destroy(n4_batch_graph_t *g) {
 static bool fit_shape_ok(int k, const float *field, const float *mask, int Z) {
   const uintptr_t al = (uintptr_t)field | (uintptr_t)mask;
   const FitShape f = kFitShape[k];
+  if (f.step == 16) return Z % 16 == 0 && Z <= kFitZMaxD && (al & 63u) == 0;
   if (f.step == 8) return Z % 8 == 0 && Z <= kFitZMaxD && (al & 31u) == 0;
   if (f.step == 4) return Z % 4 == 0 && Z <= kFitZMaxD && (al & 15u) == 0;
   return true;
@@ -1797,7 +1836,7 @@ static int fit_default_shape(const float *field, const float *mask, int Z) {
 static std::vector<int> fit_key(unsigned fx, unsigned fy, unsigned fz, unsigned nx, unsigned ny, unsigned nz,
                                 const float *field, const float *mask) {
   const uintptr_t al = (uintptr_t)field | (uintptr_t)mask;
-  const int cls = (al & 31u) == 0 ? 32 : ((al & 15u) == 0 ? 16 : 4);
+  const int cls = (al & 63u) == 0 ? 64 : ((al & 31u) == 0 ? 32 : ((al & 15u) == 0 ? 16 : 4));
   return {(int)fx, (int)fy, (int)fz, (int)nx, (int)ny, (int)nz, cls};
 }
 static std::vector<int> eval_key(unsigned fx, unsigned fy, unsigned fz, unsigned nx, unsigned ny, unsigned nz) {
@@ -1826,12 +1865,15 @@ static void launch_fit_rows(int k, const float *field, const float *mask, long l
     case 6: fit_rows_as<4, 6, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
     case 7: fit_rows_as<4, 4, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
     case 8: fit_rows_as<4, 6, 128>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 10: fit_rows_as<16, 2, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 11: fit_rows_as<16, 2, 32>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 12: fit_rows_as<16, 2, 128>(field, mask, rows, Z, az, t1n, t1d, st); break;
     default:
       k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(field, mask, rows, Z, az, t1n,
                                                                                      t1d);
   }
 }
-static_assert(kFitShapes == 10, "launch_fit_rows covers every fit shape");
+static_assert(kFitShapes == 13, "launch_fit_rows covers every fit shape");
 
 // Sizes a standalone fit accepts: every extent below 2^31 (the kernels take
 // them as int), at most 2^36 field voxels and 4096 control points per axis,

@@ -178,6 +178,8 @@ struct KahanSum {
     s = t;
   }
   __device__ __forceinline__ float value() const { return __fsub_rn(s, c); }
+  // adds another compensated sum
+  __device__ __forceinline__ void merge(const KahanSum &o) { add(o.value()); }
 };
 
 // CTA-wide reduction of four values (min, max, sum, sum) into out[0..3] of

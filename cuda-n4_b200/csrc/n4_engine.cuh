@@ -38,6 +38,13 @@ __host__ __device__ inline int volume_hist_shift(int X, int Y, int Z, int K, boo
   return hist_shift_for((rpc * Z + 7) / 8 + 160);
 }
 
+// Voxels (or rows) whose loads a thread issues together in the voxel passes:
+// 4 on the whole-GPU path, whose rows are read from L2/HBM; 1 on the cluster
+// path, whose rows are in shared memory (measured: batching there only adds
+// registers and instructions).
+template <bool Grid> struct RowBatch { static constexpr int n = Grid ? 4 : 1; };
+#define kNaN __int_as_float(0x7fc00000)
+
 // ------------------------------------------------------------------ layout
 // Byte offsets of one CTA's workspace.  "sm" offsets are always in shared
 // memory; "big" offsets are in shared memory for the cluster path and in a
@@ -125,6 +132,7 @@ enum { PH_SETUP, PH_A, PH_B, PH_SHARP, PH_C, PH_FIT, PH_UPDATE, PH_A_LOOP, PH_A_
 // ------------------------------------------------------------------ engine
 template <class Group>
 struct Engine {
+  static constexpr int kRB = RowBatch<Group::kGrid>::n;
 #ifdef N4_PHASE_TIMERS
   long long ph_acc[PH_N] = {};
   long long ph_last = 0;
@@ -225,9 +233,57 @@ struct Engine {
     }
   }
 
+  // x-planes this CTA holds rows of: cluster, vx = rank + m*K for m < nplane
+  // (local rows m*Y .. m*Y + Y - 1); grid, the planes r0/Y .. (r0+nrow-1)/Y
+  __device__ __forceinline__ int nplanes_local() const {
+    if (Group::kGrid) return nrow > 0 ? (r0 + nrow - 1) / Y - r0 / Y + 1 : 0;
+    return nplane;
+  }
+  __device__ __forceinline__ int plane_vx(int m) const { return Group::kGrid ? r0 / Y + m : rank + m * K; }
+
+  // rowtab(la, Ga) and rowtab(lb, Gb) after a lattice update, through the
+  // x-contracted planes: per local x-plane, X[cy][cz] = sum_jx wx L[sx+jx][cy][cz]
+  // (into tmp for la, aux for lb, both free outside the warm-start trial),
+  // then per row G[cz] = sum_jy wy X[sy+jy][cz]: 8 loads and multiply-adds
+  // per entry instead of 32.  Falls back to rowtab2_direct when the planes'
+  // slices do not fit in a lattice-sized buffer.  The caller synchronises.
+  __device__ void rowtab2(const float *la, float *Ga, const float *lb, float *Gb) {
+    const int np = nplanes_local(), slice = ncy * ncz;
+    if ((long long)np * slice > pl.NLAT) { rowtab2_direct(la, Ga, lb, Gb); return; }
+    float *Xa = tmp, *Xb = aux;
+    for (int t = threadIdx.x; t < np * slice; t += blockDim.x) {
+      const int m = t / slice, c = t - m * slice;
+      const int vx = plane_vx(m);
+      const int sx = ax.s[vx];
+      const float4 wx = ax.w[vx];
+      const float *pa = la + (size_t)sx * slice + c, *pb = lb + (size_t)sx * slice + c;
+      float a = __fmul_rn(wx.x, pa[0]), b = __fmul_rn(wx.x, pb[0]);
+      a = __fmaf_rn(wx.y, pa[slice], a); b = __fmaf_rn(wx.y, pb[slice], b);
+      a = __fmaf_rn(wx.z, pa[2 * slice], a); b = __fmaf_rn(wx.z, pb[2 * slice], b);
+      Xa[t] = __fmaf_rn(wx.w, pa[3 * slice], a);
+      Xb[t] = __fmaf_rn(wx.w, pb[3 * slice], b);
+    }
+    __syncthreads();
+    const int vx0 = Group::kGrid ? r0 / Y : 0;
+    for (int t = threadIdx.x; t < nrow * ncz; t += blockDim.x) {
+      const int rl = t / ncz, cz = t - rl * ncz;
+      int vx, vy;
+      row_xy(rl, vx, vy);
+      const int m = Group::kGrid ? vx - vx0 : rl / Y;
+      const int sy = ay.s[vy];
+      const float4 wy = ay.w[vy];
+      const float *xa = Xa + m * slice + sy * ncz + cz, *xb = Xb + m * slice + sy * ncz + cz;
+      float a = __fmul_rn(wy.x, xa[0]), b = __fmul_rn(wy.x, xb[0]);
+      a = __fmaf_rn(wy.y, xa[ncz], a); b = __fmaf_rn(wy.y, xb[ncz], b);
+      a = __fmaf_rn(wy.z, xa[2 * ncz], a); b = __fmaf_rn(wy.z, xb[2 * ncz], b);
+      Ga[t] = __fmaf_rn(wy.w, xa[3 * ncz], a);
+      Gb[t] = __fmaf_rn(wy.w, xb[3 * ncz], b);
+    }
+  }
+
   // rowtab(la, Ga) and rowtab(lb, Gb) in one sweep (the same operations per
   // entry; the row's spans and weights are read once for both)
-  __device__ void rowtab2(const float *la, float *Ga, const float *lb, float *Gb) {
+  __device__ void rowtab2_direct(const float *la, float *Ga, const float *lb, float *Gb) {
     const int ntask = nrow * ncz;
     for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
       const int rl = t / ncz, cz = t - rl * ncz;
@@ -315,11 +371,17 @@ struct Engine {
     const int per = (n + K - 1) / K;
     const int c0 = rank * per, c1 = min(n, c0 + per);
     T *slice = Group::kGrid ? (T *)red_global : (T *)(big + pl.b_slice);
-    for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    // one warp per entry of the slice: lane l sums the partials of CTAs
+    // l, l + 32, ... (compensated for floats), then a fixed shuffle tree adds
+    // the lanes, so that the K loads of an entry are in flight together
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int c = c0 + warp; c < c1; c += nwarp) {
       AccOf<T> acc;
-#pragma unroll 4
-      for (int k = 0; k < K; ++k) acc.add(g.load(g.peer(mine, k) + c));
-      slice[Group::kGrid ? c : c - c0] = acc.value();
+      for (int k = lane; k < K; k += 32) acc.add(g.load(g.peer(mine, k) + c));
+      T v = acc.value();
+#pragma unroll
+      for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+      if (lane == 0) slice[Group::kGrid ? c : c - c0] = v;
     }
     if (!g.sync()) return false;
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
@@ -367,26 +429,63 @@ struct Engine {
           const float *iv = imlog + (size_t)rl * Z;
           const float *gr = G + rl * ncz + sp;
           const float g0 = gr[0], g1 = gr[1], g2 = gr[2], g3 = gr[3];
-          for (int vz = lo; vz < hi; ++vz) {
-            const float v = iv[vz];
-            if (isnan(v)) continue;
-            const float4 we = az.w[vz];
-            float b = __fmul_rn(we.x, g0);
-            b = __fmaf_rn(we.y, g1, b);
-            b = __fmaf_rn(we.z, g2, b);
-            b = __fmaf_rn(we.w, g3, b);
-            const float lu = __fsub_rn(v, b);
-            const float r = degenerate ? 0.0f : (float)((double)lu - sharpened_value(bm->coord(lu), E, pr.bins));
-            const float4 w = W4[vz];
-            a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
-            a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
+          if constexpr (kRB == 1) {
+            for (int vz = lo; vz < hi; ++vz) {
+              const float v = iv[vz];
+              if (isnan(v)) continue;
+              const float4 we = az.w[vz];
+              float b = __fmul_rn(we.x, g0);
+              b = __fmaf_rn(we.y, g1, b);
+              b = __fmaf_rn(we.z, g2, b);
+              b = __fmaf_rn(we.w, g3, b);
+              const float lu = __fsub_rn(v, b);
+              const float r = degenerate ? 0.0f : (float)((double)lu - sharpened_value(bm->coord(lu), E, pr.bins));
+              const float4 w = W4[vz];
+              a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
+              a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
+            }
+          } else
+          // kRB voxels at a time: their loads are issued before the
+          // first is used; the terms are added in voxel order
+          for (int vb = lo; vb < hi; vb += kRB) {
+            float v[kRB];
+#pragma unroll
+            for (int u = 0; u < kRB; ++u) v[u] = vb + u < hi ? iv[vb + u] : kNaN;
+#pragma unroll
+            for (int u = 0; u < kRB; ++u) {
+              if (isnan(v[u])) continue;
+              const int vz = vb + u;
+              const float4 we = az.w[vz];
+              float b = __fmul_rn(we.x, g0);
+              b = __fmaf_rn(we.y, g1, b);
+              b = __fmaf_rn(we.z, g2, b);
+              b = __fmaf_rn(we.w, g3, b);
+              const float lu = __fsub_rn(v[u], b);
+              const float r = degenerate ? 0.0f : (float)((double)lu - sharpened_value(bm->coord(lu), E, pr.bins));
+              const float4 w = W4[vz];
+              a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
+              a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
+            }
           }
         } else {
           const float *iv = imlog + (size_t)rl * Z;
-          for (int vz = lo; vz < hi; ++vz) {
-            if (isnan(iv[vz])) continue;
-            const float4 w = W4[vz];
-            a0 += w.x; a1 += w.y; a2 += w.z; a3 += w.w;
+          if constexpr (kRB == 1) {
+            for (int vz = lo; vz < hi; ++vz) {
+              if (isnan(iv[vz])) continue;
+              const float4 w = W4[vz];
+              a0 += w.x; a1 += w.y; a2 += w.z; a3 += w.w;
+            }
+          } else
+          for (int vb = lo; vb < hi; vb += kRB) {
+            float v[kRB];
+#pragma unroll
+            for (int u = 0; u < kRB; ++u) v[u] = vb + u < hi ? iv[vb + u] : kNaN;
+#pragma unroll
+            for (int u = 0; u < kRB; ++u) {
+              if (isnan(v[u])) continue;
+              const float4 w = W4[vb + u];
+              a0 += w.x; a1 += w.y; a2 += w.z; a3 += w.w;
+            }
           }
         }
         float *t1 = T1 + rl * ncz + sp;
@@ -404,15 +503,20 @@ struct Engine {
       for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
         const int cz = t % ncz, cy = (t / ncz) % ncy, xl = t / (ncz * ncy);
         const int rb = (vx0 + xl) * Y - r0;   // local row of (vx, 0)
-        KahanSum acc;
+        KahanSum acc, acc2;   // two chains (alternate rows), merged at the end
         for (int j = 0; j < 4; ++j) {
           const int sp = cy - j;
           if (sp < 0 || sp >= ay.nsp) continue;
           const int lo = max(ay.lo[sp], -rb), hi = min(ay.hi[sp], nrow - rb);
           const float *wy = PY + j * Y;
-#pragma unroll 4
-          for (int vy = lo; vy < hi; ++vy) acc.add_prod(wy[vy], T1[(rb + vy) * ncz + cz]);
+          int vy = lo;
+          for (; vy + 1 < hi; vy += 2) {
+            acc.add_prod(wy[vy], T1[(rb + vy) * ncz + cz]);
+            acc2.add_prod(wy[vy + 1], T1[(rb + vy + 1) * ncz + cz]);
+          }
+          if (vy < hi) acc.add_prod(wy[vy], T1[(rb + vy) * ncz + cz]);
         }
+        acc.merge(acc2);
         T2[t] = acc.value();
       }
       __syncthreads();
@@ -436,14 +540,20 @@ struct Engine {
     for (int t = threadIdx.x; t < nt2; t += blockDim.x) {
       const int cz = t % ncz, cy = (t / ncz) % ncy, m = t / (ncz * ncy);
       const float *t1 = T1 + (size_t)m * Y * ncz + cz;
-      KahanSum acc;
+      KahanSum acc, acc2;   // two chains (alternate rows), merged at the end
       for (int j = 0; j < 4; ++j) {
         const int sp = cy - j;
         if (sp < 0 || sp >= ay.nsp) continue;
         const float *wy = PY + j * Y;
-#pragma unroll 4
-        for (int vy = ay.lo[sp]; vy < ay.hi[sp]; ++vy) acc.add_prod(wy[vy], t1[vy * ncz]);
+        int vy = ay.lo[sp];
+        const int hi = ay.hi[sp];
+        for (; vy + 1 < hi; vy += 2) {
+          acc.add_prod(wy[vy], t1[vy * ncz]);
+          acc2.add_prod(wy[vy + 1], t1[(vy + 1) * ncz]);
+        }
+        if (vy < hi) acc.add_prod(wy[vy], t1[vy * ncz]);
       }
+      acc.merge(acc2);
       T2[t] = acc.value();
     }
     __syncthreads();
@@ -475,16 +585,47 @@ struct Engine {
       if (rs < per) {
         const float4 w = az.w[vz];
         const int sz = az.s[vz];
-        for (int rl = rs; rl < nrow; rl += per) {
-          const float v = imlog[rl * Z + vz];
-          if (isnan(v)) continue;   // outside the mask
-          const float lu = __fsub_rn(v, dot4(w, G + rl * ncz + sz));
-          vmin = fminf(vmin, lu);
-          vmax = fmaxf(vmax, lu);
-          if (need_cv) {
-            const float y = expm1f(-dot4(w, Gd + rl * ncz + sz));
-            sy += (double)y;
-            syy += (double)y * (double)y;
+        if constexpr (kRB == 1) {
+          for (int rl = rs; rl < nrow; rl += per) {
+            const float v = imlog[rl * Z + vz];
+            if (isnan(v)) continue;   // outside the mask
+            const float lu = __fsub_rn(v, dot4(w, G + rl * ncz + sz));
+            vmin = fminf(vmin, lu);
+            vmax = fmaxf(vmax, lu);
+            if (need_cv) {
+              const float y = expm1f(-dot4(w, Gd + rl * ncz + sz));
+              sy += (double)y;
+              syy += (double)y * (double)y;
+            }
+          }
+        } else
+        // kRB rows at a time: their loads are all issued before the
+        // first of them is used; the values are then taken in row order
+        for (int rb = rs; rb < nrow; rb += kRB * per) {
+          float v[kRB], ev[kRB], evd[kRB];
+#pragma unroll
+          for (int u = 0; u < kRB; ++u) {
+            const int rl = rb + u * per;
+            v[u] = rl < nrow ? imlog[rl * Z + vz] : kNaN;
+          }
+#pragma unroll
+          for (int u = 0; u < kRB; ++u) {
+            const int rl = rb + u * per;
+            const bool in = !isnan(v[u]);
+            ev[u] = in ? dot4(w, G + rl * ncz + sz) : 0.0f;
+            evd[u] = (in && need_cv) ? dot4(w, Gd + rl * ncz + sz) : 0.0f;
+          }
+#pragma unroll
+          for (int u = 0; u < kRB; ++u) {
+            if (isnan(v[u])) continue;   // outside the mask
+            const float lu = __fsub_rn(v[u], ev[u]);
+            vmin = fminf(vmin, lu);
+            vmax = fmaxf(vmax, lu);
+            if (need_cv) {
+              const float y = expm1f(-evd[u]);
+              sy += (double)y;
+              syy += (double)y * (double)y;
+            }
           }
         }
       }
@@ -529,21 +670,48 @@ struct Engine {
       const int rs = (int)threadIdx.x / Z, vz = (int)threadIdx.x - rs * Z;
       const float4 w = rs < per ? az.w[vz] : make_float4(0.f, 0.f, 0.f, 0.f);
       const int sz = rs < per ? az.s[vz] : 0;
-      const int sweeps = (nrow + per - 1) / per;
-      for (int k = 0; k < sweeps; ++k) {
-        const int rl = rs + k * per;
-        int key = -1;
-        unsigned qlo = 0, qhi = 0;
-        if (rs < per && rl < nrow) {
-          const float v = imlog[rl * Z + vz];
-          if (!isnan(v)) {
-            const float lu = __fsub_rn(v, dot4(w, G + rl * ncz + sz));
-            key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
+      if constexpr (kRB == 1) {
+        const int sweeps = (nrow + per - 1) / per;
+        for (int k = 0; k < sweeps; ++k) {
+          const int rl = rs + k * per;
+          int key = -1;
+          unsigned qlo = 0, qhi = 0;
+          if (rs < per && rl < nrow) {
+            const float v = imlog[rl * Z + vz];
+            if (!isnan(v)) {
+              const float lu = __fsub_rn(v, dot4(w, G + rl * ncz + sz));
+              key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
+            }
+          }
+          if (key >= 0) {
+            atomicAdd(&hc[key], qlo);
+            if (qhi) atomicAdd(&hc[key + 1], qhi);
           }
         }
-        if (key >= 0) {
-          atomicAdd(&hc[key], qlo);
-          if (qhi) atomicAdd(&hc[key + 1], qhi);
+      } else if (rs < per) {
+        // kRB rows at a time, loads first (as in pass A)
+        for (int rb = rs; rb < nrow; rb += kRB * per) {
+          float v[kRB], ev[kRB];
+#pragma unroll
+          for (int u = 0; u < kRB; ++u) {
+            const int rl = rb + u * per;
+            v[u] = rl < nrow ? imlog[rl * Z + vz] : kNaN;
+          }
+#pragma unroll
+          for (int u = 0; u < kRB; ++u) {
+            const int rl = rb + u * per;
+            ev[u] = !isnan(v[u]) ? dot4(w, G + rl * ncz + sz) : 0.0f;
+          }
+#pragma unroll
+          for (int u = 0; u < kRB; ++u) {
+            if (isnan(v[u])) continue;
+            unsigned qlo = 0, qhi = 0;
+            const int key = hist_bin(bm.coord(__fsub_rn(v[u], ev[u])), bins, scale, qlo, qhi);
+            if (key >= 0) {
+              atomicAdd(&hc[key], qlo);
+              if (qhi) atomicAdd(&hc[key + 1], qhi);
+            }
+          }
         }
       }
     } else {

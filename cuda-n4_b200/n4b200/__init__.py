@@ -471,8 +471,10 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     cands = [(int(rep.cluster_size[k]), int(rep.threads[k]), float(rep.ms[k])) for k in range(rep.candidates)]
     corr = [(int(rep.corr_rows[k]), int(rep.corr_threads[k]), float(rep.corr_ms[k]))
             for k in range(rep.corr_candidates)]
+    subs = [float(rep.sub_ms[k]) for k in range(rep.sub_candidates)]
     return {"candidates": cands, "chosen": cands[rep.chosen][0], "chosen_threads": cands[rep.chosen][1],
-            "correction": corr, "correction_chosen": corr[rep.corr_chosen][:2] if corr else None}
+            "correction": corr, "correction_chosen": corr[rep.corr_chosen][:2] if corr else None,
+            "sub_batches_ms": subs, "sub_batches_chosen": int(rep.sub_chosen)}
 
 
 def autotune_components(field, mask, numberOfControlPoints, ctx: Optional[Context] = None) -> dict:

@@ -88,6 +88,7 @@ class n4_tune_report_t(C.Structure):
         ("chosen", C.c_int),
         ("corr_candidates", C.c_int), ("corr_rows", C.c_int * N4_TUNE_MAX),
         ("corr_threads", C.c_int * N4_TUNE_MAX), ("corr_ms", C.c_float * N4_TUNE_MAX), ("corr_chosen", C.c_int),
+        ("sub_candidates", C.c_int), ("sub_ms", C.c_float * N4_TUNE_MAX), ("sub_chosen", C.c_int),
     ]
 
 

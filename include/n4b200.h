@@ -204,7 +204,8 @@ n4_status_t n4_batch_graph_info(const n4_batch_graph_t *graph, int *kernel_launc
  * volumes side by side) and, for a single volume, the whole-GPU path, each
  * with 1024, 768 and 512 threads per CTA; then, on the fastest, every tile
  * shape of the full-resolution correction (rows per tile x threads per CTA,
- * timed by the correction stage's own device time).  It records both in the
+ * timed by the correction stage's own device time) and 1 to 4 overlapped
+ * sub-batches (N4_FLAG_SUB_BATCHES).  It records all three in the
  * context under the key (lattice, levels, bins, shrink factor, fitting-grid
  * size of every volume, in order; with the shrink factor that fixes the
  * full-resolution sizes); later n4_run, n4_run_batched and
@@ -225,6 +226,11 @@ typedef struct {
   int corr_threads[N4_TUNE_MAX];   /* threads per CTA                        */
   float corr_ms[N4_TUNE_MAX];      /* device time of the correction stage    */
   int corr_chosen;
+  /* overlapped sub-batches 1..sub_candidates on the chosen path and tile
+   * (cluster path, two or more volumes; 0 candidates otherwise) */
+  int sub_candidates;
+  float sub_ms[N4_TUNE_MAX];       /* device time of one run                 */
+  int sub_chosen;                  /* sub-batches recorded (0: default rule) */
 } n4_tune_report_t;
 
 n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *params, int n,

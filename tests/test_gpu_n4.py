@@ -350,6 +350,9 @@ def test_autotune_records_the_fastest_configuration(cuda):
     corr = t["correction"]
     assert len(corr) >= 4 and all(ms > 0 for _, _, ms in corr)
     assert t["correction_chosen"] == min(corr, key=lambda c: c[2])[:2]
+    subs = t["sub_batches_ms"]
+    assert len(subs) == 4 and all(ms > 0 for ms in subs)
+    assert t["sub_batches_chosen"] == 1 + min(range(4), key=lambda k: subs[k])
     ctx.set_profiling(True)
     again = n4b200.N4Batch(vols, p, ctx=ctx)
     tm = ctx.last_timings()
