@@ -238,7 +238,8 @@ def measure_components(dev, ctx, hbm_peak, reps=10):
     ups = 4 * nfull / (ms_eval / 1000) / 1e9
     return {
         "fit_gbs": {"value": fit, "frac": fit / hbm_peak, "ms": ms_fit,
-                    "shape": {"step_voxels": tf["fit_step"], "rows_per_cta": tf["fit_rows"]},
+                    "shape": {"step_voxels": tf["fit_step"], "steps_in_flight": tf["fit_depth"],
+                              "rows_per_cta": tf["fit_rows"], "l2_prefetch": tf["fit_prefetch"]},
                     "tuner_candidates_ms": tune_fit["fit"],
                     "workload": "FitBspline3D z-contraction pass (k_fit_rows_v5) over a 256x256x160 field + "
                                 "float mask, 11^3 lattice (8 B per voxel read; L2 evicted before each call)"},

@@ -94,7 +94,7 @@ struct Slot {
   // report bookkeeping of the run that used the slot
   int nrep = 0;
   size_t off_rep = 0, off_flags = 0;
-  std::vector<int> path, csize;
+  std::vector<int> path, csize, perm;   // per descriptor: path, cluster size, caller's index
 };
 
 // Autotuner key: lattice, levels, bins and the fitting-grid size of every
@@ -557,7 +557,12 @@ struct Choice {
 TuneKey tune_key(const n4_params_t *p, const std::vector<Dims> &vols) {
   TuneKey k{(int)p->NumberOfControlPoints_x, (int)p->NumberOfControlPoints_y, (int)p->NumberOfControlPoints_z,
             (int)p->NumberOfFittingLevels, (int)p->NumberOfHistogramBins, (int)p->ShrinkFactor, (int)vols.size()};
-  for (const Dims &d : vols) { k.push_back(d.X); k.push_back(d.Y); k.push_back(d.Z); }
+  // the volumes' sizes in a canonical order: a run plans its volumes largest
+  // first, whatever order the caller passes them in
+  std::vector<std::tuple<int, int, int>> sz;
+  for (const Dims &d : vols) sz.emplace_back(d.X, d.Y, d.Z);
+  std::sort(sz.begin(), sz.end());
+  for (const auto &t : sz) { k.push_back(std::get<0>(t)); k.push_back(std::get<1>(t)); k.push_back(std::get<2>(t)); }
   return k;
 }
 
@@ -618,6 +623,7 @@ struct Prepared {
   int corr = kCorrectDefault;    // correction tile shape
   int nsub = 1;                  // sub-batches (volume ranges sub_lo[k] .. sub_lo[k + 1])
   std::vector<int> sub_lo;
+  std::vector<int> perm;         // descriptor k holds the caller's volume perm[k]
 };
 
 // Descriptor buffer: pinned host staging and its device copy.
@@ -633,11 +639,22 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
                      Prepared &P, n4_encoder_t *enc = nullptr) {
   const int n = (int)rvs.size();
   P.n = n;
-  P.rvs = rvs;
+  // descriptors hold the volumes largest first (fitting voxels), so that
+  // sub-batches, which are contiguous descriptor ranges, end with the small
+  // ones and the last launch's tail is short; reports go back in the
+  // caller's order
+  P.perm.resize(n);
+  for (int i = 0; i < n; ++i) P.perm[i] = i;
+  std::stable_sort(P.perm.begin(), P.perm.end(), [&](int a, int b) {
+    const Dims &x = rvs[a].d, &y = rvs[b].d;
+    return (long long)x.X * x.Y * x.Z > (long long)y.X * y.Y * y.Z;
+  });
+  P.rvs.resize(n);
+  for (int i = 0; i < n; ++i) P.rvs[i] = rvs[P.perm[i]];
   if (enc) {
     if (p->NumberOfControlPoints_x != 4 || p->NumberOfControlPoints_y != 4 || p->NumberOfControlPoints_z != 4)
       return fail(N4_ERR_INVALID_ARG, "the warm-start encoder predicts 4x4x4 first-level lattices");
-    for (const RunVol &r : rvs)
+    for (const RunVol &r : P.rvs)
       if (r.warm) return fail(N4_ERR_INVALID_ARG, "warm lattices are predicted by the encoder: pass none");
     TRY(ctx->warm_x.ensure((size_t)n * kPoolCells * 2, "warm-start inputs"));
     TRY(ctx->warm_lat.ensure((size_t)n * 64 * 4, "warm-start lattices"));
@@ -647,7 +664,7 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
     if (P.enc_batch < 1) return fail(N4_ERR_INVALID_ARG, "encoder has no batch capacity");
   }
   P.pr = make_dev_params(p);
-  for (const RunVol &r : rvs) P.dims.push_back(r.d);
+  for (const RunVol &r : P.rvs) P.dims.push_back(r.d);
   const std::vector<Dims> &dims = P.dims;
   Choice ch{};
   if (forced) ch = *forced;
@@ -1049,6 +1066,7 @@ n4_status_t run_volumes(n4_context *ctx, const n4_params_t *p, const std::vector
   slot.off_flags = P.o_flg;
   slot.path = P.path;
   slot.csize = P.csize;
+  slot.perm = P.perm;
   // reports back to the slot's pinned buffer
   CK(cudaMemcpyAsync(B.h + P.o_rep, B.d + P.o_rep, sizeof(n4_report_t) * P.n, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(B.h + P.o_flg, B.d + P.o_flg, 4 * P.n, cudaMemcpyDeviceToHost, st));
@@ -1076,7 +1094,7 @@ n4_status_t collect_slot(n4_context *ctx, int slot, n4_report_t *out, int n) {
     if (r.status == N4_OK && flg[i]) r.status = N4_ERR_NONFINITE;
     r.path = s.path[i];
     r.cluster_size = s.csize[i];
-    if (out && i < n) out[i] = r;
+    if (out && s.perm[i] < n) out[s.perm[i]] = r;
     if (r.status != N4_OK && worst == N4_OK) worst = (n4_status_t)r.status;
   }
   if (worst != N4_OK) return fail(worst, std::string("volume failed: ") + n4_status_string(worst));
@@ -1507,6 +1525,8 @@ n4_status_t n4_last_timings(n4_context_t *ctx, n4_timings_t *t) {
   const int fs = ctx->prof_fit_shape, cs = ctx->prof_corr_shape;
   t->fit_rows = fs >= 0 ? kFitShape[fs].rows : -1;
   t->fit_step = fs >= 0 ? kFitShape[fs].step : -1;
+  t->fit_depth = fs >= 0 ? kFitShape[fs].depth : -1;
+  t->fit_prefetch = fs >= 0 ? kFitShape[fs].prefetch : -1;
   t->correct_rows = cs >= 0 ? kCorrectShape[cs].rows : -1;
   t->correct_threads = cs >= 0 ? kCorrectShape[cs].threads : -1;
   return N4_OK;
@@ -1788,7 +1808,7 @@ n4_status_t n4_batch_graph_sync(n4_batch_graph_t *g, n4_report_t *reports, int n
     if (r.status == N4_OK && flg[i]) r.status = N4_ERR_NONFINITE;
     r.path = P.path[i];
     r.cluster_size = P.csize[i];
-    if (reports && i < n) reports[i] = r;
+    if (reports && P.perm[i] < n) reports[P.perm[i]] = r;
     if (r.status != N4_OK && worst == N4_OK) worst = (n4_status_t)r.status;
   }
   if (worst != N4_OK) return fail(worst, std::string("volume failed: ") + n4_status_string(worst));
@@ -1844,11 +1864,11 @@ static std::vector<int> eval_key(unsigned fx, unsigned fy, unsigned fz, unsigned
 }
 
 extern "C++" {
-template <int S, int D, int R>
+template <int S, int D, int R, int PF = 0>
 static void fit_rows_as(const float *field, const float *mask, long long rows, int Z, const Axis &az, float *t1n,
                         float *t1d, cudaStream_t st) {
-  k_fit_rows_v5<S, D, R><<<(unsigned)((rows + R - 1) / R), R, kFitTableBytes(Z), st>>>(field, mask, rows, Z, az, t1n,
-                                                                                      t1d);
+  k_fit_rows_v5<S, D, R, PF><<<(unsigned)((rows + R - 1) / R), R, kFitTableBytes(Z), st>>>(field, mask, rows, Z, az,
+                                                                                          t1n, t1d);
 }
 }  // extern "C++"
 
@@ -1868,12 +1888,15 @@ static void launch_fit_rows(int k, const float *field, const float *mask, long l
     case 10: fit_rows_as<16, 2, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
     case 11: fit_rows_as<16, 2, 32>(field, mask, rows, Z, az, t1n, t1d, st); break;
     case 12: fit_rows_as<16, 2, 128>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 13: fit_rows_as<8, 2, 64, 1>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 14: fit_rows_as<8, 3, 64, 1>(field, mask, rows, Z, az, t1n, t1d, st); break;
+    case 15: fit_rows_as<8, 2, 128, 1>(field, mask, rows, Z, az, t1n, t1d, st); break;
     default:
       k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(field, mask, rows, Z, az, t1n,
                                                                                      t1d);
   }
 }
-static_assert(kFitShapes == 13, "launch_fit_rows covers every fit shape");
+static_assert(kFitShapes == 16, "launch_fit_rows covers every fit shape");
 
 // Sizes a standalone fit accepts: every extent below 2^31 (the kernels take
 // them as int), at most 2^36 field voxels and 4096 control points per axis,
@@ -2041,6 +2064,7 @@ n4_status_t n4_autotune_components(n4_context_t *ctx, const float *d_field, cons
     rep.fit_step[c] = kFitShape[k].step;
     rep.fit_depth[c] = kFitShape[k].depth;
     rep.fit_rows[c] = kFitShape[k].rows;
+    rep.fit_prefetch[c] = kFitShape[k].prefetch;
     rep.fit_ms[c] = ms;
     if (c == 0 || ms < rep.fit_ms[rep.fit_chosen]) { rep.fit_chosen = c; rep.fit_shape = k; }
   }

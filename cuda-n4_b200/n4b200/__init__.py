@@ -167,6 +167,7 @@ class Context:
         check(_lib.load().n4_last_timings(self._h, C.byref(t)))
         return dict(stage_ms=list(t.stage_ms), launches=t.launches, fit_voxels=t.fit_voxels,
                     full_voxels=t.full_voxels, fit_rows=t.fit_rows, fit_step=t.fit_step,
+                    fit_depth=t.fit_depth, fit_prefetch=t.fit_prefetch,
                     correct_rows=t.correct_rows, correct_threads=t.correct_threads)
 
     @classmethod
@@ -494,10 +495,10 @@ def autotune_components(field, mask, numberOfControlPoints, ctx: Optional[Contex
     X, Y, Z = (int(d) for d in f.shape)
     check(_lib.load().n4_autotune_components(c.handle, _ptr(f), _ptr(m), *nc, X, Y, Z, _ptr(lat), _ptr(out),
                                              _stream(f.device), C.byref(rep)))
-    fit = [(int(rep.fit_step[k]), int(rep.fit_depth[k]), int(rep.fit_rows[k]), float(rep.fit_ms[k]))
-           for k in range(rep.fit_candidates)]
+    fit = [(int(rep.fit_step[k]), int(rep.fit_depth[k]), int(rep.fit_rows[k]), int(rep.fit_prefetch[k]),
+            float(rep.fit_ms[k])) for k in range(rep.fit_candidates)]
     ev = [(int(rep.eval_rows[k]), int(rep.eval_threads[k]), float(rep.eval_ms[k])) for k in range(rep.eval_candidates)]
-    return {"fit": fit, "fit_chosen": fit[rep.fit_chosen][:3], "evaluate": ev,
+    return {"fit": fit, "fit_chosen": fit[rep.fit_chosen][:4], "evaluate": ev,
             "evaluate_chosen": ev[rep.eval_chosen][:2]}
 
 

@@ -95,7 +95,8 @@ class n4_tune_report_t(C.Structure):
 class n4_component_tune_t(C.Structure):
     _fields_ = [
         ("fit_candidates", C.c_int), ("fit_step", C.c_int * N4_TUNE_MAX), ("fit_depth", C.c_int * N4_TUNE_MAX),
-        ("fit_rows", C.c_int * N4_TUNE_MAX), ("fit_ms", C.c_float * N4_TUNE_MAX), ("fit_chosen", C.c_int),
+        ("fit_rows", C.c_int * N4_TUNE_MAX), ("fit_prefetch", C.c_int * N4_TUNE_MAX),
+        ("fit_ms", C.c_float * N4_TUNE_MAX), ("fit_chosen", C.c_int),
         ("fit_shape", C.c_int),
         ("eval_candidates", C.c_int), ("eval_rows", C.c_int * N4_TUNE_MAX), ("eval_threads", C.c_int * N4_TUNE_MAX),
         ("eval_ms", C.c_float * N4_TUNE_MAX), ("eval_chosen", C.c_int), ("eval_shape", C.c_int),
@@ -106,7 +107,8 @@ class n4_timings_t(C.Structure):
     _fields_ = [
         ("stage_ms", C.c_float * 4), ("launches", C.c_int), ("fit_voxels", C.c_longlong),
         ("full_voxels", C.c_longlong),
-        ("fit_rows", C.c_int), ("fit_step", C.c_int), ("correct_rows", C.c_int), ("correct_threads", C.c_int),
+        ("fit_rows", C.c_int), ("fit_step", C.c_int), ("fit_depth", C.c_int), ("fit_prefetch", C.c_int),
+        ("correct_rows", C.c_int), ("correct_threads", C.c_int),
     ]
 
 

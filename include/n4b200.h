@@ -251,6 +251,7 @@ typedef struct {
   long long fit_voxels;    /* fitting-grid voxels of the call             */
   long long full_voxels;   /* full-resolution voxels of the call          */
   int fit_rows, fit_step;  /* z-contraction shape of a fit call (-1: none) */
+  int fit_depth, fit_prefetch;
   int correct_rows, correct_threads;   /* correction tile (-1: none)      */
 } n4_timings_t;
 
@@ -305,6 +306,7 @@ typedef struct {
   int fit_step[N4_TUNE_MAX];       /* voxels per load step (0: staged kernel) */
   int fit_depth[N4_TUNE_MAX];      /* load steps in flight per thread         */
   int fit_rows[N4_TUNE_MAX];       /* field rows per CTA                      */
+  int fit_prefetch[N4_TUNE_MAX];   /* 1: the CTA's rows requested into L2 first */
   float fit_ms[N4_TUNE_MAX];       /* z contraction, L2 evicted               */
   int fit_chosen, fit_shape;       /* candidate index, library shape index    */
   int eval_candidates;

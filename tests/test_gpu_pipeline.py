@@ -85,3 +85,27 @@ def test_nonfinite_voxel_is_reported_on_its_own_volume(cuda):
         assert _lib.STATUS[st] == "N4_ERR_NONFINITE"
         got = [_lib.STATUS[r.status] for r in reps]
         assert got == ["N4_OK", "N4_OK", "N4_ERR_NONFINITE", "N4_OK", "N4_OK", "N4_OK"], (sub, got)
+
+
+def test_reports_follow_the_callers_order(cuda):
+    """A run holds its volumes largest first (sub-batches end with the small
+    ones); outputs and reports still belong to the caller's volumes: given
+    smallest first, every volume's foreground count and iterations equal
+    those of its own single run, and its lattice is bitwise that run's
+    (same cluster size)."""
+    import n4b200
+    shapes = [(24, 24, 24), (32, 32, 24), (40, 32, 32), (48, 40, 40), (56, 48, 48), (64, 56, 56)]
+    vols = []
+    for i, sh in enumerate(shapes):
+        ph = make_phantom(sh, seed=950 + i)
+        vols.append((cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")))
+    p = _param(3)
+    p.flags |= n4b200.cluster_size_flag(8)
+    batch = n4b200.N4Batch(vols, p)
+    p1 = _param(1)
+    p1.flags |= n4b200.cluster_size_flag(8)
+    for (im, mk), r in zip(vols, batch):
+        s = n4b200.N4(im, mk, p1)
+        assert r.report["foreground"] == s.report["foreground"] == int((mk != 0).sum())
+        assert r.report["iterations"] == s.report["iterations"]
+        assert cuda.equal(r.lattice, s.lattice)
