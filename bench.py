@@ -239,7 +239,7 @@ def measure_components(dev, ctx, hbm_peak, reps=10):
     return {
         "fit_gbs": {"value": fit, "frac": fit / hbm_peak, "ms": ms_fit,
                     "shape": {"step_voxels": tf["fit_step"], "steps_in_flight": tf["fit_depth"],
-                              "rows_per_cta": tf["fit_rows"], "l2_prefetch": tf["fit_prefetch"]},
+                              "rows_per_cta": tf["fit_rows"]},
                     "tuner_candidates_ms": tune_fit["fit"],
                     "workload": "FitBspline3D z-contraction pass (k_fit_rows_v5) over a 256x256x160 field + "
                                 "float mask, 11^3 lattice (8 B per voxel read; L2 evicted before each call)"},
@@ -270,9 +270,18 @@ def measure_c3(dev, ctx, reps=2):
     e1.record()
     torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1) / reps
+    # stage times of one run (library events on the launching stream)
+    ctx.set_profiling(True)
+    n4b200.N4(im[0], mk[0], p, ctx=ctx)
+    t = ctx.last_timings()
+    ctx.set_profiling(False)
+    st = dict(zip(("prologue", "n4_levels_iterations", "tables", "correction"), t["stage_ms"]))
+    full = t["full_voxels"]
     return {"workload": "512x512x320 float32 phantom, shrink 2 -> 256x256x160, 4 levels, <=50 it/level, CV<0.001",
             "ms_per_volume": ms, "volumes_per_s": 1000.0 / ms, "iterations": res.report["iterations"][:4],
-            "path": res.report["path"], "ctas": res.report["cluster_size"]}
+            "path": res.report["path"], "ctas": res.report["cluster_size"], "stages_ms": st,
+            "prologue_gbs": (8 * full + 4 * t["fit_voxels"]) / (st["prologue"] / 1000.0) / 1e9,
+            "correction_gbs": 8 * full / (st["correction"] / 1000.0) / 1e9}
 
 
 def schedule_summary(reports, fit_voxels):
@@ -570,7 +579,7 @@ def run_ours(args, rank, world, local_rank):
         },
         "e2e": {"value": world * B * args.steps / (ms_e2e / 1000.0), "unit": "volumes/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "path": "n4_run_batched_host (float masks, warm start, sub-batches of 8 over 3 staging slots)",
+                "path": "n4_run_batched_host (float masks, warm start, sub-batches of 8 on 4 lanes)",
                 "wall_ms_per_step": wall_e2e / args.steps, "link_gbs": link,
                 "link_bound_volumes_per_s": world * link_bound(h2d)},
         "e2e_byte_masks": {"value": world * B * args.steps / (ms_e2e_u8 / 1000.0), "unit": "volumes/s",

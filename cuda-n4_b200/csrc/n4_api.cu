@@ -106,11 +106,13 @@ struct TuneVal {
   int nt;     // threads per CTA
   int corr;   // correction tile shape (index into kCorrectShape)
   int nsub;   // overlapped sub-batches (0: the default rule)
+  int taper;  // 1: the first and last sub-batch half the size of the others
 };
 
 constexpr int kStaticSmemReserve = 1024;
 constexpr int kSlots = 4;
 constexpr int kMaxSub = 4;   // sub-batches of a pipelined batch
+constexpr int kHostLanes = 4;   // lanes of n4_run_batched_host
 
 }  // namespace
 
@@ -122,11 +124,10 @@ struct n4_context {
   DevBuf s1, s2, s3, s4, s5;   // component scratch
   DevBuf warm_x, warm_lat;     // learned warm start: network inputs, predicted lattices
   DevBuf h_im, h_mask, h_out, h_lat, h_bias, h_warm;   // host-run staging
-  // pipelined host batches: device staging slots and the upload, run and
-  // download streams with one event of each kind per slot
+  // pipelined host batches: one stream and one device staging slot per lane
   DevBuf hb;
-  cudaStream_t hst[3] = {};
-  cudaEvent_t hev[3 * 4] = {};
+  cudaStream_t hst[kHostLanes] = {};
+  cudaEvent_t hev[kHostLanes] = {};
   cudaEvent_t hclock[2] = {};
   Slot slots[kSlots];
   int next_slot = 0;
@@ -549,6 +550,7 @@ struct Choice {
   int K, nt;
   int corr = -1;   // correction tile shape; -1: the recorded or default one
   int nsub = 0;    // overlapped sub-batches; 0: the recorded count or the default rule
+  int taper = 0;   // 1: first and last sub-batch half-size (three or more sub-batches)
 };
 
 // Autotuner key: first-level lattice, levels, bins, shrink factor and the
@@ -591,6 +593,7 @@ n4_status_t choose_path(n4_context *ctx, const n4_params_t *p, const std::vector
       c.K = it->second.K;
       c.corr = it->second.corr;
       c.nsub = it->second.nsub;
+      c.taper = it->second.taper;
       if (!(p->flags & N4_FLAG_CTA_512)) c.nt = it->second.nt;
       return N4_OK;
     }
@@ -727,7 +730,17 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
     P.nsub = std::max(1, std::min(std::min(S, kMaxSub), n));
   }
   P.sub_lo.resize(P.nsub + 1);
-  for (int k = 0; k <= P.nsub; ++k) P.sub_lo[k] = (int)((long long)n * k / P.nsub);
+  if (P.nsub >= 3 && ch.taper && !want_sub) {
+    // half-size first and last sub-batches: the first N4 launch starts after a
+    // shorter prologue, and a shorter correction follows the last one
+    const int S = P.nsub;
+    for (int k = 0; k <= S; ++k) {
+      const int w2 = k == 0 ? 0 : (k == S ? 2 * (S - 1) : 2 * k - 1);   // twice the cumulative weight
+      P.sub_lo[k] = (int)((long long)n * w2 / (2 * (S - 1)));
+    }
+  } else {
+    for (int k = 0; k <= P.nsub; ++k) P.sub_lo[k] = (int)((long long)n * k / P.nsub);
+  }
   // workspaces
   P.NCX = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
   P.NCY = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);
@@ -1468,12 +1481,16 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
   ctx->profiling = 0;
   // overlapped sub-batches (cluster path, batches of two or more): 1 to 4,
   // each timed over two runs on the chosen configuration and tile
-  int best_sub = 0;
+  int best_sub = 0, best_taper = 0;
   if (status == N4_OK && K > 0 && n > 1) {
     ch.corr = rep.corr_chosen;
     float best_sub_ms = 0.0f;
-    for (int S = 1; S <= std::min(kMaxSub, n) && status == N4_OK; ++S) {
+    // 1..4 even sub-batches, then 3 and 4 with half-size ends
+    const int nc = std::min(kMaxSub, n) + (n >= 4 ? 2 : 0);
+    for (int c = 0; c < nc && status == N4_OK; ++c) {
+      const int S = c < std::min(kMaxSub, n) ? c + 1 : c - std::min(kMaxSub, n) + 3;
       ch.nsub = S;
+      ch.taper = c >= std::min(kMaxSub, n) ? 1 : 0;
       status = run_volumes(ctx, p, v, st, &ch);   // untimed
       if (status == N4_OK) status = collect(ctx, reps.data(), n);
       if (status != N4_OK) break;
@@ -1493,16 +1510,17 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
       cudaEventDestroy(e1);
       e0 = e1 = nullptr;
       if (status != N4_OK) break;
-      rep.sub_ms[S - 1] = ms / 2;
-      rep.sub_candidates = S;
-      if (S == 1 || ms / 2 < best_sub_ms) { best_sub = S; best_sub_ms = ms / 2; }
+      rep.sub_ms[c] = ms / 2;
+      rep.sub_count[c] = S;
+      rep.sub_tapered[c] = ch.taper;
+      rep.sub_candidates = c + 1;
+      if (c == 0 || ms / 2 < best_sub_ms) { best_sub = S; best_taper = ch.taper; best_sub_ms = ms / 2; rep.sub_chosen = c; }
     }
-    rep.sub_chosen = best_sub;
   }
   ctx->profiling = saved_prof;
   ctx->prof_valid = false;
   if (status != N4_OK) return status;
-  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, rep.threads[best], rep.corr_chosen, best_sub};
+  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, rep.threads[best], rep.corr_chosen, best_sub, best_taper};
   if (report) *report = rep;
   return N4_OK;
 }
@@ -1526,7 +1544,6 @@ n4_status_t n4_last_timings(n4_context_t *ctx, n4_timings_t *t) {
   t->fit_rows = fs >= 0 ? kFitShape[fs].rows : -1;
   t->fit_step = fs >= 0 ? kFitShape[fs].step : -1;
   t->fit_depth = fs >= 0 ? kFitShape[fs].depth : -1;
-  t->fit_prefetch = fs >= 0 ? kFitShape[fs].prefetch : -1;
   t->correct_rows = cs >= 0 ? kCorrectShape[cs].rows : -1;
   t->correct_threads = cs >= 0 ? kCorrectShape[cs].threads : -1;
   return N4_OK;
@@ -1598,26 +1615,24 @@ n4_status_t n4_run_batched_host(n4_context_t *ctx, const n4_params_t *p, int n, 
   if (enc && any_warm) return fail(N4_ERR_INVALID_ARG, "warm lattices are predicted by the encoder: pass none");
   if (per == 0) per = std::min(n, 8);
   per = std::min(per, n);
-  // one staging slot: per volumes of input, mask, output, bias, lattice, warm lattice
+  // one staging slot per lane: per volumes of input, mask, output, bias, lattice, warm lattice
   auto al = [](size_t b) { return align_up(b, 256); };
   const size_t vin = al(vmax * 4), vmask = any_mask ? al(vmax * mask_b) : 0, vout = al(vmax * 4),
                vbias = any_bias ? al(vmax * 4) : 0, vlat = al(nlat * 4), vwarm = any_warm ? al(nwarm * 4) : 0;
   const size_t per_vol = vin + vmask + vout + vbias + vlat + vwarm;
-  constexpr int D = 3;   // staging slots: upload k + 2 while k + 1 runs and k downloads
-  TRY(ctx->hb.ensure((size_t)D * per * per_vol, "host-batch staging"));
+  constexpr int L = kHostLanes;
+  TRY(ctx->hb.ensure((size_t)L * per * per_vol, "host-batch staging"));
   for (cudaStream_t &s2 : ctx->hst)
     if (!s2) CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
   for (cudaEvent_t &e : ctx->hev)
     if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   for (cudaEvent_t &e : ctx->hclock)
     if (!e) CK(cudaEventCreate(&e));
-  cudaStream_t up = ctx->hst[0], run = ctx->hst[1], down = ctx->hst[2];
-  auto ev_up = [&](int d) { return ctx->hev[d]; };
-  auto ev_run = [&](int d) { return ctx->hev[4 + d]; };
-  auto ev_down = [&](int d) { return ctx->hev[8 + d]; };
-  // the previous work of this context (any stream) comes first
-  if (ctx->last_done && ctx->last_slot >= 0) CK(cudaStreamWaitEvent(up, ctx->last_done, 0));
-  CK(cudaEventRecord(ctx->hclock[0], up));
+  // every lane starts after the context's earlier work and after the clock
+  cudaStream_t lane0 = ctx->hst[0];
+  if (ctx->last_done && ctx->last_slot >= 0) CK(cudaStreamWaitEvent(lane0, ctx->last_done, 0));
+  CK(cudaEventRecord(ctx->hclock[0], lane0));
+  for (int l = 1; l < L; ++l) CK(cudaStreamWaitEvent(ctx->hst[l], ctx->hclock[0], 0));
   const int nsb = (n + per - 1) / per;
   std::vector<int> run_slot(nsb, -1);
   n4_status_t worst = N4_OK;
@@ -1631,22 +1646,25 @@ n4_status_t n4_run_batched_host(n4_context_t *ctx, const n4_params_t *p, int n, 
     return N4_OK;
   };
   for (int k = 0; k < nsb; ++k) {
-    const int d = k % D, lo = k * per, cnt = std::min(per, n - lo);
-    char *base = (char *)ctx->hb.p + (size_t)d * per * per_vol;
-    auto vol_at = [&](int j) { return base + (size_t)j * per_vol; };
-    // upload: after the download that last used this staging slot
-    if (k >= D) CK(cudaStreamWaitEvent(up, ev_down(d), 0));
+    // sub-batch k on lane k % L: its uploads, its run and its downloads in
+    // that lane's stream order (so the lane's staging slot is free again once
+    // its previous downloads are done); the runs of successive sub-batches
+    // are ordered by the context (each waits for the previous run, not for
+    // its downloads), and the copies of the other lanes overlap them
+    const int l = k % L, lo = k * per, cnt = std::min(per, n - lo);
+    cudaStream_t st = ctx->hst[l];
+    char *base = (char *)ctx->hb.p + (size_t)l * per * per_vol;
     std::vector<RunVol> rvs(cnt);
     for (int j = 0; j < cnt; ++j) {
       const n4_volume_t &q = vols[lo + j];
       const size_t nv = (size_t)q.fx * q.fy * q.fz;
-      char *v = vol_at(j);
+      char *v = base + (size_t)j * per_vol;
       float *im = (float *)v, *mk = (float *)(v + vin), *out = (float *)(v + vin + vmask),
             *bias = (float *)(v + vin + vmask + vout), *lat = (float *)(v + vin + vmask + vout + vbias),
             *warm = (float *)(v + vin + vmask + vout + vbias + vlat);
-      CK(cudaMemcpyAsync(im, q.im, nv * 4, cudaMemcpyHostToDevice, up));
-      if (q.mask) CK(cudaMemcpyAsync(mk, q.mask, nv * mask_b, cudaMemcpyHostToDevice, up));
-      if (q.warm_lattice) CK(cudaMemcpyAsync(warm, q.warm_lattice, nwarm * 4, cudaMemcpyHostToDevice, up));
+      CK(cudaMemcpyAsync(im, q.im, nv * 4, cudaMemcpyHostToDevice, st));
+      if (q.mask) CK(cudaMemcpyAsync(mk, q.mask, nv * mask_b, cudaMemcpyHostToDevice, st));
+      if (q.warm_lattice) CK(cudaMemcpyAsync(warm, q.warm_lattice, nwarm * 4, cudaMemcpyHostToDevice, st));
       RunVol &r = rvs[j];
       TRY(make_dims(p, q.fx, q.fy, q.fz, r.d));
       r.im = im;
@@ -1656,30 +1674,29 @@ n4_status_t n4_run_batched_host(n4_context_t *ctx, const n4_params_t *p, int n, 
       r.bias = q.bias_field ? bias : nullptr;
       r.warm = q.warm_lattice ? warm : nullptr;
     }
-    CK(cudaEventRecord(ev_up(d), up));
-    // the run: its descriptor slot is the one run k - 4 used; take that run's
-    // reports before the slot is reused
+    // the run's descriptor slot is the one run k - kSlots used: take that
+    // run's reports first
     TRY(harvest(k - kSlots));
-    CK(cudaStreamWaitEvent(run, ev_up(d), 0));
-    TRY(run_volumes(ctx, p, rvs, run, nullptr, enc));
+    TRY(run_volumes(ctx, p, rvs, st, nullptr, enc));
     run_slot[k] = ctx->last_slot;
-    CK(cudaEventRecord(ev_run(d), run));
-    // download
-    CK(cudaStreamWaitEvent(down, ev_run(d), 0));
     for (int j = 0; j < cnt; ++j) {
       const n4_volume_t &q = vols[lo + j];
       const size_t nv = (size_t)q.fx * q.fy * q.fz;
       const RunVol &r = rvs[j];
-      CK(cudaMemcpyAsync(q.im_normalized, r.out, nv * 4, cudaMemcpyDeviceToHost, down));
-      CK(cudaMemcpyAsync(q.lattice, r.lat, nlat * 4, cudaMemcpyDeviceToHost, down));
-      if (q.bias_field) CK(cudaMemcpyAsync(q.bias_field, r.bias, nv * 4, cudaMemcpyDeviceToHost, down));
+      CK(cudaMemcpyAsync(q.im_normalized, r.out, nv * 4, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(q.lattice, r.lat, nlat * 4, cudaMemcpyDeviceToHost, st));
+      if (q.bias_field) CK(cudaMemcpyAsync(q.bias_field, r.bias, nv * 4, cudaMemcpyDeviceToHost, st));
     }
-    CK(cudaEventRecord(ev_down(d), down));
   }
-  CK(cudaEventRecord(ctx->hclock[1], down));
+  // join the lanes on lane 0
+  for (int l = 1; l < L; ++l) {
+    CK(cudaEventRecord(ctx->hev[l], ctx->hst[l]));
+    CK(cudaStreamWaitEvent(lane0, ctx->hev[l], 0));
+  }
+  CK(cudaEventRecord(ctx->hclock[1], lane0));
   // later work of this context waits for the downloads
-  CK(cudaEventRecord(ctx->last_done, down));
-  ctx->last_stream = down;
+  CK(cudaEventRecord(ctx->last_done, lane0));
+  ctx->last_stream = lane0;
   for (int k = std::max(0, nsb - kSlots); k < nsb; ++k) TRY(harvest(k));
   CK(cudaEventSynchronize(ctx->hclock[1]));
   if (device_ms) CK(cudaEventElapsedTime(device_ms, ctx->hclock[0], ctx->hclock[1]));
@@ -1864,11 +1881,11 @@ static std::vector<int> eval_key(unsigned fx, unsigned fy, unsigned fz, unsigned
 }
 
 extern "C++" {
-template <int S, int D, int R, int PF = 0>
+template <int S, int D, int R>
 static void fit_rows_as(const float *field, const float *mask, long long rows, int Z, const Axis &az, float *t1n,
                         float *t1d, cudaStream_t st) {
-  k_fit_rows_v5<S, D, R, PF><<<(unsigned)((rows + R - 1) / R), R, kFitTableBytes(Z), st>>>(field, mask, rows, Z, az,
-                                                                                          t1n, t1d);
+  k_fit_rows_v5<S, D, R><<<(unsigned)((rows + R - 1) / R), R, kFitTableBytes(Z), st>>>(field, mask, rows, Z, az, t1n,
+                                                                                      t1d);
 }
 }  // extern "C++"
 
@@ -1888,15 +1905,12 @@ static void launch_fit_rows(int k, const float *field, const float *mask, long l
     case 10: fit_rows_as<16, 2, 64>(field, mask, rows, Z, az, t1n, t1d, st); break;
     case 11: fit_rows_as<16, 2, 32>(field, mask, rows, Z, az, t1n, t1d, st); break;
     case 12: fit_rows_as<16, 2, 128>(field, mask, rows, Z, az, t1n, t1d, st); break;
-    case 13: fit_rows_as<8, 2, 64, 1>(field, mask, rows, Z, az, t1n, t1d, st); break;
-    case 14: fit_rows_as<8, 3, 64, 1>(field, mask, rows, Z, az, t1n, t1d, st); break;
-    case 15: fit_rows_as<8, 2, 128, 1>(field, mask, rows, Z, az, t1n, t1d, st); break;
     default:
       k_fit_rows<<<(unsigned)((rows + kFitRows - 1) / kFitRows), kFitRows, 0, st>>>(field, mask, rows, Z, az, t1n,
                                                                                      t1d);
   }
 }
-static_assert(kFitShapes == 16, "launch_fit_rows covers every fit shape");
+static_assert(kFitShapes == 13, "launch_fit_rows covers every fit shape");
 
 // Sizes a standalone fit accepts: every extent below 2^31 (the kernels take
 // them as int), at most 2^36 field voxels and 4096 control points per axis,
@@ -2064,7 +2078,6 @@ n4_status_t n4_autotune_components(n4_context_t *ctx, const float *d_field, cons
     rep.fit_step[c] = kFitShape[k].step;
     rep.fit_depth[c] = kFitShape[k].depth;
     rep.fit_rows[c] = kFitShape[k].rows;
-    rep.fit_prefetch[c] = kFitShape[k].prefetch;
     rep.fit_ms[c] = ms;
     if (c == 0 || ms < rep.fit_ms[rep.fit_chosen]) { rep.fit_chosen = c; rep.fit_shape = k; }
   }

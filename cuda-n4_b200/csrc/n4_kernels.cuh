@@ -666,13 +666,12 @@ constexpr int kFitZMaxD = 1024;
 // flight per thread and rows per CTA.  The autotuner times the ones the
 // field's alignment allows; kFitDefault8 / kFitDefault4 are used otherwise.
 struct FitShape {
-  int step, depth, rows, prefetch;   // prefetch: the CTA's rows are first requested into L2 as one block
+  int step, depth, rows;
 };
-constexpr int kFitShapes = 16;
-constexpr FitShape kFitShape[kFitShapes] = {
-    {8, 3, 64, 0},  {8, 2, 64, 0},  {8, 4, 64, 0},  {8, 3, 32, 0},  {8, 3, 128, 0},   {8, 2, 128, 0},
-    {4, 6, 64, 0},  {4, 4, 64, 0},  {4, 6, 128, 0}, {0, 0, kFitRows, 0}, {16, 2, 64, 0}, {16, 2, 32, 0},
-    {16, 2, 128, 0}, {8, 2, 64, 1}, {8, 3, 64, 1},  {8, 2, 128, 1}};
+constexpr int kFitShapes = 13;
+constexpr FitShape kFitShape[kFitShapes] = {{8, 3, 64},  {8, 2, 64},  {8, 4, 64},  {8, 3, 32},  {8, 3, 128},
+                                            {8, 2, 128}, {4, 6, 64},  {4, 4, 64},  {4, 6, 128}, {0, 0, kFitRows},
+                                            {16, 2, 64}, {16, 2, 32}, {16, 2, 128}};
 constexpr int kFitDefault8 = 0, kFitDefault4 = 6, kFitScalar = 9;
 __host__ __device__ inline size_t kFitTableBytes(int Z) { return (size_t)Z * 36; }
 
@@ -764,12 +763,7 @@ __device__ __forceinline__ void fit_table(const Axis &az, int Z, char *tab) {
   }
 }
 
-// PF: thread 0 first asks L2 for the CTA's whole block of rows of field and
-// mask (cp.async.bulk.prefetch.L2, a hint that completes on its own), so that
-// DRAM is read in contiguous blocks while the row walks below read 32-byte
-// pieces of every row at once.  Needs the block's byte size a multiple of 16
-// (Z % 4 == 0) and 16-byte aligned rows, which every vector shape has.
-template <int S, int D, int R, int PF = 0>
+template <int S, int D, int R>
 __global__ void __launch_bounds__(R, 512 / R) k_fit_rows_v5(const float *__restrict__ field,
                                                               const float *__restrict__ mask, long long rows, int Z,
                                                               Axis az, float *__restrict__ t1n,
@@ -782,13 +776,6 @@ __global__ void __launch_bounds__(R, 512 / R) k_fit_rows_v5(const float *__restr
   const int nq = Z / S;                             // steps per row
   const float *fp = field + (live ? row : 0) * Z;
   const float *mp = mask ? mask + (live ? row : 0) * Z : nullptr;
-  if (PF && threadIdx.x == 0) {
-    const long long r0 = (long long)blockIdx.x * R;
-    const long long nr = rows - r0 < R ? rows - r0 : R;
-    const unsigned bytes = (unsigned)(nr * Z * 4);
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(field + r0 * Z), "r"(bytes) : "memory");
-    if (mask) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(mask + r0 * Z), "r"(bytes) : "memory");
-  }
   FitStep<S> F[D], M[D];
   // the first steps are requested before the table is built
 #pragma unroll

@@ -167,7 +167,7 @@ class Context:
         check(_lib.load().n4_last_timings(self._h, C.byref(t)))
         return dict(stage_ms=list(t.stage_ms), launches=t.launches, fit_voxels=t.fit_voxels,
                     full_voxels=t.full_voxels, fit_rows=t.fit_rows, fit_step=t.fit_step,
-                    fit_depth=t.fit_depth, fit_prefetch=t.fit_prefetch,
+                    fit_depth=t.fit_depth,
                     correct_rows=t.correct_rows, correct_threads=t.correct_threads)
 
     @classmethod
@@ -472,10 +472,10 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     cands = [(int(rep.cluster_size[k]), int(rep.threads[k]), float(rep.ms[k])) for k in range(rep.candidates)]
     corr = [(int(rep.corr_rows[k]), int(rep.corr_threads[k]), float(rep.corr_ms[k]))
             for k in range(rep.corr_candidates)]
-    subs = [float(rep.sub_ms[k]) for k in range(rep.sub_candidates)]
+    subs = [(int(rep.sub_count[k]), bool(rep.sub_tapered[k]), float(rep.sub_ms[k])) for k in range(rep.sub_candidates)]
     return {"candidates": cands, "chosen": cands[rep.chosen][0], "chosen_threads": cands[rep.chosen][1],
             "correction": corr, "correction_chosen": corr[rep.corr_chosen][:2] if corr else None,
-            "sub_batches_ms": subs, "sub_batches_chosen": int(rep.sub_chosen)}
+            "sub_batches_ms": subs, "sub_batches_chosen": subs[rep.sub_chosen][:2] if subs else None}
 
 
 def autotune_components(field, mask, numberOfControlPoints, ctx: Optional[Context] = None) -> dict:
@@ -495,10 +495,10 @@ def autotune_components(field, mask, numberOfControlPoints, ctx: Optional[Contex
     X, Y, Z = (int(d) for d in f.shape)
     check(_lib.load().n4_autotune_components(c.handle, _ptr(f), _ptr(m), *nc, X, Y, Z, _ptr(lat), _ptr(out),
                                              _stream(f.device), C.byref(rep)))
-    fit = [(int(rep.fit_step[k]), int(rep.fit_depth[k]), int(rep.fit_rows[k]), int(rep.fit_prefetch[k]),
-            float(rep.fit_ms[k])) for k in range(rep.fit_candidates)]
+    fit = [(int(rep.fit_step[k]), int(rep.fit_depth[k]), int(rep.fit_rows[k]), float(rep.fit_ms[k]))
+           for k in range(rep.fit_candidates)]
     ev = [(int(rep.eval_rows[k]), int(rep.eval_threads[k]), float(rep.eval_ms[k])) for k in range(rep.eval_candidates)]
-    return {"fit": fit, "fit_chosen": fit[rep.fit_chosen][:4], "evaluate": ev,
+    return {"fit": fit, "fit_chosen": fit[rep.fit_chosen][:3], "evaluate": ev,
             "evaluate_chosen": ev[rep.eval_chosen][:2]}
 
 

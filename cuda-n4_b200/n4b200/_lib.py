@@ -88,15 +88,15 @@ class n4_tune_report_t(C.Structure):
         ("chosen", C.c_int),
         ("corr_candidates", C.c_int), ("corr_rows", C.c_int * N4_TUNE_MAX),
         ("corr_threads", C.c_int * N4_TUNE_MAX), ("corr_ms", C.c_float * N4_TUNE_MAX), ("corr_chosen", C.c_int),
-        ("sub_candidates", C.c_int), ("sub_ms", C.c_float * N4_TUNE_MAX), ("sub_chosen", C.c_int),
+        ("sub_candidates", C.c_int), ("sub_count", C.c_int * N4_TUNE_MAX), ("sub_tapered", C.c_int * N4_TUNE_MAX),
+        ("sub_ms", C.c_float * N4_TUNE_MAX), ("sub_chosen", C.c_int),
     ]
 
 
 class n4_component_tune_t(C.Structure):
     _fields_ = [
         ("fit_candidates", C.c_int), ("fit_step", C.c_int * N4_TUNE_MAX), ("fit_depth", C.c_int * N4_TUNE_MAX),
-        ("fit_rows", C.c_int * N4_TUNE_MAX), ("fit_prefetch", C.c_int * N4_TUNE_MAX),
-        ("fit_ms", C.c_float * N4_TUNE_MAX), ("fit_chosen", C.c_int),
+        ("fit_rows", C.c_int * N4_TUNE_MAX), ("fit_ms", C.c_float * N4_TUNE_MAX), ("fit_chosen", C.c_int),
         ("fit_shape", C.c_int),
         ("eval_candidates", C.c_int), ("eval_rows", C.c_int * N4_TUNE_MAX), ("eval_threads", C.c_int * N4_TUNE_MAX),
         ("eval_ms", C.c_float * N4_TUNE_MAX), ("eval_chosen", C.c_int), ("eval_shape", C.c_int),
@@ -107,7 +107,7 @@ class n4_timings_t(C.Structure):
     _fields_ = [
         ("stage_ms", C.c_float * 4), ("launches", C.c_int), ("fit_voxels", C.c_longlong),
         ("full_voxels", C.c_longlong),
-        ("fit_rows", C.c_int), ("fit_step", C.c_int), ("fit_depth", C.c_int), ("fit_prefetch", C.c_int),
+        ("fit_rows", C.c_int), ("fit_step", C.c_int), ("fit_depth", C.c_int), ("reserved", C.c_int),
         ("correct_rows", C.c_int), ("correct_threads", C.c_int),
     ]
 

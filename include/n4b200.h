@@ -158,10 +158,11 @@ n4_status_t n4_run_host(n4_context_t *ctx, const n4_params_t *p,
 /* Batched host-pointer twin (testN4, cudaN4.h:367-387, corrects one volume
  * per call).  vols[i] holds HOST pointers (im, mask, outputs, optional bias
  * and warm lattice).  The volumes are corrected in sub-batches of `per`
- * (0: the library's choice, 8) through three device staging slots: the
- * upload of one sub-batch, the batched run of the previous one and the
- * download of the one before run on three streams at once, so the host link
- * and the GPU stay busy together.  Host buffers should be page-locked
+ * (0: the library's choice, 8) on four lanes: a lane's stream carries its
+ * sub-batch's uploads into the lane's device staging slot, the batched run
+ * and the downloads, the runs of successive sub-batches follow one another
+ * (one context), and the copies of the other lanes overlap them, so the host
+ * link and the GPU stay busy together.  Host buffers should be page-locked
  * (cudaHostAlloc / cudaHostRegister) for the copies to overlap.  enc: the
  * learned warm start (as n4_run_batched_warm) or NULL.  reports: n entries
  * or NULL.  device_ms (may be NULL): GPU time from the first upload to the
@@ -226,11 +227,14 @@ typedef struct {
   int corr_threads[N4_TUNE_MAX];   /* threads per CTA                        */
   float corr_ms[N4_TUNE_MAX];      /* device time of the correction stage    */
   int corr_chosen;
-  /* overlapped sub-batches 1..sub_candidates on the chosen path and tile
-   * (cluster path, two or more volumes; 0 candidates otherwise) */
+  /* overlapped sub-batches on the chosen path and tile (cluster path, two
+   * or more volumes; 0 candidates otherwise): 1..4 of equal size, then 3
+   * and 4 with the first and last half the size of the others */
   int sub_candidates;
+  int sub_count[N4_TUNE_MAX];      /* sub-batches                            */
+  int sub_tapered[N4_TUNE_MAX];    /* 1: half-size first and last            */
   float sub_ms[N4_TUNE_MAX];       /* device time of one run                 */
-  int sub_chosen;                  /* sub-batches recorded (0: default rule) */
+  int sub_chosen;                  /* index of the candidate recorded        */
 } n4_tune_report_t;
 
 n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *params, int n,
@@ -251,7 +255,7 @@ typedef struct {
   long long fit_voxels;    /* fitting-grid voxels of the call             */
   long long full_voxels;   /* full-resolution voxels of the call          */
   int fit_rows, fit_step;  /* z-contraction shape of a fit call (-1: none) */
-  int fit_depth, fit_prefetch;
+  int fit_depth, reserved;
   int correct_rows, correct_threads;   /* correction tile (-1: none)      */
 } n4_timings_t;
 
@@ -306,7 +310,6 @@ typedef struct {
   int fit_step[N4_TUNE_MAX];       /* voxels per load step (0: staged kernel) */
   int fit_depth[N4_TUNE_MAX];      /* load steps in flight per thread         */
   int fit_rows[N4_TUNE_MAX];       /* field rows per CTA                      */
-  int fit_prefetch[N4_TUNE_MAX];   /* 1: the CTA's rows requested into L2 first */
   float fit_ms[N4_TUNE_MAX];       /* z contraction, L2 evicted               */
   int fit_chosen, fit_shape;       /* candidate index, library shape index    */
   int eval_candidates;

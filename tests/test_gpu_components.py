@@ -167,14 +167,14 @@ def test_component_autotuner_records_and_reuses_tile_shapes(cuda):
     t = n4b200.autotune_components(f, m, nc, ctx=ctx)
     assert len(t["fit"]) >= 8 and len(t["evaluate"]) >= 4
     assert all(ms > 0 for *_, ms in t["fit"]) and all(ms > 0 for *_, ms in t["evaluate"])
-    assert t["fit_chosen"] == min(t["fit"], key=lambda c: c[4])[:4]
+    assert t["fit_chosen"] == min(t["fit"], key=lambda c: c[3])[:3]
     assert t["evaluate_chosen"] == min(t["evaluate"], key=lambda c: c[2])[:2]
     ctx.set_profiling(True)
     lat1 = n4b200.FitBspline3D(f, m, nc, ctx=ctx)
     tf = ctx.last_timings()
     ev1 = n4b200.EvaluateBspline3D(lat1, nc, shape, ctx=ctx)
     te = ctx.last_timings()
-    assert (tf["fit_step"], tf["fit_depth"], tf["fit_rows"], tf["fit_prefetch"]) == t["fit_chosen"]
+    assert (tf["fit_step"], tf["fit_depth"], tf["fit_rows"]) == t["fit_chosen"]
     assert (te["correct_rows"], te["correct_threads"]) == t["evaluate_chosen"]
     assert cuda.equal(lat0, lat1) and cuda.equal(ev0, ev1)
     # a different field size: the default shapes

@@ -31,7 +31,7 @@ def test_host_batch_matches_device_batches(cuda, u8):
     vols = _vols(cuda, shapes, 700, u8)
     p = n4b200.N4Param(NumberOfFittingLevels=3, MaximumNumberOfIterations=20, ConvergenceThreshold=0.001,
                        low_value=0.0, ShrinkFactor=4)
-    per = 2   # 4 sub-batches (the last of one volume) over 3 staging slots
+    per = 1   # 7 sub-batches over the 4 lanes: every lane's staging slot is reused
     res, ms = n4b200.N4BatchHost(vols, p, per=per, return_bias=True, ctx=n4b200.Context())
     assert ms > 0
     ctx = n4b200.Context()

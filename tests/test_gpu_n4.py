@@ -351,8 +351,9 @@ def test_autotune_records_the_fastest_configuration(cuda):
     assert len(corr) >= 4 and all(ms > 0 for _, _, ms in corr)
     assert t["correction_chosen"] == min(corr, key=lambda c: c[2])[:2]
     subs = t["sub_batches_ms"]
-    assert len(subs) == 4 and all(ms > 0 for ms in subs)
-    assert t["sub_batches_chosen"] == 1 + min(range(4), key=lambda k: subs[k])
+    assert [(s, tp) for s, tp, _ in subs] == [(1, False), (2, False), (3, False), (4, False), (3, True), (4, True)]
+    assert all(ms > 0 for *_, ms in subs)
+    assert t["sub_batches_chosen"] == min(subs, key=lambda c: c[2])[:2]
     ctx.set_profiling(True)
     again = n4b200.N4Batch(vols, p, ctx=ctx)
     tm = ctx.last_timings()
