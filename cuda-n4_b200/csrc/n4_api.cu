@@ -290,17 +290,18 @@ Plan make_plan(const n4_params_t *p, int K, const std::vector<Dims> &vols, bool 
   pl.o_H = take((size_t)pl.bins * 8);
   pl.o_E = take((size_t)pl.bins * 8);
   pl.o_tw = take((size_t)pl.npad * 16);
-  pl.o_ff = take((size_t)pl.npad * 8);
+  pl.o_ff = grid ? take((size_t)pl.npad * 8) : 0;   // cluster: in the Gd region
   pl.o_red = take(160 * 8);
   pl.o_misc = take(64);
   pl.sm_bytes = (int)align_up(o, 128);
   o = 0;
-  if (!grid) pl.b_imlog = take(((size_t)pl.slab_floats + 8) * 4);
-  pl.b_G = take((size_t)pl.rows_max * pl.NCZ * 4);
+  pl.b_imlog = take(((size_t)pl.slab_floats + 8) * 4);   // logU (cluster: the staged rows first)
   pl.a_fa = 0;
   pl.a_fb = (int)fft_bytes;
   pl.a_hist = (int)(2 * fft_bytes);
-  pl.b_Gd = take(std::max((size_t)pl.rows_max * pl.NCZ * 4, grid ? 0 : 2 * fft_bytes + hist_bytes));
+  pl.a_ff = pl.a_hist;   // written by the sharpening after the histogram copies are merged
+  const size_t ff_bytes = (size_t)pl.npad * 8;
+  pl.b_Gd = take(std::max((size_t)pl.rows_max * pl.NCZ * 4, grid ? 0 : 2 * fft_bytes + std::max(hist_bytes, ff_bytes)));
   pl.b_T2 = take((size_t)pl.nvxl * pl.NCY * pl.NCZ * 4);
   pl.b_slotA = take(sizeof(Stats));
   pl.b_slotB = take((size_t)pl.bins * 8);
@@ -741,6 +742,10 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
   } else {
     for (int k = 0; k <= P.nsub; ++k) P.sub_lo[k] = (int)((long long)n * k / P.nsub);
   }
+  // a split of few volumes can leave a sub-batch empty (4 volumes tapered
+  // over 4: 0,0,2,3,4); drop it, no launch may see an empty sub-batch
+  P.sub_lo.erase(std::unique(P.sub_lo.begin(), P.sub_lo.end()), P.sub_lo.end());
+  P.nsub = (int)P.sub_lo.size() - 1;
   // workspaces
   P.NCX = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
   P.NCY = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);

@@ -8,17 +8,23 @@
 // memory; a bounded software barrier).  The algorithm below is written once
 // for both.
 //
-// Per level, with L the control lattice and G/Gd the per-row partial
-// evaluations of L and of the last update D:
-//   pass A  logU = im_log - eval(G), masked min/max, and the convergence
-//           value of the previous update from eval(Gd)       (group reduce)
+// Per level, with L the control lattice, D its last update and Gd = rows(D)
+// the per-row partial evaluation of D (x/y contracted, one value per z
+// control point), the slab holds logU, one float per fitting voxel:
+//   reset   logU = im_log - eval(rows(L))    (level start, warm-start trial)
+//   pass A  logU -= eval(Gd): the previous update applied, its convergence
+//           value, masked min/max of logU                   (group reduce)
 //   pass B  fractional histogram of logU                        (group reduce)
 //           Wiener sharpening map E (every CTA, in shared memory)
 //   pass C  residual R = logU - remap(logU)
 //   fit     separable contraction of R with the fit weights     (group reduce)
-//   update  D = num / (den + eps), L += D, G = rows(L), Gd = rows(D)
+//   update  D = num / (den + eps), L += D, Gd = rows(D)
+// logU follows L by the same updates, applied per voxel: eval is linear, so
+// logU = im_log - eval(rows(L)) up to FP32 rounding, which the reset at every
+// level start clears.
 #pragma once
 #include <cooperative_groups.h>
+#include <new>
 #include <type_traits>
 
 #include "n4_device.cuh"
@@ -59,10 +65,12 @@ struct Plan {
   int o_fa, o_fb, o_tw, o_ff, o_red, o_misc;
   int sm_bytes;
   // big
-  int b_imlog, b_G, b_Gd, b_T2, b_slotA, b_slotB, b_slotC, b_slice, big_bytes;
-  // cluster path: the FFT work buffers and the histogram copies live in the
-  // Gd region (dead from the end of pass A until the update) at these offsets
-  int alias_sharpen, a_fa, a_fb, a_hist;
+  int b_imlog, b_Gd, b_T2, b_slotA, b_slotB, b_slotC, b_slice, big_bytes;
+  // cluster path: the FFT work buffers, the histogram copies and the
+  // Gaussian's transform (which the sharpening writes after the copies are
+  // merged, over them) live in the Gd region, dead from the end of pass A
+  // until the update, at these offsets
+  int alias_sharpen, a_fa, a_fb, a_hist, a_ff;
 };
 
 struct Params {
@@ -113,14 +121,16 @@ struct GridGroup {
 
 // ------------------------------------------------------------------ phase timers
 // Compile with -DN4_PHASE_TIMERS to print, per volume, the cycles thread 0
-// of the first CTA spends between phase marks (measurement builds only).
+// of the first CTA spends between phase marks (measurement builds only).  The
+// counters live in shared memory, so that the timed build allocates the
+// kernel's registers as the product build does.
 #ifdef N4_PHASE_TIMERS
 #define N4_MARK(k)                                                     \
   do {                                                                 \
     if (threadIdx.x == 0) {                                            \
       const long long t_ = clock64();                                  \
-      ph_acc[k] += t_ - ph_last;                                       \
-      ph_last = t_;                                                    \
+      ph_acc[k] += t_ - ph_acc[PH_N];                                  \
+      ph_acc[PH_N] = t_;                                               \
     }                                                                  \
   } while (0)
 #else
@@ -128,15 +138,27 @@ struct GridGroup {
 #endif
 enum { PH_SETUP, PH_A, PH_B, PH_SHARP, PH_C, PH_FIT, PH_UPDATE, PH_A_LOOP, PH_A_RED, PH_B_ZERO, PH_B_LOOP, PH_B_MERGE,
        PH_B_RED, PH_F_T1, PH_F_T2, PH_F_P, PH_F_RED, PH_N };
+#ifdef N4_PHASE_TIMERS
+__shared__ long long ph_acc[PH_N + 1];   // per-phase cycles, then the last mark
+#endif
 
 // ------------------------------------------------------------------ engine
+// The Engine's fields are uniform over the CTA.  Whole-GPU path: one object
+// per CTA in shared memory (EngineSlot), its fields written by thread 0 only
+// (construction, run, set_level, each followed by a barrier); held in
+// registers, the ~50 fields (pointers of the axis tables and work arrays)
+// stay live through every pass and push the voxel loops into local-memory
+// spills (measured: 512x512x320 in 6.2 ms instead of 6.5).  Cluster path: one
+// object per thread, every thread writing its own copy (measured: the shared
+// object made the 256x256x176 batch 11 % slower, its loops reloading fields
+// after every shared-memory store or atomic).
 template <class Group>
 struct Engine {
   static constexpr int kRB = RowBatch<Group::kGrid>::n;
-#ifdef N4_PHASE_TIMERS
-  long long ph_acc[PH_N] = {};
-  long long ph_last = 0;
-#endif
+  static constexpr bool kShared = Group::kGrid;   // the object lives in shared memory
+  // the threads that write the fields, and the barrier that publishes them
+  __device__ __forceinline__ bool writer() const { return !kShared || threadIdx.x == 0; }
+  __device__ __forceinline__ void publish() const { if (kShared) __syncthreads(); }
   Group g;
   const Plan &pl;
   const Params &pr;
@@ -150,7 +172,8 @@ struct Engine {
   int r0, nplane;
   int hshift;   // fixed-point scale of this volume's histogram
   FastDiv divZ;
-  const float *imlog;
+  float *logu;         // [nrow][Z] logU of the local rows (NaN outside the mask)
+  const float *src;    // the job's log volume (global memory), read by reset
   // level
   int ncx, ncy, ncz, nlat;
   Axis ax, ay, az;
@@ -161,7 +184,7 @@ struct Engine {
   unsigned long long *H64;
   double2 *fa, *fb, *tw;
   double *red;
-  float *G, *Gd, *T2, *slotC;
+  float *Gd, *T2, *slotC;
   Stats *slotA;
   unsigned long long *slotB;
 
@@ -173,10 +196,12 @@ struct Engine {
     H = (double *)(sm + pl.o_H); E = (double *)(sm + pl.o_E);
     fa = (double2 *)(sm + pl.o_fa); fb = (double2 *)(sm + pl.o_fb); tw = (double2 *)(sm + pl.o_tw);
     Ff = (double *)(sm + pl.o_ff); red = (double *)(sm + pl.o_red);
-    G = (float *)(big + pl.b_G); Gd = (float *)(big + pl.b_Gd); T2 = (float *)(big + pl.b_T2);
+    Gd = (float *)(big + pl.b_Gd); T2 = (float *)(big + pl.b_T2);
+    logu = (float *)(big + pl.b_imlog);
     if (pl.alias_sharpen) {
       fa = (double2 *)(big + pl.b_Gd + pl.a_fa); fb = (double2 *)(big + pl.b_Gd + pl.a_fb);
       hist = (unsigned *)(big + pl.b_Gd + pl.a_hist);
+      Ff = (double *)(big + pl.b_Gd + pl.a_ff);
     }
     slotA = (Stats *)(big + pl.b_slotA); slotB = (unsigned long long *)(big + pl.b_slotB);
     slotC = (float *)(big + pl.b_slotC);
@@ -184,13 +209,16 @@ struct Engine {
 
   // ---- level geometry
   __device__ void set_level(int level) {
-    ncx = ((pl.nc0x - 3) << level) + 3;
-    ncy = ((pl.nc0y - 3) << level) + 3;
-    ncz = ((pl.nc0z - 3) << level) + 3;
-    nlat = ncx * ncy * ncz;
-    ax = axis_at(sm + pl.o_ax, X, ncx);
-    ay = axis_at(sm + pl.o_ay, Y, ncy);
-    az = axis_at(sm + pl.o_az, Z, ncz);
+    if (writer()) {
+      ncx = ((pl.nc0x - 3) << level) + 3;
+      ncy = ((pl.nc0y - 3) << level) + 3;
+      ncz = ((pl.nc0z - 3) << level) + 3;
+      nlat = ncx * ncy * ncz;
+      ax = axis_at(sm + pl.o_ax, X, ncx);
+      ay = axis_at(sm + pl.o_ay, Y, ncy);
+      az = axis_at(sm + pl.o_az, Z, ncz);
+    }
+    publish();
     build_axis(ax);
     build_axis(ay);
     build_axis(az);
@@ -241,27 +269,26 @@ struct Engine {
   }
   __device__ __forceinline__ int plane_vx(int m) const { return Group::kGrid ? r0 / Y + m : rank + m * K; }
 
-  // rowtab(la, Ga) and rowtab(lb, Gb) after a lattice update, through the
-  // x-contracted planes: per local x-plane, X[cy][cz] = sum_jx wx L[sx+jx][cy][cz]
-  // (into tmp for la, aux for lb, both free outside the warm-start trial),
-  // then per row G[cz] = sum_jy wy X[sy+jy][cz]: 8 loads and multiply-adds
-  // per entry instead of 32.  Falls back to rowtab2_direct when the planes'
-  // slices do not fit in a lattice-sized buffer.  The caller synchronises.
-  __device__ void rowtab2(const float *la, float *Ga, const float *lb, float *Gb) {
+  // rowtab(lat, Gt) after a lattice update, through the x-contracted planes:
+  // per local x-plane, X[cy][cz] = sum_jx wx lat[sx+jx][cy][cz] (into aux,
+  // free outside the warm-start trial), then per row Gt[cz] = sum_jy wy
+  // X[sy+jy][cz]: 8 loads and multiply-adds per entry instead of 32.  Falls
+  // back to rowtab when the planes' slices do not fit in a lattice-sized
+  // buffer.  The caller synchronises.
+  __device__ void rowtab_planes(const float *lat, float *Gt) {
     const int np = nplanes_local(), slice = ncy * ncz;
-    if ((long long)np * slice > pl.NLAT) { rowtab2_direct(la, Ga, lb, Gb); return; }
-    float *Xa = tmp, *Xb = aux;
+    if ((long long)np * slice > pl.NLAT) { rowtab(lat, Gt); return; }
+    float *Xp = aux;
     for (int t = threadIdx.x; t < np * slice; t += blockDim.x) {
       const int m = t / slice, c = t - m * slice;
       const int vx = plane_vx(m);
       const int sx = ax.s[vx];
       const float4 wx = ax.w[vx];
-      const float *pa = la + (size_t)sx * slice + c, *pb = lb + (size_t)sx * slice + c;
-      float a = __fmul_rn(wx.x, pa[0]), b = __fmul_rn(wx.x, pb[0]);
-      a = __fmaf_rn(wx.y, pa[slice], a); b = __fmaf_rn(wx.y, pb[slice], b);
-      a = __fmaf_rn(wx.z, pa[2 * slice], a); b = __fmaf_rn(wx.z, pb[2 * slice], b);
-      Xa[t] = __fmaf_rn(wx.w, pa[3 * slice], a);
-      Xb[t] = __fmaf_rn(wx.w, pb[3 * slice], b);
+      const float *pa = lat + (size_t)sx * slice + c;
+      float a = __fmul_rn(wx.x, pa[0]);
+      a = __fmaf_rn(wx.y, pa[slice], a);
+      a = __fmaf_rn(wx.z, pa[2 * slice], a);
+      Xp[t] = __fmaf_rn(wx.w, pa[3 * slice], a);
     }
     __syncthreads();
     const int vx0 = Group::kGrid ? r0 / Y : 0;
@@ -272,43 +299,37 @@ struct Engine {
       const int m = Group::kGrid ? vx - vx0 : rl / Y;
       const int sy = ay.s[vy];
       const float4 wy = ay.w[vy];
-      const float *xa = Xa + m * slice + sy * ncz + cz, *xb = Xb + m * slice + sy * ncz + cz;
-      float a = __fmul_rn(wy.x, xa[0]), b = __fmul_rn(wy.x, xb[0]);
-      a = __fmaf_rn(wy.y, xa[ncz], a); b = __fmaf_rn(wy.y, xb[ncz], b);
-      a = __fmaf_rn(wy.z, xa[2 * ncz], a); b = __fmaf_rn(wy.z, xb[2 * ncz], b);
-      Ga[t] = __fmaf_rn(wy.w, xa[3 * ncz], a);
-      Gb[t] = __fmaf_rn(wy.w, xb[3 * ncz], b);
+      const float *xa = Xp + m * slice + sy * ncz + cz;
+      float a = __fmul_rn(wy.x, xa[0]);
+      a = __fmaf_rn(wy.y, xa[ncz], a);
+      a = __fmaf_rn(wy.z, xa[2 * ncz], a);
+      Gt[t] = __fmaf_rn(wy.w, xa[3 * ncz], a);
     }
   }
 
-  // rowtab(la, Ga) and rowtab(lb, Gb) in one sweep (the same operations per
-  // entry; the row's spans and weights are read once for both)
-  __device__ void rowtab2_direct(const float *la, float *Ga, const float *lb, float *Gb) {
-    const int ntask = nrow * ncz;
-    for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
-      const int rl = t / ncz, cz = t - rl * ncz;
-      int vx, vy;
-      row_xy(rl, vx, vy);
-      const int sx = ax.s[vx], sy = ay.s[vy];
-      const float4 wx = ax.w[vx], wy = ay.w[vy];
-      const float wxa[4] = {wx.x, wx.y, wx.z, wx.w};
-      const float wya[4] = {wy.x, wy.y, wy.z, wy.w};
-      float acca = 0.0f, accb = 0.0f;
-#pragma unroll
-      for (int jx = 0; jx < 4; ++jx) {
-        const int o = ((sx + jx) * ncy + sy) * ncz + cz;
-        float sa = 0.0f, sb = 0.0f;
-#pragma unroll
-        for (int jy = 0; jy < 4; ++jy) {
-          sa = __fmaf_rn(wya[jy], la[o + jy * ncz], sa);
-          sb = __fmaf_rn(wya[jy], lb[o + jy * ncz], sb);
-        }
-        acca = __fmaf_rn(wxa[jx], sa, acca);
-        accb = __fmaf_rn(wxa[jx], sb, accb);
-      }
-      Ga[t] = acca;
-      Gb[t] = accb;
+  // First voxel of local row rl in the job's log volume: grid, contiguous
+  // rows r0 + rl; cluster, plane vx = rank + m*K, row vy of it
+  __device__ __forceinline__ const float *src_row(int rl) const {
+    if (Group::kGrid) return src + (size_t)(r0 + rl) * Z;
+    const int m = rl / Y;
+    return src + ((size_t)(rank + m * K) * Y + (rl - m * Y)) * Z;
+  }
+
+  // logU = im_log - eval(rows(lat)) for every local voxel, im_log read from
+  // the slab itself when `staged` (the cluster kernel's bulk copy of the
+  // volume, before the first reset), else from the job's log volume in
+  // global memory; rows(lat) goes through the Gd region (free at every
+  // reset: level start, warm-start trial).
+  __device__ void reset(const float *lat, bool staged = false) {
+    rowtab(lat, Gd);
+    __syncthreads();
+    const int n = nrow * Z;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
+      const float v = staged ? logu[i] : src_row(rl)[vz];
+      logu[i] = isnan(v) ? v : __fsub_rn(v, eval(Gd, rl, vz));
     }
+    __syncthreads();
   }
 
   __device__ __forceinline__ float eval(const float *Gt, int rl, int vz) const {
@@ -423,22 +444,12 @@ struct Engine {
         const int lo = az.lo[sp], hi = az.hi[sp];
         float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
         if (num_mode) {
-          // residual R = logU - E(logU) of each masked voxel, with logU =
-          // im_log - eval(G) recomputed exactly as pass A computes it (every
-          // voxel of span sp evaluates the same 4 entries of its row of G)
-          const float *iv = imlog + (size_t)rl * Z;
-          const float *gr = G + rl * ncz + sp;
-          const float g0 = gr[0], g1 = gr[1], g2 = gr[2], g3 = gr[3];
+          // residual R = logU - E(logU) of each masked voxel
+          const float *iv = logu + (size_t)rl * Z;
           if constexpr (kRB == 1) {
             for (int vz = lo; vz < hi; ++vz) {
-              const float v = iv[vz];
-              if (isnan(v)) continue;
-              const float4 we = az.w[vz];
-              float b = __fmul_rn(we.x, g0);
-              b = __fmaf_rn(we.y, g1, b);
-              b = __fmaf_rn(we.z, g2, b);
-              b = __fmaf_rn(we.w, g3, b);
-              const float lu = __fsub_rn(v, b);
+              const float lu = iv[vz];
+              if (isnan(lu)) continue;
               const float r = degenerate ? 0.0f : (float)((double)lu - sharpened_value(bm->coord(lu), E, pr.bins));
               const float4 w = W4[vz];
               a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
@@ -455,12 +466,7 @@ struct Engine {
             for (int u = 0; u < kRB; ++u) {
               if (isnan(v[u])) continue;
               const int vz = vb + u;
-              const float4 we = az.w[vz];
-              float b = __fmul_rn(we.x, g0);
-              b = __fmaf_rn(we.y, g1, b);
-              b = __fmaf_rn(we.z, g2, b);
-              b = __fmaf_rn(we.w, g3, b);
-              const float lu = __fsub_rn(v[u], b);
+              const float lu = v[u];
               const float r = degenerate ? 0.0f : (float)((double)lu - sharpened_value(bm->coord(lu), E, pr.bins));
               const float4 w = W4[vz];
               a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
@@ -468,7 +474,7 @@ struct Engine {
             }
           }
         } else {
-          const float *iv = imlog + (size_t)rl * Z;
+          const float *iv = logu + (size_t)rl * Z;
           if constexpr (kRB == 1) {
             for (int vz = lo; vz < hi; ++vz) {
               if (isnan(iv[vz])) continue;
@@ -574,9 +580,10 @@ struct Engine {
     }
   }
 
-  // ---- pass A: logU = im_log - eval(G) (not stored: the passes that need it
-  // recompute it bitwise), masked min/max and the previous update's CV sums
-  __device__ bool pass_a(bool need_cv, double st[4]) {
+  // ---- pass A: the previous update's convergence sums from eval(Gd) (when
+  // need_cv), applied to logU (when apply: logU -= eval(Gd)), and the masked
+  // min/max of logU
+  __device__ bool pass_a(bool need_cv, bool apply, double st[4]) {
     float vmin = INFINITY, vmax = -INFINITY;
     double sy = 0.0, syy = 0.0;
     const int per = (int)blockDim.x / Z;   // whole rows per sweep: each thread keeps one z
@@ -587,62 +594,72 @@ struct Engine {
         const int sz = az.s[vz];
         if constexpr (kRB == 1) {
           for (int rl = rs; rl < nrow; rl += per) {
-            const float v = imlog[rl * Z + vz];
-            if (isnan(v)) continue;   // outside the mask
-            const float lu = __fsub_rn(v, dot4(w, G + rl * ncz + sz));
-            vmin = fminf(vmin, lu);
-            vmax = fmaxf(vmax, lu);
+            float lu = logu[rl * Z + vz];
+            if (isnan(lu)) continue;   // outside the mask
             if (need_cv) {
-              const float y = expm1f(-dot4(w, Gd + rl * ncz + sz));
+              const float ed = dot4(w, Gd + rl * ncz + sz);
+              const float y = expm1f(-ed);
               sy += (double)y;
               syy += (double)y * (double)y;
+              if (apply) {
+                lu = __fsub_rn(lu, ed);
+                logu[rl * Z + vz] = lu;
+              }
             }
+            vmin = fminf(vmin, lu);
+            vmax = fmaxf(vmax, lu);
           }
         } else
         // kRB rows at a time: their loads are all issued before the
         // first of them is used; the values are then taken in row order
         for (int rb = rs; rb < nrow; rb += kRB * per) {
-          float v[kRB], ev[kRB], evd[kRB];
+          float v[kRB], evd[kRB];
 #pragma unroll
           for (int u = 0; u < kRB; ++u) {
             const int rl = rb + u * per;
-            v[u] = rl < nrow ? imlog[rl * Z + vz] : kNaN;
+            v[u] = rl < nrow ? logu[rl * Z + vz] : kNaN;
           }
 #pragma unroll
           for (int u = 0; u < kRB; ++u) {
             const int rl = rb + u * per;
-            const bool in = !isnan(v[u]);
-            ev[u] = in ? dot4(w, G + rl * ncz + sz) : 0.0f;
-            evd[u] = (in && need_cv) ? dot4(w, Gd + rl * ncz + sz) : 0.0f;
+            evd[u] = (!isnan(v[u]) && need_cv) ? dot4(w, Gd + rl * ncz + sz) : 0.0f;
           }
 #pragma unroll
           for (int u = 0; u < kRB; ++u) {
             if (isnan(v[u])) continue;   // outside the mask
-            const float lu = __fsub_rn(v[u], ev[u]);
-            vmin = fminf(vmin, lu);
-            vmax = fmaxf(vmax, lu);
+            float lu = v[u];
             if (need_cv) {
               const float y = expm1f(-evd[u]);
               sy += (double)y;
               syy += (double)y * (double)y;
+              if (apply) {
+                lu = __fsub_rn(lu, evd[u]);
+                logu[(rb + u * per) * Z + vz] = lu;
+              }
             }
+            vmin = fminf(vmin, lu);
+            vmax = fmaxf(vmax, lu);
           }
         }
       }
     } else {
       const int n = nrow * Z;
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const float v = imlog[i];
-        if (isnan(v)) continue;
-        const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
-        const float lu = __fsub_rn(v, eval(G, rl, vz));
-        vmin = fminf(vmin, lu);
-        vmax = fmaxf(vmax, lu);
+        float lu = logu[i];
+        if (isnan(lu)) continue;
         if (need_cv) {
-          const float y = expm1f(-eval(Gd, rl, vz));
+          const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
+          const float ed = eval(Gd, rl, vz);
+          const float y = expm1f(-ed);
           sy += (double)y;
           syy += (double)y * (double)y;
+          if (apply) {
+            lu = __fsub_rn(lu, ed);
+            logu[i] = lu;
+          }
         }
+        vmin = fminf(vmin, lu);
+        vmax = fmaxf(vmax, lu);
       }
     }
     double loc[4];
@@ -665,72 +682,39 @@ struct Engine {
     __syncthreads();
     N4_MARK(PH_B_ZERO);
     unsigned *hc = hist + ((threadIdx.x >> 5) % kHistCopies) * bins;
-    const int per = (int)blockDim.x / Z;   // whole rows per sweep, as in pass A
-    if (per > 0) {
-      const int rs = (int)threadIdx.x / Z, vz = (int)threadIdx.x - rs * Z;
-      const float4 w = rs < per ? az.w[vz] : make_float4(0.f, 0.f, 0.f, 0.f);
-      const int sz = rs < per ? az.s[vz] : 0;
-      if constexpr (kRB == 1) {
-        const int sweeps = (nrow + per - 1) / per;
-        for (int k = 0; k < sweeps; ++k) {
-          const int rl = rs + k * per;
-          int key = -1;
-          unsigned qlo = 0, qhi = 0;
-          if (rs < per && rl < nrow) {
-            const float v = imlog[rl * Z + vz];
-            if (!isnan(v)) {
-              const float lu = __fsub_rn(v, dot4(w, G + rl * ncz + sz));
-              key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
-            }
-          }
-          if (key >= 0) {
-            atomicAdd(&hc[key], qlo);
-            if (qhi) atomicAdd(&hc[key + 1], qhi);
-          }
-        }
-      } else if (rs < per) {
-        // kRB rows at a time, loads first (as in pass A)
-        for (int rb = rs; rb < nrow; rb += kRB * per) {
-          float v[kRB], ev[kRB];
-#pragma unroll
-          for (int u = 0; u < kRB; ++u) {
-            const int rl = rb + u * per;
-            v[u] = rl < nrow ? imlog[rl * Z + vz] : kNaN;
-          }
-#pragma unroll
-          for (int u = 0; u < kRB; ++u) {
-            const int rl = rb + u * per;
-            ev[u] = !isnan(v[u]) ? dot4(w, G + rl * ncz + sz) : 0.0f;
-          }
-#pragma unroll
-          for (int u = 0; u < kRB; ++u) {
-            if (isnan(v[u])) continue;
-            unsigned qlo = 0, qhi = 0;
-            const int key = hist_bin(bm.coord(__fsub_rn(v[u], ev[u])), bins, scale, qlo, qhi);
-            if (key >= 0) {
-              atomicAdd(&hc[key], qlo);
-              if (qhi) atomicAdd(&hc[key + 1], qhi);
-            }
-          }
-        }
-      }
-    } else {
-      const int n = nrow * Z;
+    const int n = nrow * Z;   // the local voxels in order: lanes take consecutive voxels
+    if constexpr (kRB == 1) {
       for (int base = 0; base < n; base += blockDim.x) {
         const int i = base + threadIdx.x;
         int key = -1;
         unsigned qlo = 0, qhi = 0;
         if (i < n) {
-          const float v = imlog[i];
-          if (!isnan(v)) {
-            const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
-            const float lu = __fsub_rn(v, eval(G, rl, vz));
-            key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
-          }
+          const float lu = logu[i];
+          if (!isnan(lu)) key = hist_bin(bm.coord(lu), bins, scale, qlo, qhi);
         }
         if (key >= 0) {
           atomicAdd(&hc[key], qlo);
           if (qhi) atomicAdd(&hc[key + 1], qhi);
+        }
+      }
+    } else {
+      // kRB voxels per thread at a time, their loads issued first
+      for (int base = 0; base < n; base += kRB * blockDim.x) {
+        float v[kRB];
+#pragma unroll
+        for (int u = 0; u < kRB; ++u) {
+          const int i = base + u * (int)blockDim.x + (int)threadIdx.x;
+          v[u] = i < n ? logu[i] : kNaN;
+        }
+#pragma unroll
+        for (int u = 0; u < kRB; ++u) {
+          if (isnan(v[u])) continue;
+          unsigned qlo = 0, qhi = 0;
+          const int key = hist_bin(bm.coord(v[u]), bins, scale, qlo, qhi);
+          if (key >= 0) {
+            atomicAdd(&hc[key], qlo);
+            if (qhi) atomicAdd(&hc[key + 1], qhi);
+          }
         }
       }
     }
@@ -755,7 +739,7 @@ struct Engine {
     return true;
   }
 
-  // ---- one sharpen + fit step from the current G; leaves the update in D
+  // ---- one sharpen + fit step from the current logU; leaves the update in D
   __device__ bool fit_step(const double st[4]) {
     // bin range of the masked logU (N4.py:14-15); st holds FP32 values
     const double bmin = st[0], bmax = st[1];
@@ -784,34 +768,45 @@ struct Engine {
     return (float)(sqrt(var > 0.0 ? var : 0.0) / (1.0 + mean_y));
   }
 
-  // ---- the whole volume
-  __device__ void run(const VolJob &job, const float *imlog_in) {
-    X = job.X; Y = job.Y; Z = job.Z;
-    rank = g.rank(); K = g.size();
-    if constexpr (Group::kGrid) {  // contiguous rows: the volume lives in global memory
-      r0 = (int)((long long)X * Y * rank / K);
-      nrow = (int)((long long)X * Y * (rank + 1) / K) - r0;
-      nplane = 0;
-    } else {                       // interleaved planes: every CTA samples the whole volume
-      r0 = 0;
-      nplane = X > rank ? (X - rank + K - 1) / K : 0;
-      nrow = nplane * Y;
+  // ---- the whole volume (logU of the local rows in the big region's slab;
+  // im_log read from job.imlog; cluster path: the slab holds the local rows
+  // of im_log on entry)
+  __device__ void run(const VolJob &job) {
+    if (writer()) {
+      X = job.X; Y = job.Y; Z = job.Z;
+      rank = g.rank(); K = g.size();
+      if constexpr (Group::kGrid) {  // contiguous rows: the volume lives in global memory
+        r0 = (int)((long long)X * Y * rank / K);
+        nrow = (int)((long long)X * Y * (rank + 1) / K) - r0;
+        nplane = 0;
+      } else {                       // interleaved planes: every CTA samples the whole volume
+        r0 = 0;
+        nplane = X > rank ? (X - rank + K - 1) / K : 0;
+        nrow = nplane * Y;
+      }
+      divZ = FastDiv((unsigned)Z);
+      hshift = volume_hist_shift(X, Y, Z, K, Group::kGrid);
+      src = job.imlog;
     }
-    divZ = FastDiv((unsigned)Z);
-    hshift = volume_hist_shift(X, Y, Z, K, Group::kGrid);
-    imlog = imlog_in;
+    publish();
     const bool lead = (rank == 0 && threadIdx.x == 0);
     n4_report_t *rep = job.report;
     if (lead) { rep->device_begin_ns = global_ns(); rep->device_end_ns = 0; rep->sm = sm_id(); }
 
 #ifdef N4_PHASE_TIMERS
-    if (threadIdx.x == 0) ph_last = clock64();
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < PH_N; ++k) ph_acc[k] = 0;
+      ph_acc[PH_N] = clock64();
+    }
 #endif
     fft_twiddles(tw, pl.npad);
     // foreground count of the group
     float cnt = 0.0f;
     double cntd = 0.0;
-    for (int i = threadIdx.x; i < nrow * Z; i += blockDim.x) cnt += isnan(imlog[i]) ? 0.0f : 1.0f;
+    for (int i = threadIdx.x; i < nrow * Z; i += blockDim.x) {
+      const int rl = (int)divZ.div((unsigned)i);
+      cnt += isnan(Group::kGrid ? src_row(rl)[i - rl * Z] : logu[i]) ? 0.0f : 1.0f;   // cluster: staged
+    }
     cntd = cnt;
     double loc[4], st[4];
     block_reduce4(0.0f, 0.0f, cntd, 0.0, red + 8, loc);
@@ -844,33 +839,29 @@ struct Engine {
         for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] = tmp[c];
         __syncthreads();
       }
-      // constant denominator of the fit at this level
+      // logU of this level's lattice, then the constant denominator of the fit
+      reset(L, level == 0 && !Group::kGrid);
       contract(false);
       if (!allreduce(slotC, den, nlat)) goto timeout;
-      rowtab(L, G);
-      __syncthreads();
       const int maxIt = pr.iters[level];
       int it = 0;
       float cv = 1e10f;
       if (level == 0 && job.warm && maxIt > 0) {
         // warm start: one iteration from the warm lattice and one from zero;
-        // keep the one whose first convergence value is not larger
-        for (int c = threadIdx.x; c < nlat; c += blockDim.x) aux[c] = L[c];   // warm
-        __syncthreads();
+        // keep the one whose first convergence value is not larger.  Each
+        // arm starts from a reset and leaves logU one update (D, in Gd)
+        // behind L, as the main loop expects after an iteration.
         float cvs[2];
         for (int arm = 0; arm < 2; ++arm) {
-          for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] = arm == 0 ? aux[c] : 0.0f;
+          for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] = arm == 0 ? job.warm[c] : 0.0f;
           __syncthreads();
-          rowtab(L, G);
-          __syncthreads();
-          if (!pass_a(false, st)) goto timeout;
+          if (arm == 1) reset(L);   // arm 0 starts from the level's reset (L = warm)
+          if (!pass_a(false, false, st)) goto timeout;
           if (!fit_step(st)) goto timeout;
           rowtab(D, Gd);
           for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] += D[c];
           __syncthreads();
-          rowtab(L, G);
-          __syncthreads();
-          if (!pass_a(true, st)) goto timeout;
+          if (!pass_a(true, false, st)) goto timeout;   // the update's CV; logU not advanced
           cvs[arm] = cv_from(st, nfg);
           if (arm == 0) {   // keep the warm result in aux, its update in tmp
             for (int c = threadIdx.x; c < nlat; c += blockDim.x) { aux[c] = L[c]; tmp[c] = D[c]; }
@@ -879,9 +870,11 @@ struct Engine {
         }
         const bool use_warm = cvs[0] <= cvs[1];
         if (use_warm) {
+          // logU back to the warm lattice, L and D to the warm arm's update
+          reset(job.warm);
           for (int c = threadIdx.x; c < nlat; c += blockDim.x) { L[c] = aux[c]; D[c] = tmp[c]; }
           __syncthreads();
-          rowtab2(L, G, D, Gd);
+          rowtab_planes(D, Gd);
           __syncthreads();
         }
         cv = use_warm ? cvs[0] : cvs[1];
@@ -894,14 +887,14 @@ struct Engine {
       }
       N4_MARK(PH_SETUP);
       for (;;) {
-        if (!pass_a(it > 0, st)) goto timeout;
+        if (!pass_a(it > 0, it > 0, st)) goto timeout;   // applies the last update
         N4_MARK(PH_A);
         if (it > 0) cv = cv_from(st, nfg);
         if (!((double)cv > pr.thr) || it >= maxIt) break;
         if (!fit_step(st)) goto timeout;
         for (int c = threadIdx.x; c < nlat; c += blockDim.x) L[c] += D[c];
         __syncthreads();
-        rowtab2(L, G, D, Gd);
+        rowtab_planes(D, Gd);
         __syncthreads();
         N4_MARK(PH_UPDATE);
         ++it;
@@ -924,6 +917,19 @@ struct Engine {
     return;
   timeout:
     if (lead) rep->status = N4_ERR_TIMEOUT;
+  }
+};
+
+// Shared-memory home of a CTA's Engine on the whole-GPU path: thread 0
+// constructs it, then every thread of the CTA uses the same object.
+template <class Group>
+struct EngineSlot {
+  static_assert(Engine<Group>::kShared, "only the whole-GPU path keeps its Engine in shared memory");
+  alignas(16) unsigned char raw[sizeof(Engine<Group>)];
+  __device__ Engine<Group> &make(const Group &g, const Plan &p, const Params &r, char *sm, char *big, float *rg) {
+    if (threadIdx.x == 0) new (raw) Engine<Group>(g, p, r, sm, big, rg);
+    __syncthreads();
+    return *reinterpret_cast<Engine<Group> *>(raw);
   }
 };
 

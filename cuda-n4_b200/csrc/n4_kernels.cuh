@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(NT, 1) k_n4_cluster(const __grid_constant__ Cl
       break;
     }
     Engine<ClusterGroup> e(g, s_pl, s_pr, sm, big, nullptr);
-    e.run(job, slab);
+    e.run(job);   // the slab holds the staged rows
   }
 }
 
@@ -338,9 +338,9 @@ __global__ void __launch_bounds__(NT, 1) k_n4_grid(const __grid_constant__ GridA
   __syncthreads();
   GridGroup g{a.bar, a.big_base, a.big_stride};
   char *big = a.big_base + (size_t)blockIdx.x * a.big_stride;
-  const int r0 = (int)((long long)a.job.X * a.job.Y * g.rank() / g.size());
-  Engine<GridGroup> e(g, s_pl, s_pr, smem, big, a.red_global);
-  e.run(a.job, a.job.imlog + (size_t)r0 * a.job.Z);
+  __shared__ EngineSlot<GridGroup> s_eng;
+  Engine<GridGroup> &e = s_eng.make(g, s_pl, s_pr, smem, big, a.red_global);
+  e.run(a.job);
 }
 
 // ------------------------------------------------------------------ tables

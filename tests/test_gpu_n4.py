@@ -397,8 +397,8 @@ def test_batch_mixing_cluster_and_whole_gpu_volumes(cuda):
     on the cluster path, it on the whole-GPU path, each as in a single run;
     the autotuner's record keeps that split."""
     import n4b200
-    # fitting grids 32x32x24, 96x96x64 (more than a 16-CTA cluster holds), 48x40x32
-    shapes = [(64, 64, 48), (192, 192, 128), (96, 80, 64)]
+    # fitting grids 32x32x24, 112x112x64 (more than a 16-CTA cluster holds), 48x40x32
+    shapes = [(64, 64, 48), (224, 224, 128), (96, 80, 64)]
     vols = []
     for i, sh in enumerate(shapes):
         ph = make_phantom(sh, seed=400 + i)
