@@ -336,7 +336,7 @@ struct SharpenBufs {
 // each elementwise step is folded into the first pass of the FFT after it.
 template <class HistF>
 __device__ void sharpen_map(const HistF &hv, int bins, int N, int off, double binMin, double slope,
-                            double wiener, double fwhm, const SharpenBufs &sb, double *E) {
+                            double wiener, double fwhm, const SharpenBufs &sb, double *E, float2 *E2 = nullptr) {
   const double ln2 = 0.69314718055994530942;
   const double scaledFWHM = fwhm / slope;
   const double expFactor = 4.0 * ln2 / (scaledFWHM * scaledFWHM);
@@ -385,23 +385,63 @@ __device__ void sharpen_map(const HistF &hv, int bins, int N, int off, double bi
   for (int b = threadIdx.x; b < bins; b += blockDim.x) {
     const double2 v = S[off + b];
     const double nu = v.x * invN, de = -v.y * invN;
-    E[b] = (de != 0.0) ? nu / de : 0.0;
+    const double e = (de != 0.0) ? nu / de : 0.0;
+    E[b] = e;
+    if (E2) {
+      const float hi = (float)e;
+      E2[b] = make_float2(hi, (float)(e - (double)hi));
+    }
   }
   __syncthreads();
+}
+
+// Float-float arithmetic (a value as the unevaluated sum of two floats, ~48
+// significant bits): Knuth's TwoSum and the FMA form of Dekker's TwoProduct
+// are error-free, so x - binMin and products keep their rounding errors
+// exactly.  The _rn intrinsics keep the compiler from contracting or
+// reassociating these sequences.
+__device__ __forceinline__ float two_sum(float a, float b, float &err) {
+  const float s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  err = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  return s;
 }
 
 // Bin coordinate of a value, (x - binMin) / slope, in FP64.  The reciprocal
 // product is within an ulp of the quotient; near the last bin the quotient
 // itself is taken, because there one ulp decides whether the reference
 // counts or drops the maximum voxel (N4.py:27).
+//
+// coord_ff gives the same coordinate from float-float arithmetic as a bin k
+// and a fraction f (|error| < 2^-24, the resolution of the histogram's fixed
+// point): d = x - binMin exactly by TwoSum (binMin is the minimum of FP32
+// values, a float), times 1/slope held as a float-float.  It declines values
+// within two bins of the top, which take the FP64 path.
 struct BinMap {
   double binMin, slope, inv_slope, top;
+  float fmin, ih, il, ff_limit;
   __device__ BinMap(double mn, double sl, int bins)
-      : binMin(mn), slope(sl), inv_slope(1.0 / sl), top((double)bins - 1.5) {}
+      : binMin(mn), slope(sl), inv_slope(1.0 / sl), top((double)bins - 1.5), fmin((float)mn),
+        ih((float)inv_slope), il((float)(inv_slope - (double)ih)), ff_limit((float)(bins - 2)) {}
   __device__ __forceinline__ double coord(float x) const {
     const double d = (double)x - binMin;
     const double c = d * inv_slope;
     return c > top ? d / slope : c;
+  }
+  __device__ __forceinline__ bool coord_ff(float x, int &k, float &f) const {
+    float dl;
+    const float dh = two_sum(x, -fmin, dl);                  // x - binMin = dh + dl exactly
+    const float p = __fmul_rn(dh, ih);
+    const float pe = __fmaf_rn(dh, ih, -p);                  // p + pe = dh * ih exactly
+    const float cl = __fadd_rn(pe, __fmaf_rn(dh, il, __fmul_rn(dl, ih)));
+    if (!(p < ff_limit)) return false;                       // near the top bin (or NaN)
+    const float kf = floorf(p);
+    f = __fadd_rn(__fsub_rn(p, kf), cl);                     // p - kf is exact
+    k = (int)kf;
+    if (f < 0.0f) { f = __fadd_rn(f, 1.0f); --k; }
+    else if (f >= 1.0f) { f = __fsub_rn(f, 1.0f); ++k; }
+    if (k < 0) { k = 0; f = 0.0f; }                          // x >= binMin: only rounding reaches here
+    return true;
   }
 };
 
@@ -422,6 +462,31 @@ __device__ __forceinline__ int hist_bin(double c, int bins, double scale, unsign
     return idx;
   }
   return -1;                                             // the reference drops it
+}
+
+// hist_bin from a coordinate given as bin k (< bins - 1) and fraction f.
+__device__ __forceinline__ int hist_bin_ff(int k, float f, double scale, unsigned &qlo, unsigned &qhi) {
+  const unsigned one = (unsigned)scale;
+  if (f == 0.0f) { qlo = one; qhi = 0u; return k; }
+  qhi = min(__float2uint_rn(__fmul_rn(f, (float)scale)), one);
+  qlo = one - qhi;
+  return k;
+}
+
+// The FP64 path of a value near the top bin, out of line: inlined, the
+// compiler may evaluate it for every value under a predicate.
+__device__ __noinline__ int hist_bin_top(const BinMap &bm, float x, int bins, double scale, unsigned &qlo,
+                                         unsigned &qhi) {
+  return hist_bin(bm.coord(x), bins, scale, qlo, qhi);
+}
+
+// Histogram contribution of one value: float-float below the top two bins.
+__device__ __forceinline__ int hist_bin_of(const BinMap &bm, float x, int bins, double scale, unsigned &qlo,
+                                           unsigned &qhi) {
+  int k;
+  float f;
+  if (bm.coord_ff(x, k, f)) return hist_bin_ff(k, f, scale, qlo, qhi);
+  return hist_bin_top(bm, x, bins, scale, qlo, qhi);
 }
 
 // Largest shift <= 24 for which `n` voxels cannot overflow a 32-bit bin.
@@ -456,6 +521,34 @@ __device__ __forceinline__ double sharpened_value(double c, const double *E, int
     return e0 + (e1 - e0) * (c - fc);
   }
   return E[bins - 1];
+}
+
+// Residual x - E(x) of the piecewise-linear remap for a value in bin
+// k < bins - 1 at fraction f, from E as float-float pairs (E2[b] = E[b] as
+// hi + lo): x - e0 by TwoSum, the slope term in FP32; within about an ulp of
+// the FP32 rounding of the FP64 residual.
+__device__ __forceinline__ float residual_ff(float x, int k, float f, const float2 *E2) {
+  const float2 e0 = E2[k], e1 = E2[k + 1];
+  const float de = __fadd_rn(__fsub_rn(e1.x, e0.x), __fsub_rn(e1.y, e0.y));
+  float terr;
+  const float t = two_sum(x, -e0.x, terr);
+  return __fadd_rn(t, __fsub_rn(__fsub_rn(terr, e0.y), __fmul_rn(de, f)));
+}
+
+// Residual x - E(x) of a masked value.  The remap is continuous in the bin
+// coordinate c (N4.py:107-113), so c enters only through E's slope within
+// one bin: an FP32 c (error ~2^-24 c, ~1e-5 at c = 200) moves the residual
+// by that error times the slope of E per bin (~1e-7 here), a per-voxel error
+// the fit averages over thousands of voxels per control point; x - E(c) itself
+// is formed in float-float.  Beyond the last bin E is constant.
+__device__ __forceinline__ float residual_of(const BinMap &bm, float x, const float2 *E2, int bins) {
+  const float c = __fmul_rn(__fsub_rn(x, bm.fmin), bm.ih);
+  const float kf = floorf(c);
+  int k = (int)kf;
+  float f = __fsub_rn(c, kf);
+  if (k >= bins - 1) { k = bins - 2; f = 1.0f; }
+  if (k < 0) { k = 0; f = 0.0f; }                      // x >= binMin: only rounding reaches here
+  return residual_ff(x, k, f, E2);
 }
 
 // Refined lattice value at output index (ox, oy, oz) (array indices), from

@@ -10,7 +10,7 @@ each (run from the repository root)::
   Rician 0.02) through ``n4_run`` at shrink 2 (256x256x160 fitting grid,
   whole-GPU path), 4 levels, <= 50 iterations, convergence 0.001.
 * ``c2x4``: four 256x256x176 phantoms (6^3 grid, N(0, 0.25^2), Rician 0.02)
-  in one batched run on 8-CTA clusters of 512 threads (the configuration the
+  in one batched run on 6-CTA clusters of 512 threads (the configuration the
   autotuner picks for this workload), shrink 4, 4 levels, convergence 0.001.
 * ``encoder``: the warm-start encoder's forward pass over 96 inputs.
 * ``fit``: ``FitBspline3D`` of a 256x256x160 field with a float mask on an
@@ -43,7 +43,7 @@ def c2x4():
     im, mk = phantoms_gpu(4, (256, 256, 176), seed=9, sigma=0.02, grid=6, coeff_std=0.25, device="cuda")
     p = n4b200.N4Param(NumberOfFittingLevels=4, MaximumNumberOfIterations=50, ConvergenceThreshold=0.001,
                        low_value=0.0, ShrinkFactor=4)
-    p.flags = n4b200.cluster_size_flag(8) | _lib.FLAG_CTA_512
+    p.flags = n4b200.cluster_size_flag(6) | _lib.FLAG_CTA_512
     res = n4b200.N4Batch([(im[i], mk[i]) for i in range(4)], p)
     torch.cuda.synchronize()
     return f"c2x4 iterations {[r.report['iterations'] for r in res]}"
