@@ -107,6 +107,7 @@ struct TuneVal {
   int corr;   // correction tile shape (index into kCorrectShape)
   int nsub;   // overlapped sub-batches (0: the default rule)
   int taper;  // 1: the first and last sub-batch half the size of the others
+  int adapt;  // > 0: each sub-batch on the smallest cluster size >= adapt its volumes fit
 };
 
 constexpr int kStaticSmemReserve = 1024;
@@ -142,8 +143,8 @@ struct n4_context {
   std::map<std::tuple<int, int, int>, int> cluster_cap;
   // sub-batch pipeline: N4 launches on two high-priority streams, prologues
   // and warm starts on one low-priority stream, corrections on another
-  cudaStream_t pipe[4] = {};
-  cudaEvent_t pev[16] = {};
+  cudaStream_t pipe[5] = {};   // N4 (2), prologues and pooling, corrections, encoder
+  cudaEvent_t pev[24] = {};
   // profiling
   int profiling = 0;
   cudaEvent_t ev[5] = {};
@@ -552,6 +553,7 @@ struct Choice {
   int corr = -1;   // correction tile shape; -1: the recorded or default one
   int nsub = 0;    // overlapped sub-batches; 0: the recorded count or the default rule
   int taper = 0;   // 1: first and last sub-batch half-size (three or more sub-batches)
+  int adapt = 0;   // > 0: per sub-batch, the smallest cluster size >= adapt that holds its volumes
 };
 
 // Autotuner key: first-level lattice, levels, bins, shrink factor and the
@@ -595,6 +597,7 @@ n4_status_t choose_path(n4_context *ctx, const n4_params_t *p, const std::vector
       c.corr = it->second.corr;
       c.nsub = it->second.nsub;
       c.taper = it->second.taper;
+      c.adapt = it->second.adapt;
       if (!(p->flags & N4_FLAG_CTA_512)) c.nt = it->second.nt;
       return N4_OK;
     }
@@ -627,6 +630,7 @@ struct Prepared {
   int corr = kCorrectDefault;    // correction tile shape
   int nsub = 1;                  // sub-batches (volume ranges sub_lo[k] .. sub_lo[k + 1])
   std::vector<int> sub_lo;
+  std::vector<int> subK;         // cluster size of each sub-batch (empty: ch.K for all)
   std::vector<int> perm;         // descriptor k holds the caller's volume perm[k]
 };
 
@@ -746,6 +750,28 @@ n4_status_t plan_run(n4_context *ctx, const n4_params_t *p, const std::vector<Ru
   // over 4: 0,0,2,3,4); drop it, no launch may see an empty sub-batch
   P.sub_lo.erase(std::unique(P.sub_lo.begin(), P.sub_lo.end()), P.sub_lo.end());
   P.nsub = (int)P.sub_lo.size() - 1;
+  // per-sub-batch cluster sizes: the volumes are planned largest first, so
+  // later sub-batches hold smaller volumes and may take smaller clusters,
+  // more of them side by side; their launches overlap the earlier ones'
+  // tails on the other engine stream
+  P.subK.clear();
+  const int want_floor = (int)((p->flags >> 19) & 31u);
+  if (want_floor) ch.adapt = want_floor;
+  if (ch.adapt > 0 && P.nsub > 1 && P.in_grid.empty()) {
+    for (int k = 0; k < P.nsub; ++k) {
+      std::vector<Dims> sub(dims.begin() + P.sub_lo[k], dims.begin() + P.sub_lo[k + 1]);
+      int Kk = 0;
+      for (int K : {2, 4, 6, 8, 12, 16}) {
+        if (K < ch.adapt) continue;
+        const Plan pl = make_plan(p, K, sub, false);
+        int cap = 0;
+        if (cluster_fits(ctx, pl)) TRY(capacity(ctx, ch.nt, K, pl.sm_bytes + pl.big_bytes, &cap));
+        if (cap > 0) { Kk = K; break; }
+      }
+      P.subK.push_back(Kk > 0 ? Kk : ch.K);
+      for (int i = P.sub_lo[k]; i < P.sub_lo[k + 1]; ++i) P.csize[i] = P.subK[k];
+    }
+  }
   // workspaces
   P.NCX = final_nc(p->NumberOfControlPoints_x, p->NumberOfFittingLevels);
   P.NCY = final_nc(p->NumberOfControlPoints_y, p->NumberOfFittingLevels);
@@ -871,12 +897,20 @@ n4_status_t enqueue_pool(n4_context *ctx, const Prepared &P, const DescBuf &B, _
 // The cluster kernel over the queue ord[o0 .. o0 + njobs) with queue counter q.
 n4_status_t launch_engine(n4_context *ctx, const n4_params_t *p, const Prepared &P, const DescBuf &B, int o0,
                           int njobs, int q, cudaStream_t st) {
+  // one shared-memory layout for every launch of the run, or, with
+  // per-sub-batch cluster sizes, the layout of this sub-batch's volumes
+  const bool own = !P.subK.empty();
+  const int K = own ? P.subK[q] : P.ch.K;
   std::vector<Dims> sub;
-  for (int i : P.in_cluster) sub.push_back(P.dims[i]);
-  Plan pl = make_plan(p, P.ch.K, sub, false);
+  if (own) {
+    for (int j = o0; j < o0 + njobs; ++j) sub.push_back(P.dims[j]);
+  } else {
+    for (int i : P.in_cluster) sub.push_back(P.dims[i]);
+  }
+  Plan pl = make_plan(p, K, sub, false);
   const int smem = pl.sm_bytes + pl.big_bytes;
   int cap = 0;
-  TRY(capacity(ctx, P.ch.nt, P.ch.K, smem, &cap));
+  TRY(capacity(ctx, P.ch.nt, K, smem, &cap));
   if (cap < 1) return fail(N4_ERR_TOO_LARGE, "no cluster of this size fits on the device");
   ClusterArgs a{};
   a.pl = pl;
@@ -887,9 +921,9 @@ n4_status_t launch_engine(n4_context *ctx, const n4_params_t *p, const Prepared 
   a.queue = B.dp<int>(P.o_q) + 4 * q;
   a.use_tma = 1;
   const int ncl = std::min<int>(cap, njobs);
-  if (P.ch.nt == 1024) TRY(launch_cluster_kernel<1024>(ctx, a, P.ch.K, ncl, smem, st));
-  else if (P.ch.nt == 768) TRY(launch_cluster_kernel<768>(ctx, a, P.ch.K, ncl, smem, st));
-  else TRY(launch_cluster_kernel<512>(ctx, a, P.ch.K, ncl, smem, st));
+  if (P.ch.nt == 1024) TRY(launch_cluster_kernel<1024>(ctx, a, K, ncl, smem, st));
+  else if (P.ch.nt == 768) TRY(launch_cluster_kernel<768>(ctx, a, K, ncl, smem, st));
+  else TRY(launch_cluster_kernel<512>(ctx, a, K, ncl, smem, st));
   return N4_OK;
 }
 
@@ -897,7 +931,7 @@ n4_status_t ensure_pipe(n4_context *ctx) {
   if (ctx->pipe[0]) return N4_OK;
   int least = 0, greatest = 0;
   CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 5; ++i)
     CK(cudaStreamCreateWithPriority(&ctx->pipe[i], cudaStreamNonBlocking, i < 2 ? greatest : least));
   for (cudaEvent_t &e : ctx->pev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   return N4_OK;
@@ -907,11 +941,13 @@ n4_status_t ensure_pipe(n4_context *ctx) {
 // device; capturable).  Sub-batch k's N4 launch waits only for its own
 // prologue and warm start, and runs on stream pipe[k % 2], so that it can
 // start on the SMs the previous launch frees while that launch's last volumes
-// finish; the prologues, pooling and encoder calls run in order on pipe[2]
-// and the corrections on pipe[3], on the SMs the clusters leave free (the N4
-// streams have the higher priority; measured, it makes no difference).
-// Every kernel reads and writes only its own volumes' buffers; st waits for
-// all four streams.
+// finish; the prologues and pooling run in order on pipe[2], the encoder
+// calls on pipe[4] (sub-batch k's after its pooling, beside sub-batch k+1's
+// prologue: measured on 48 uneven volumes, the encoder calls in line with the
+// prologues delayed the last N4 launch by 0.4 ms) and the corrections on
+// pipe[3], on the SMs the clusters leave free (the N4 streams have the
+// higher priority; measured, it makes no difference).  Every kernel reads
+// and writes only its own volumes' buffers; st waits for all five streams.
 // k_correct over `tiles` tiles from t0 with tile shape `shape`.
 n4_status_t launch_correct(int shape, long long tiles, int ncz, cudaStream_t st, const CorrectVol *vols,
                            const long long *tile_starts, int nvol, long long t0, float low) {
@@ -930,8 +966,10 @@ n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepa
                               cudaStream_t st) {
   TRY(ensure_pipe(ctx));
   const int S = P.nsub;
-  cudaStream_t side = ctx->pipe[2], corr = ctx->pipe[3];
-  cudaEvent_t *ev = ctx->pev;   // 0 fork, 1 tables, 2+k prologue k, 6+k N4 k, 10+i join of pipe[i]
+  cudaStream_t side = ctx->pipe[2], corr = ctx->pipe[3], encs = ctx->pipe[4];
+  // events: 0 fork, 1 tables, 2+k inputs of sub-batch k ready (prologue, or
+  // encoder), 6+k N4 k, 10+i join of pipe[i], 16+k pooling k
+  cudaEvent_t *ev = ctx->pev;
   CK(cudaEventRecord(ev[0], st));
   for (cudaStream_t s2 : ctx->pipe) CK(cudaStreamWaitEvent(s2, ev[0], 0));
   const int n = P.n;
@@ -967,13 +1005,17 @@ n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepa
       k_pool_fitgrid<<<pb, 256, 0, side>>>(B.dp<PoolJob>(P.o_pool) + lo, nk, x + (size_t)lo * kPoolCells);
       CK(cudaGetLastError());
       ++launches;
+      CK(cudaEventRecord(ev[16 + k], side));
+      CK(cudaStreamWaitEvent(encs, ev[16 + k], 0));
       for (int c0 = lo; c0 < hi; c0 += P.enc_batch) {
         const int nb = std::min(P.enc_batch, hi - c0);
-        TRY(n4_encoder_predict(P.enc, x + (size_t)c0 * kPoolCells, nb, ctx->warm_lat.as<float>() + 64 * c0, side));
+        TRY(n4_encoder_predict(P.enc, x + (size_t)c0 * kPoolCells, nb, ctx->warm_lat.as<float>() + 64 * c0, encs));
         launches += kEncoderLaunches;
       }
+      CK(cudaEventRecord(ev[2 + k], encs));
+    } else {
+      CK(cudaEventRecord(ev[2 + k], side));
     }
-    CK(cudaEventRecord(ev[2 + k], side));
   }
   for (int k = 0; k < S; ++k) {
     cudaStream_t es = ctx->pipe[k & 1];
@@ -990,7 +1032,7 @@ n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepa
                        hi - lo, t0, p->low_value));
     ++launches;
   }
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 5; ++i) {
     CK(cudaEventRecord(ev[10 + i], ctx->pipe[i]));
     CK(cudaStreamWaitEvent(st, ev[10 + i], 0));
   }
@@ -1039,7 +1081,13 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
     }
   }
   if (profile) TRY(prof_mark(ctx, 1, st));
-  if (!P.in_cluster.empty()) {
+  if (!P.subK.empty()) {
+    // per-sub-batch cluster sizes: one launch per sub-batch, in order
+    for (int k = 0; k < P.nsub; ++k) {
+      TRY(launch_engine(ctx, p, P, B, P.sub_lo[k], P.sub_lo[k + 1] - P.sub_lo[k], k, st));
+      ++launches;
+    }
+  } else if (!P.in_cluster.empty()) {
     TRY(launch_engine(ctx, p, P, B, 0, (int)P.in_cluster.size(), 0, st));
     ++launches;
   }
@@ -1485,24 +1533,35 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
   }
   ctx->profiling = 0;
   // overlapped sub-batches (cluster path, batches of two or more): 1 to 4,
-  // each timed over two runs on the chosen configuration and tile
-  int best_sub = 0, best_taper = 0;
+  // each timed over two runs on the chosen configuration and tile; then, on
+  // the best split and on 4 tapered sub-batches, per-sub-batch cluster sizes
+  // (each sub-batch on the smallest size >= a floor that holds its volumes)
+  // for every floor that gives sizes not timed yet
+  int best_sub = 0, best_taper = 0, best_adapt = 0;
   if (status == N4_OK && K > 0 && n > 1) {
     ch.corr = rep.corr_chosen;
     float best_sub_ms = 0.0f;
-    // 1..4 even sub-batches, then 3 and 4 with half-size ends
-    const int nc = std::min(kMaxSub, n) + (n >= 4 ? 2 : 0);
-    for (int c = 0; c < nc && status == N4_OK; ++c) {
-      const int S = c < std::min(kMaxSub, n) ? c + 1 : c - std::min(kMaxSub, n) + 3;
-      ch.nsub = S;
-      ch.taper = c >= std::min(kMaxSub, n) ? 1 : 0;
+    struct SubCand { int S, taper, adapt; };
+    std::vector<std::vector<int>> seen;   // split and per-volume cluster sizes of the candidates timed
+    // one candidate: an untimed run, then two timed ones; a per-sub-batch
+    // candidate whose split and sizes repeat a timed one is skipped
+    auto time_split = [&](const SubCand &sc) {
+      ch.nsub = sc.S;
+      ch.taper = sc.taper;
+      ch.adapt = sc.adapt;
       status = run_volumes(ctx, p, v, st, &ch);   // untimed
       if (status == N4_OK) status = collect(ctx, reps.data(), n);
-      if (status != N4_OK) break;
+      if (status != N4_OK) return;
+      std::vector<int> sig{sc.S, sc.taper};
+      for (int i = 0; i < n; ++i) sig.push_back(reps[i].cluster_size);
+      for (const auto &q : seen)
+        if (sc.adapt > 0 && q == sig) return;
+      seen.push_back(sig);
+      if (rep.sub_candidates >= N4_TUNE_MAX) return;
       if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         cudaGetLastError();
         status = fail(N4_ERR_CUDA, "cudaEventCreate failed");
-        break;
+        return;
       }
       if (cudaEventRecord(e0, st) != cudaSuccess) status = fail(N4_ERR_CUDA, "cudaEventRecord failed");
       for (int r = 0; r < 2 && status == N4_OK; ++r) status = run_volumes(ctx, p, v, st, &ch);
@@ -1514,18 +1573,36 @@ n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *p, int n, const n4
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       e0 = e1 = nullptr;
-      if (status != N4_OK) break;
-      rep.sub_ms[c] = ms / 2;
-      rep.sub_count[c] = S;
-      rep.sub_tapered[c] = ch.taper;
-      rep.sub_candidates = c + 1;
-      if (c == 0 || ms / 2 < best_sub_ms) { best_sub = S; best_taper = ch.taper; best_sub_ms = ms / 2; rep.sub_chosen = c; }
+      if (status != N4_OK) return;
+      const int k = rep.sub_candidates++;
+      rep.sub_ms[k] = ms / 2;
+      rep.sub_count[k] = sc.S;
+      rep.sub_tapered[k] = sc.taper;
+      rep.sub_adapt[k] = sc.adapt;
+      if (k == 0 || ms / 2 < best_sub_ms) {
+        best_sub = sc.S; best_taper = sc.taper; best_adapt = sc.adapt;
+        best_sub_ms = ms / 2;
+        rep.sub_chosen = k;
+      }
+    };
+    // 1..4 even sub-batches, then 3 and 4 with half-size ends
+    for (int S = 1; S <= std::min(kMaxSub, n) && status == N4_OK; ++S) time_split({S, 0, 0});
+    if (n >= 4) {
+      if (status == N4_OK) time_split({3, 1, 0});
+      if (status == N4_OK) time_split({4, 1, 0});
+    }
+    // per-sub-batch cluster sizes on the best split so far and on 4 tapered
+    const int s0 = best_sub, t0 = best_taper;
+    for (int fl : {2, 4, 6, 8}) {
+      if (status == N4_OK && s0 > 1) time_split({s0, t0, fl});
+      if (status == N4_OK && n >= 4 && !(s0 == 4 && t0 == 1)) time_split({4, 1, fl});
     }
   }
   ctx->profiling = saved_prof;
   ctx->prof_valid = false;
   if (status != N4_OK) return status;
-  ctx->tune[tune_key(p, dims)] = TuneVal{K == 0 ? 1 : 0, K, rep.threads[best], rep.corr_chosen, best_sub, best_taper};
+  ctx->tune[tune_key(p, dims)] =
+      TuneVal{K == 0 ? 1 : 0, K, rep.threads[best], rep.corr_chosen, best_sub, best_taper, best_adapt};
   if (report) *report = rep;
   return N4_OK;
 }

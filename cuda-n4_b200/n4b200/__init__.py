@@ -443,9 +443,12 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     of volumes of the same sizes with the same lattice, levels and bins.
     Returns ``{"candidates": [(cluster_size, threads, ms), ...], "chosen":
     cluster_size, "chosen_threads": threads, "correction": [(rows, threads,
-    ms), ...], "correction_chosen": (rows, threads)}`` (cluster size 0 =
-    whole-GPU path; the correction tile shapes are timed on the chosen
-    path)."""
+    ms), ...], "correction_chosen": (rows, threads), "sub_batches_ms":
+    [(count, tapered, adapt, ms), ...], "sub_batches_chosen": (count,
+    tapered, adapt)}`` (cluster size 0 = whole-GPU path; the correction tile
+    shapes and the sub-batch splits are timed on the chosen path; adapt > 0:
+    each sub-batch on the smallest cluster size >= adapt that holds its
+    volumes, 0: every sub-batch on the chosen size)."""
     torch = _torch()
     param = param or N4Param()
     cpar = param.to_c()
@@ -472,10 +475,11 @@ def autotune(volumes: Sequence, param: Optional[N4Param] = None, ctx: Optional[C
     cands = [(int(rep.cluster_size[k]), int(rep.threads[k]), float(rep.ms[k])) for k in range(rep.candidates)]
     corr = [(int(rep.corr_rows[k]), int(rep.corr_threads[k]), float(rep.corr_ms[k]))
             for k in range(rep.corr_candidates)]
-    subs = [(int(rep.sub_count[k]), bool(rep.sub_tapered[k]), float(rep.sub_ms[k])) for k in range(rep.sub_candidates)]
+    subs = [(int(rep.sub_count[k]), bool(rep.sub_tapered[k]), int(rep.sub_adapt[k]), float(rep.sub_ms[k]))
+            for k in range(rep.sub_candidates)]
     return {"candidates": cands, "chosen": cands[rep.chosen][0], "chosen_threads": cands[rep.chosen][1],
             "correction": corr, "correction_chosen": corr[rep.corr_chosen][:2] if corr else None,
-            "sub_batches_ms": subs, "sub_batches_chosen": subs[rep.sub_chosen][:2] if subs else None}
+            "sub_batches_ms": subs, "sub_batches_chosen": subs[rep.sub_chosen][:3] if subs else None}
 
 
 def autotune_components(field, mask, numberOfControlPoints, ctx: Optional[Context] = None) -> dict:

@@ -31,6 +31,12 @@ def FLAG_SUB_BATCHES(k: int) -> int:
     return (int(k) & 7) << 16
 
 
+def FLAG_SUB_CLUSTER_FLOOR(k: int) -> int:
+    """Bits 19-23 of n4_params_t.flags: with two or more sub-batches, each on
+    the smallest cluster size >= k that holds its volumes (0 = one size)."""
+    return (int(k) & 31) << 19
+
+
 class n4_params_t(C.Structure):
     _fields_ = [
         ("NumberOfHistogramBins", C.c_uint),
@@ -89,7 +95,7 @@ class n4_tune_report_t(C.Structure):
         ("corr_candidates", C.c_int), ("corr_rows", C.c_int * N4_TUNE_MAX),
         ("corr_threads", C.c_int * N4_TUNE_MAX), ("corr_ms", C.c_float * N4_TUNE_MAX), ("corr_chosen", C.c_int),
         ("sub_candidates", C.c_int), ("sub_count", C.c_int * N4_TUNE_MAX), ("sub_tapered", C.c_int * N4_TUNE_MAX),
-        ("sub_ms", C.c_float * N4_TUNE_MAX), ("sub_chosen", C.c_int),
+        ("sub_ms", C.c_float * N4_TUNE_MAX), ("sub_chosen", C.c_int), ("sub_adapt", C.c_int * N4_TUNE_MAX),
     ]
 
 

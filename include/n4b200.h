@@ -62,6 +62,13 @@ typedef enum {
  * pass, no overlap; 0 = choose: one sub-batch per two waves of clusters, at
  * most 4).  Every volume's result is the same either way. */
 #define N4_FLAG_SUB_BATCHES(k)  (((unsigned int)(k) & 7u) << 16)
+/* Bits 19-23: with two or more sub-batches, each sub-batch runs on the
+ * smallest cluster size >= k (of 2, 4, 6, 8, 12, 16) that holds its volumes
+ * instead of one size for the whole batch.  Volumes are planned largest
+ * first, so later sub-batches take smaller clusters, more of them side by
+ * side.  0 = one cluster size (or the autotuner's record).  A volume's result
+ * is its single run's on the same cluster size. */
+#define N4_FLAG_SUB_CLUSTER_FLOOR(k) (((unsigned int)(k) & 31u) << 19)
 
 /* Mirrors N4Param (cudaN4.h:24-94).  Obtain defaults from n4_params_default. */
 typedef struct {
@@ -229,12 +236,18 @@ typedef struct {
   int corr_chosen;
   /* overlapped sub-batches on the chosen path and tile (cluster path, two
    * or more volumes; 0 candidates otherwise): 1..4 of equal size, then 3
-   * and 4 with the first and last half the size of the others */
+   * and 4 with the first and last half the size of the others, all on the
+   * chosen cluster size; then per-sub-batch cluster sizes (sub_adapt > 0:
+   * each sub-batch on the smallest size >= sub_adapt that holds its
+   * volumes; the volumes are planned largest first, so later sub-batches
+   * take smaller clusters), on the best split and on 4 tapered, for each
+   * floor that gives sizes not timed before */
   int sub_candidates;
   int sub_count[N4_TUNE_MAX];      /* sub-batches                            */
   int sub_tapered[N4_TUNE_MAX];    /* 1: half-size first and last            */
   float sub_ms[N4_TUNE_MAX];       /* device time of one run                 */
   int sub_chosen;                  /* index of the candidate recorded        */
+  int sub_adapt[N4_TUNE_MAX];      /* 0: one cluster size; > 0: the floor    */
 } n4_tune_report_t;
 
 n4_status_t n4_autotune(n4_context_t *ctx, const n4_params_t *params, int n,

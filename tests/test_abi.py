@@ -41,7 +41,7 @@ def test_struct_layouts_match_header():
     assert C.sizeof(_lib.n4_report_t) == 4 * 2 + 4 * 8 * 2 + 4 * 3 + 4 + 8 + 4 * 2 + 8 * 2 + 4 * 2
     assert _lib.n4_report_t.device_begin_ns.offset % 8 == 0
     T = _lib.N4_TUNE_MAX
-    assert C.sizeof(_lib.n4_tune_report_t) == 4 + 4 * T * 3 + 4 + 4 + 4 * T * 3 + 4 + 4 + 4 * T * 3 + 4
+    assert C.sizeof(_lib.n4_tune_report_t) == 4 + 4 * T * 3 + 4 + 4 + 4 * T * 3 + 4 + 4 + 4 * T * 3 + 4 + 4 * T
     assert C.sizeof(_lib.n4_component_tune_t) == 4 + 4 * T * 4 + 8 + 4 + 4 * T * 3 + 8
     assert C.sizeof(_lib.n4_timings_t) == 4 * 4 + 4 + 4 + 8 + 8 + 4 * 6
 

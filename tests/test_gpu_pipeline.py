@@ -109,3 +109,41 @@ def test_reports_follow_the_callers_order(cuda):
         assert r.report["foreground"] == s.report["foreground"] == int((mk != 0).sum())
         assert r.report["iterations"] == s.report["iterations"]
         assert cuda.equal(r.lattice, s.lattice)
+
+
+def test_sub_batches_on_their_own_cluster_sizes(cuda):
+    """N4_FLAG_SUB_CLUSTER_FLOOR: the largest volumes' sub-batch runs on a
+    large cluster, the small volumes' on the smallest size that holds them;
+    every volume's result is bitwise its single run on the same size."""
+    import n4b200
+    from n4b200 import _lib
+    shapes = [(192, 192, 128), (64, 64, 48), (176, 192, 128), (56, 64, 48)]
+    vols = []
+    for i, sh in enumerate(shapes):
+        ph = make_phantom(sh, seed=700 + i, sigma=0.03, grid=4, coeff_std=0.15)
+        vols.append((cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda")))
+    flags = _lib.FLAG_CTA_512 | _lib.FLAG_SUB_BATCHES(2) | _lib.FLAG_SUB_CLUSTER_FLOOR(2)
+    p = n4b200.N4Param(NumberOfFittingLevels=3, MaximumNumberOfIterations=[6] * 3, ConvergenceThreshold=0.001,
+                       low_value=0.0, ShrinkFactor=2, flags=flags)
+    res = n4b200.N4Batch(vols, p)
+    sizes = [r.report["cluster_size"] for r in res]
+    print("cluster sizes", sizes)
+    assert all(r.report["status"] == "N4_OK" and r.report["path"] == "cluster" for r in res)
+    # planned largest first: the two large volumes form the first sub-batch,
+    # on a larger cluster than the two small ones
+    assert sizes[0] == sizes[2] and sizes[1] == sizes[3] and sizes[0] > sizes[1]
+    for (im, mk), r in zip(vols, res):
+        q = n4b200.N4Param(NumberOfFittingLevels=3, MaximumNumberOfIterations=[6] * 3, ConvergenceThreshold=0.001,
+                           low_value=0.0, ShrinkFactor=2,
+                           flags=_lib.FLAG_CTA_512 | n4b200.cluster_size_flag(r.report["cluster_size"]))
+        s = n4b200.N4(im, mk, q)
+        assert s.report["cluster_size"] == r.report["cluster_size"]
+        assert r.report["iterations"] == s.report["iterations"]
+        assert cuda.equal(r.lattice, s.lattice) and cuda.equal(r.im_normalized, s.im_normalized)
+    # the same in a recorded graph
+    g = n4b200.N4BatchGraph(vols, p)
+    g.launch()
+    for r, gr in zip(res, g.sync()):
+        assert gr.report["cluster_size"] == r.report["cluster_size"]
+        assert cuda.equal(r.lattice, gr.lattice)
+    g.close()
