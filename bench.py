@@ -316,8 +316,9 @@ def schedule_summary(reports, fit_voxels):
 def measure_c4(dev, enc, n=48, reps=5):
     """48 phantoms with every axis drawn from 96, 104, ..., 288 (4^3-grid bias
     N(0, 0.15^2), Rician 0.03), shrink 4, 4 levels, <= 50 iterations,
-    convergence 0.001: one batched run each, with and without the learned
-    warm start, after autotuning the batch."""
+    convergence 0.001: the batch with and without the learned warm start,
+    after autotuning it (cluster sizes, sub-batches and their per-sub-batch
+    cluster sizes), recorded as a graph and replayed, and called eagerly."""
     import numpy as np
     import torch
     import n4b200
@@ -333,22 +334,36 @@ def measure_c4(dev, enc, n=48, reps=5):
     tune = n4b200.autotune(vols, p, ctx=ctx)
     out = {"workload": f"{n} phantoms, axes uniform in 96..288 step 8, shrink 4, 4 levels, <=50 it/level, CV<0.001",
            "autotune": tune}
-    for name, kw in (("plain", {}), ("warm", {"encoder": enc})):
-        for _ in range(2):
-            res = n4b200.N4Batch(vols, p, ctx=ctx, **kw)
+    def median_ms(fn):
         times = []
         for _ in range(reps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize(dev)
             e0.record()
-            n4b200.N4Batch(vols, p, ctx=ctx, synchronous=False, **kw)
+            fn()
             e1.record()
             torch.cuda.synchronize(dev)
             times.append(e0.elapsed_time(e1))
-        ms = sorted(times)[len(times) // 2]
+        return sorted(times)[len(times) // 2], times
+
+    for name, kw in (("plain", {}), ("warm", {"encoder": enc})):
+        for _ in range(2):
+            res = n4b200.N4Batch(vols, p, ctx=ctx, **kw)
+        # the batch recorded as a graph and replayed (as the headline measures
+        # its batch), and n4_run_batched called eagerly (host planning and
+        # descriptor upload inside the timed region)
+        g = n4b200.N4BatchGraph(vols, p, ctx=ctx, **kw)
+        g.launch()
+        g.sync()
+        ms, times = median_ms(g.launch)
+        g.sync()
+        g.close()
+        ms_eager, _ = median_ms(lambda: n4b200.N4Batch(vols, p, ctx=ctx, synchronous=False, **kw))
         fv = [int(np.prod(n4b200.fitting_dims(p, tuple(im.shape)))) for im, _ in vols]
         out[name] = {"volumes_per_s": n * 1000.0 / ms, "ms_per_batch_median": ms, "ms_per_batch_all": times,
+                     "eager_volumes_per_s": n * 1000.0 / ms_eager, "eager_ms_per_batch_median": ms_eager,
                      "iterations_per_volume": sum(sum(r.report["iterations"][:r.report["levels"]]) for r in res) / n,
+                     "cluster_sizes": sorted({r.report["cluster_size"] for r in res}),
                      "paths": {k: sum(1 for r in res if r.report["path"] == k) for k in ("cluster", "grid")},
                      "schedule": schedule_summary([r.report for r in res], fv)}
     ctx.close()

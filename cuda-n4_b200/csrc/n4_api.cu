@@ -36,8 +36,8 @@ n4_status_t fail(n4_status_t s, const std::string &msg) {
 n4_status_t n4_record_error(n4_status_t s, const char *msg) { return fail(s, msg); }
 // defined in the encoder translation unit
 int n4_encoder_capacity(const n4_encoder_t *enc);
-// kernels one n4_encoder_predict call launches (4 convolutions + the head)
-constexpr int kEncoderLaunches = 5;
+// kernels one n4_encoder_predict call of batch B launches
+int n4_encoder_predict_launches(const n4_encoder_t *enc, int B);
 
 namespace {
 
@@ -1010,22 +1010,20 @@ n4_status_t enqueue_pipelined(n4_context *ctx, const n4_params_t *p, const Prepa
       for (int c0 = lo; c0 < hi; c0 += P.enc_batch) {
         const int nb = std::min(P.enc_batch, hi - c0);
         TRY(n4_encoder_predict(P.enc, x + (size_t)c0 * kPoolCells, nb, ctx->warm_lat.as<float>() + 64 * c0, encs));
-        launches += kEncoderLaunches;
+        launches += n4_encoder_predict_launches(P.enc, nb);
       }
       CK(cudaEventRecord(ev[2 + k], encs));
     } else {
       CK(cudaEventRecord(ev[2 + k], side));
     }
-  }
-  for (int k = 0; k < S; ++k) {
+    // sub-batch k's N4 launch and correction are enqueued right after its
+    // inputs, so that the device need not wait for the host to enqueue the
+    // later sub-batches' prologues and encoder calls first
     cudaStream_t es = ctx->pipe[k & 1];
     CK(cudaStreamWaitEvent(es, ev[2 + k], 0));
-    TRY(launch_engine(ctx, p, P, B, P.sub_lo[k], P.sub_lo[k + 1] - P.sub_lo[k], k, es));
+    TRY(launch_engine(ctx, p, P, B, lo, nk, k, es));
     CK(cudaEventRecord(ev[6 + k], es));
     ++launches;
-  }
-  for (int k = 0; k < S; ++k) {
-    const int lo = P.sub_lo[k], hi = P.sub_lo[k + 1];
     const long long t0 = tst[lo], t1 = hi < n ? tst[hi] : P.tiles;
     CK(cudaStreamWaitEvent(corr, ev[6 + k], 0));
     TRY(launch_correct(P.corr, t1 - t0, P.NCZ, corr, B.dp<CorrectVol>(P.o_cor) + lo, B.dp<long long>(P.o_tst) + lo,
@@ -1077,7 +1075,7 @@ n4_status_t enqueue_run(n4_context *ctx, const n4_params_t *p, const Prepared &P
       const int nb = std::min(P.enc_batch, n - c0);
       TRY(n4_encoder_predict(P.enc, (const __nv_bfloat16 *)ctx->warm_x.p + (size_t)c0 * kPoolCells, nb,
                              ctx->warm_lat.as<float>() + 64 * c0, st));
-      launches += kEncoderLaunches;
+      launches += n4_encoder_predict_launches(P.enc, nb);
     }
   }
   if (profile) TRY(prof_mark(ctx, 1, st));

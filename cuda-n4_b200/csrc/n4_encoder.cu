@@ -14,6 +14,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -299,6 +300,27 @@ __global__ void k_sum_splits(const float *part, int splits, int n, float *out) {
   }
 }
 
+// A forward GEMM split over K: each block stores its partial sums (the
+// wrapper's store), then k_finish adds the splits in order and applies the
+// layer's own store (bias, ReLU, BF16 for the convolutions).  The forward's
+// small layers (conv3, conv4, the linear head: 1 to 6 blocks of 64x64) would
+// otherwise walk 16-54 K steps in one block each.
+template <class P>
+struct Partial : P {
+  float *part;   // [splits][M][N]
+  __device__ void store(int m, int n, int z, float v) const { part[((size_t)z * this->M + m) * this->N + n] = v; }
+};
+
+template <class P>
+__global__ void k_finish(const P p, const float *part, int splits) {
+  const long long mn = (long long)p.M * p.N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < mn; i += (long long)gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int z = 0; z < splits; ++z) s += part[z * mn + i];
+    p.store((int)(i / p.N), (int)(i % p.N), 0, s);
+  }
+}
+
 // bias gradient: sum of dy' over batch and positions, one block per channel
 __global__ void k_bias_grad(const bf16 *dy, const bf16 *y, int B, int C, int pos, int relu, float *db) {
   const int c = blockIdx.x;
@@ -363,6 +385,32 @@ cudaError_t run_gemm(const P &p, int splits, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Splits of a forward GEMM: enough blocks for about two per SM, at least two
+// K steps per split, within the partials buffer (cap floats).
+inline int fwd_splits(int M, int N, int K, size_t cap) {
+  const long long tiles = (long long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+  const int steps = (K + BK - 1) / BK;
+  long long s = std::max<long long>(1, 296 / tiles);
+  s = std::min<long long>(s, std::max(1, steps / 2));
+  while (s > 1 && (size_t)s * M * N > cap) --s;
+  return (int)s;
+}
+
+// A forward layer: one pass, or split over K into `part` and finished in order.
+template <class P>
+cudaError_t run_forward(const P &p, float *part, size_t cap, cudaStream_t st) {
+  const int splits = fwd_splits(p.M, p.N, p.K, cap);
+  if (splits == 1) return run_gemm(p, 1, st);
+  Partial<P> q;
+  static_cast<P &>(q) = p;
+  q.part = part;
+  cudaError_t e = run_gemm(q, splits, st);
+  if (e != cudaSuccess) return e;
+  const long long mn = (long long)p.M * p.N;
+  k_finish<P><<<(int)std::min<long long>((mn + 255) / 256, 1024), 256, 0, st>>>(p, part, splits);
+  return cudaGetLastError();
+}
+
 struct Layout {
   // parameter offsets (floats) in the flat parameter vector
   size_t w[kLayers + 1], b[kLayers + 1], total;
@@ -406,6 +454,18 @@ n4_status_t n4_record_error(n4_status_t s, const char *msg);
 
 // largest batch one n4_encoder_predict call takes (used by n4_api.cu)
 int n4_encoder_capacity(const n4_encoder_t *enc) { return enc ? enc->max_batch : 0; }
+
+// kernels one n4_encoder_predict call of batch B launches (used by n4_api.cu):
+// a GEMM per layer and the head, and a finishing pass for each split one
+int n4_encoder_predict_launches(const n4_encoder_t *enc, int B) {
+  if (!enc || B < 1) return 0;
+  const enc::Layout L(B);
+  int n = enc::kLayers + 1;
+  for (int l = 0; l < enc::kLayers; ++l)
+    n += enc::fwd_splits(B * L.s[l].out_pos(), L.s[l].Co, L.s[l].Ci * 27, enc->part_cap) > 1 ? 1 : 0;
+  n += enc::fwd_splits(B, enc::kOut, enc::kFeat, enc->part_cap) > 1 ? 1 : 0;
+  return n;
+}
 
 namespace {
 n4_status_t efail(n4_status_t s, const std::string &m) { return n4_record_error(s, m.c_str()); }
@@ -508,10 +568,10 @@ static n4_status_t forward(n4_encoder *e, const void *d_x, int B, cudaStream_t s
   for (int l = 0; l < kLayers; ++l) {
     const Shape &s = L.s[l];
     ConvFwd p{B * s.out_pos(), s.Co, s.Ci * 27, s, e->act[l], e->pb + L.w[l], e->p + L.b[l], e->act[l + 1], 1};
-    ECK(run_gemm(p, 1, st));
+    ECK(run_forward(p, e->part, e->part_cap, st));
   }
   LinFwd lf{B, kOut, kFeat, e->act[kLayers], e->pb + L.w[kLayers], e->p + L.b[kLayers], e->out};
-  ECK(run_gemm(lf, 1, st));
+  ECK(run_forward(lf, e->part, e->part_cap, st));
   return N4_OK;
 }
 
