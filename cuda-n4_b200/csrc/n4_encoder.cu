@@ -519,6 +519,16 @@ n4_status_t n4_encoder_create(n4_encoder_t **out, int device, int max_batch) {
     need = std::max(need, (size_t)wgrad_splits(K) * L.s[l].Co * L.s[l].Ci * 27);
   }
   need = std::max(need, (size_t)wgrad_splits(max_batch) * kOut * kFeat);
+  // and the forward's split layers at every batch size up to max_batch
+  const size_t unbounded = ~(size_t)0;
+  for (int b = 1; b <= max_batch; ++b) {
+    const Layout Lb(b);
+    for (int l = 0; l < kLayers; ++l) {
+      const int M = b * Lb.s[l].out_pos(), N = Lb.s[l].Co;
+      need = std::max(need, (size_t)fwd_splits(M, N, Lb.s[l].Ci * 27, unbounded) * M * N);
+    }
+    need = std::max(need, (size_t)fwd_splits(b, kOut, kFeat, unbounded) * b * kOut);
+  }
   if ((err = cudaMalloc(&e->part, need * 4))) return fail_free(err);
   e->part_cap = need;
   *out = e;
