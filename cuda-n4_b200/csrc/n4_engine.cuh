@@ -451,7 +451,7 @@ struct Engine {
             for (int vz = lo; vz < hi; ++vz) {
               const float lu = iv[vz];
               if (isnan(lu)) continue;
-              const float r = degenerate ? 0.0f : residual_of(*bm, lu, E2, pr.bins);
+              const float r = degenerate ? 0.0f : residual_of(*bm, lu, E2, E, pr.bins);
               const float4 w = W4[vz];
               a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
               a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
@@ -468,7 +468,7 @@ struct Engine {
               if (isnan(v[u])) continue;
               const int vz = vb + u;
               const float lu = v[u];
-              const float r = degenerate ? 0.0f : residual_of(*bm, lu, E2, pr.bins);
+              const float r = degenerate ? 0.0f : residual_of(*bm, lu, E2, E, pr.bins);
               const float4 w = W4[vz];
               a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
               a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);

@@ -54,6 +54,21 @@ def test_small_vs_reference_n4py(cuda, golden_small, tag, force):
     assert nrel(np.log(b), log_bias(lat_ref, im.shape)) < TOL
 
 
+def test_small_volume_few_iterations(cuda):
+    """32x32x24 (a 24 k-voxel fitting grid), 2 levels x 4 iterations: a small
+    lattice (max |L| ~0.04), where an error of the remap's bin coordinate shows
+    most (an FP32 coordinate alone moves the oracle's lattice by 1.4e-4)."""
+    import n4b200
+    for seed in (3, 4, 5):
+        ph = make_phantom((32, 32, 24), seed=seed, sigma=0.03, grid=4, coeff_std=0.15)
+        res = n4b200.N4(cuda.tensor(ph.im, device="cuda"), cuda.tensor(ph.mask, device="cuda"),
+                        param(2, [4, 4], 0.0))
+        out, lat = O.N4(ph.im, ph.mask, low_value=0, maximumNumberOfLevels=2, maximumNumberOfIterations=[4, 4],
+                        ConvergenceThreshold=0.0)
+        assert nrel(res.lattice, lat) < TOL
+        assert nrel(res.im_normalized, out) < TOL
+
+
 def test_c1_fixed_iterations(cuda, golden_c1):
     """64x64x48 phantom, 3 levels x 50 iterations, against N4.py's run."""
     import n4b200
