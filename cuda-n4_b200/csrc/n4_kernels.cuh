@@ -506,62 +506,68 @@ __device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long 
       cq[q][3] = sh ? w.z : w.w;
       cq[q][4] = sh ? w.w : 0.0f;
     }
+    // the tile's evaluation of row r at the thread's 4 voxels
+    auto eval_row = [&](int r, float (&bz)[4]) {
+      const float *g = Gs + r * ncz;
+      if (two) {
+        const float g0 = g[s0], g1 = g[s0 + 1], g2 = g[s0 + 2], g3 = g[s0 + 3];
+        const float g4 = has5 ? g[s0 + 4] : 0.0f;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float b = __fmul_rn(cq[q][0], g0);
+          b = __fmaf_rn(cq[q][1], g1, b);
+          b = __fmaf_rn(cq[q][2], g2, b);
+          b = __fmaf_rn(cq[q][3], g3, b);
+          bz[q] = __fmaf_rn(cq[q][4], g4, b);
+        }
+      } else {   // short spans: the general form (weights re-read, rare)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) bz[q] = dot4(az.w[z + q], g + sz[q]);
+      }
+    };
+    if (!C.im) {
+      // the log field only (EvaluateBspline3D): stores, no loads
+#pragma unroll 4
+      for (int r = r_first; r < nr; r += rpp) {
+        float bz[4];
+        eval_row(r, bz);
+        __stcs((float4 *)(C.out + base + (long long)r * FZ + z), make_float4(bz[0], bz[1], bz[2], bz[3]));
+      }
+      return;
+    }
     for (int rb = r_first; rb < nr; rb += kCorrectPre * rpp) {
       // the next step's loads go out before this step's rows are evaluated
       // (double buffering: 4 % faster on the 96-volume bench batch)
       float4 xnx[kCorrectPre];
-      if (C.im) {
 #pragma unroll
-        for (int k = 0; k < kCorrectPre; ++k) {
-          const int r = rb + (kCorrectPre + k) * rpp;
-          xnx[k] = r < nr ? __ldcs((const float4 *)(C.im + base + (long long)r * FZ + z))
-                          : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+      for (int k = 0; k < kCorrectPre; ++k) {
+        const int r = rb + (kCorrectPre + k) * rpp;
+        xnx[k] = r < nr ? __ldcs((const float4 *)(C.im + base + (long long)r * FZ + z))
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
       }
 #pragma unroll
       for (int k = 0; k < kCorrectPre; ++k) {
         const int r = rb + k * rpp;
         if (r >= nr) break;
-        const float *g = Gs + r * ncz;
         float bz[4];
-        if (two) {
-          const float g0 = g[s0], g1 = g[s0 + 1], g2 = g[s0 + 2], g3 = g[s0 + 3];
-          const float g4 = has5 ? g[s0 + 4] : 0.0f;
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            float b = __fmul_rn(cq[q][0], g0);
-            b = __fmaf_rn(cq[q][1], g1, b);
-            b = __fmaf_rn(cq[q][2], g2, b);
-            b = __fmaf_rn(cq[q][3], g3, b);
-            bz[q] = __fmaf_rn(cq[q][4], g4, b);
-          }
-        } else {   // short spans: the general form (weights re-read, rare)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) bz[q] = dot4(az.w[z + q], g + sz[q]);
-        }
+        eval_row(r, bz);
         const long long off = base + (long long)r * FZ + z;
-        if (C.im) {
-          // im / exp(b) as im * exp(-b): one special-function op per voxel
-          // (fast intrinsic, a few ulp); exp(b) only when it is an output
-          const float xa[4] = {xin[k].x, xin[k].y, xin[k].z, xin[k].w};
-          float o[4];
+        // im / exp(b) as im * exp(-b): one special-function op per voxel
+        // (fast intrinsic, a few ulp); exp(b) only when it is an output
+        const float xa[4] = {xin[k].x, xin[k].y, xin[k].z, xin[k].w};
+        float o[4];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) o[q] = xa[q] > low ? xa[q] * __expf(-bz[q]) : 0.0f;
-          if (C.bias) {
-            float e[4];
+        for (int q = 0; q < 4; ++q) o[q] = xa[q] > low ? xa[q] * __expf(-bz[q]) : 0.0f;
+        if (C.bias) {
+          float e[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) e[q] = __expf(bz[q]);
-            __stcs((float4 *)(C.bias + off), make_float4(e[0], e[1], e[2], e[3]));
-          }
-          __stcs((float4 *)(C.out + off), make_float4(o[0], o[1], o[2], o[3]));
-        } else {
-          __stcs((float4 *)(C.out + off), make_float4(bz[0], bz[1], bz[2], bz[3]));
+          for (int q = 0; q < 4; ++q) e[q] = __expf(bz[q]);
+          __stcs((float4 *)(C.bias + off), make_float4(e[0], e[1], e[2], e[3]));
         }
+        __stcs((float4 *)(C.out + off), make_float4(o[0], o[1], o[2], o[3]));
       }
-      if (C.im) {
 #pragma unroll
-        for (int k = 0; k < kCorrectPre; ++k) xin[k] = xnx[k];
-      }
+      for (int k = 0; k < kCorrectPre; ++k) xin[k] = xnx[k];
     }
   } else {
     for (int t = threadIdx.x; t < nr * FZ; t += blockDim.x) {
