@@ -117,6 +117,12 @@ def test_c2_shape_shrink4(cuda):
     assert all(abs(a - b) <= 1 for a, b in zip(got, rep["iterations"])), (got, rep["iterations"])
     if got == rep["iterations"]:
         assert nrel(conv.lattice, lat2) < TOL
+    # the oracle's own stopping points, run as fixed counts: the converged
+    # lattice is pinned even where a CV within rounding of the threshold
+    # stops the two runs one iteration apart
+    pinned = n4b200.N4(im, mk, param(4, rep["iterations"], 0.0, ShrinkFactor=4))
+    assert pinned.report["iterations"][:4] == rep["iterations"]
+    assert nrel(pinned.lattice, lat2) < TOL
 
 
 def test_cluster_and_grid_paths_agree(cuda):
