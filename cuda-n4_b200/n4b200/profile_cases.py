@@ -2,9 +2,10 @@
 each (run from the repository root)::
 
     PYTHONPATH=cuda-n4_b200 python -m n4b200.profile_cases c3       # k_n4_grid
-    PYTHONPATH=cuda-n4_b200 python -m n4b200.profile_cases c2x4     # k_n4_cluster
+    PYTHONPATH=cuda-n4_b200 python -m n4b200.profile_cases c2x4     # k_n4_cluster, k_prologue, k_correct
     PYTHONPATH=cuda-n4_b200 python -m n4b200.profile_cases encoder  # enc::k_igemm
     PYTHONPATH=cuda-n4_b200 python -m n4b200.profile_cases fit      # k_fit_rows_v5
+    PYTHONPATH=cuda-n4_b200 python -m n4b200.profile_cases evaluate # k_correct (log field only)
 
 * ``c3``: one 512x512x320 phantom (0.5 mm, 8^3-grid bias N(0, 0.25^2),
   Rician 0.02) through ``n4_run`` at shrink 2 (256x256x160 fitting grid,
@@ -15,6 +16,8 @@ each (run from the repository root)::
 * ``encoder``: the warm-start encoder's forward pass over 96 inputs.
 * ``fit``: ``FitBspline3D`` of a 256x256x160 field with a float mask on an
   11^3 lattice (the z contraction reads 8 B per voxel).
+* ``evaluate``: ``EvaluateBspline3D`` of an 11^3 lattice at 512x512x320 (4 B
+  per voxel written), after the component autotuner picked its tile.
 
 Every case prints one line and exits 0 on success.
 """
@@ -71,7 +74,20 @@ def fit():
     return f"fit lattice {tuple(lat.shape)}"
 
 
-CASES = {"c3": c3, "c2x4": c2x4, "encoder": encoder, "fit": fit}
+def evaluate():
+    import torch
+    import n4b200
+    ctx = n4b200.Context(0)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    lat = torch.randn((11, 11, 11), device="cuda", generator=g) * 0.1
+    field = torch.zeros((512, 512, 320), device="cuda")
+    n4b200.autotune_components(field, None, (11, 11, 11), ctx=ctx)
+    out = n4b200.EvaluateBspline3D(lat, (11, 11, 11), (512, 512, 320), ctx=ctx)
+    torch.cuda.synchronize()
+    return f"evaluate {tuple(out.shape)}"
+
+
+CASES = {"c3": c3, "c2x4": c2x4, "encoder": encoder, "fit": fit, "evaluate": evaluate}
 
 
 def main(argv=None):
