@@ -950,14 +950,18 @@ n4_status_t ensure_pipe(n4_context *ctx) {
 // and writes only its own volumes' buffers; st waits for all five streams.
 // k_correct over `tiles` tiles from t0 with tile shape `shape`.
 n4_status_t launch_correct(int shape, long long tiles, int ncz, cudaStream_t st, const CorrectVol *vols,
-                           const long long *tile_starts, int nvol, long long t0, float low) {
+                           const long long *tile_starts, int nvol, long long t0, float low, bool log_only = false) {
   if (tiles <= 0) return N4_OK;
   const CorrectShape cs = kCorrectShape[shape];
   const size_t smem = correct_smem_bytes(cs.rows, ncz);
-  if (cs.threads == 512)
-    k_correct<512><<<(unsigned)tiles, 512, smem, st>>>(vols, tile_starts, nvol, t0, low, cs.rows);
-  else
-    k_correct<256><<<(unsigned)tiles, 256, smem, st>>>(vols, tile_starts, nvol, t0, low, cs.rows);
+  const unsigned g = (unsigned)tiles;
+  if (log_only) {
+    if (cs.threads == 512) k_correct<512, true><<<g, 512, smem, st>>>(vols, tile_starts, nvol, t0, low, cs.rows);
+    else k_correct<256, true><<<g, 256, smem, st>>>(vols, tile_starts, nvol, t0, low, cs.rows);
+  } else {
+    if (cs.threads == 512) k_correct<512, false><<<g, 512, smem, st>>>(vols, tile_starts, nvol, t0, low, cs.rows);
+    else k_correct<256, false><<<g, 256, smem, st>>>(vols, tile_starts, nvol, t0, low, cs.rows);
+  }
   CK(cudaGetLastError());
   return N4_OK;
 }
@@ -1244,8 +1248,10 @@ n4_status_t n4_create(n4_context_t **out, int device) {
   CK(cudaDeviceGetAttribute(&c->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   // the largest correction tile: 512 rows of kMaxNcz z control points
   const int corr_smem = (int)correct_smem_bytes(512, kMaxNcz);
-  if (cudaFuncSetAttribute(k_correct<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, corr_smem) != cudaSuccess ||
-      cudaFuncSetAttribute(k_correct<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, corr_smem) != cudaSuccess) {
+  if (cudaFuncSetAttribute(k_correct<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, corr_smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_correct<512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, corr_smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_correct<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, corr_smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_correct<512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, corr_smem) != cudaSuccess) {
     cudaGetLastError();
     delete c;
     return fail(N4_ERR_CUDA, "cannot raise the correction kernel's shared-memory limit");
@@ -2090,7 +2096,7 @@ n4_status_t n4_evaluate_bspline3d(n4_context_t *ctx, const float *d_lattice, uns
   const size_t so = align_up(sizeof(cv), 16);
   const bool prof = ctx->profiling != 0;
   if (prof) TRY(prof_mark(ctx, 1, st));
-  TRY(launch_correct(shape, tiles, (int)ncpt_z, st, u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0, 0.0f));
+  TRY(launch_correct(shape, tiles, (int)ncpt_z, st, u.dp<CorrectVol>(0), u.dp<long long>(so), 1, 0, 0.0f, true));
   if (prof) { TRY(prof_mark(ctx, 2, st)); TRY(prof_mark(ctx, 3, st)); TRY(prof_mark(ctx, 4, st)); }
   ctx->prof_launches = 2;
   ctx->prof_fit = 0;
@@ -2182,7 +2188,7 @@ n4_status_t n4_autotune_components(n4_context_t *ctx, const float *d_field, cons
       float ms = 0.0f;
       n4_status_t ls = N4_OK;
       status = timed([&] { ls = launch_correct(k, tiles, (int)ncpt_z, st, u.dp<CorrectVol>(0),
-                                               u.dp<long long>(so), 1, 0, 0.0f); }, &ms);
+                                               u.dp<long long>(so), 1, 0, 0.0f, true); }, &ms);
       if (status == N4_OK) status = ls;
       if (status != N4_OK) break;
       const int c = rep.eval_candidates++;

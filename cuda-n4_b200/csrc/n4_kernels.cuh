@@ -392,10 +392,13 @@ __host__ __device__ inline size_t correct_smem_bytes(int rows, int ncz) {
 // (a tile spanning more than two planes, or a slice larger than kLxMax,
 // contracts each row directly).  Then z is evaluated per voxel with float4
 // I/O.  HBM traffic: read im, write out (+ bias).
-constexpr int kCorrectPre = 4;   // rows of input float4s a thread loads per step (two steps in flight)
+constexpr int kCorrectPre = 3;   // rows of input float4s a thread loads per step (two steps in flight)
 
 // Tile `tile` of a batch (numbered as in CorrectVol::tile0) of the volumes
-// vols[0 .. nvol); Gs and Lx in shared memory.
+// vols[0 .. nvol); Gs and Lx in shared memory.  kLog: every volume's im is
+// null and the log field is the output (its own instantiation: no input
+// registers held).
+template <bool kLog>
 __device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long long *tile_starts, int nvol,
                                              long long tile, float low, int rt, float *Gs, float *Lx) {
   const int v = find_volume(tile_starts, nvol, tile);
@@ -435,16 +438,21 @@ __device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long 
         Lx[t] = __fmaf_rn(wx.w, __ldg(lp + 3 * slice), acc);
       }
       __syncthreads();
-      for (int t = threadIdx.x; t < nr * ncz; t += blockDim.x) {
-        const int r = t / ncz, cz = t - r * ncz;
-        const unsigned row = rw0 + (unsigned)r;
-        const int vx = (int)(row / FY), vy = (int)(row - (unsigned)vx * FY);
-        const float *lx = Lx + (vx - vxa) * slice + ay.s[vy] * ncz + cz;
+      // entry (r, cz) at t = r * lanes + cz, lanes the power of two >= ncz
+      // (no divisions); rows past the first plane's end continue in the next
+      const int lsh = ncz <= 16 ? 4 : (ncz <= 32 ? 5 : 6);
+      const int vy0 = (int)(rw0 - (unsigned)vxa * FY);
+      for (int t = threadIdx.x; t < (nr << lsh); t += blockDim.x) {
+        const int r = t >> lsh, cz = t & ((1 << lsh) - 1);
+        if (cz >= ncz) continue;
+        int vy = vy0 + r, pl = 0;
+        if (vy >= (int)FY) { vy -= (int)FY; pl = 1; }
+        const float *lx = Lx + pl * slice + ay.s[vy] * ncz + cz;
         const float4 wy = ay.w[vy];
         float acc = __fmul_rn(wy.x, lx[0]);
         acc = __fmaf_rn(wy.y, lx[ncz], acc);
         acc = __fmaf_rn(wy.z, lx[2 * ncz], acc);
-        Gs[t] = __fmaf_rn(wy.w, lx[3 * ncz], acc);
+        Gs[r * ncz + cz] = __fmaf_rn(wy.w, lx[3 * ncz], acc);
       }
     } else {
       const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
@@ -473,7 +481,7 @@ __device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long 
     }
   }
   float4 xin[kCorrectPre];
-  if (act && C.im) {
+  if (!kLog && act) {
 #pragma unroll
     for (int k = 0; k < kCorrectPre; ++k) {
       const int r = r_first + k * rpp;
@@ -506,75 +514,87 @@ __device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long 
       cq[q][3] = sh ? w.z : w.w;
       cq[q][4] = sh ? w.w : 0.0f;
     }
-    // the tile's evaluation of row r at the thread's 4 voxels
-    auto eval_row = [&](int r, float (&bz)[4]) {
-      const float *g = Gs + r * ncz;
-      if (two) {
-        const float g0 = g[s0], g1 = g[s0 + 1], g2 = g[s0 + 2], g3 = g[s0 + 3];
-        const float g4 = has5 ? g[s0 + 4] : 0.0f;
+    // the thread's 4 voxels of the row whose contraction starts at g: the
+    // two-span form above, or the general form (weights re-read, short spans)
+    auto eval_two = [&](const float *g, float (&bz)[4]) {
+      const float g0 = g[s0], g1 = g[s0 + 1], g2 = g[s0 + 2], g3 = g[s0 + 3];
+      const float g4 = has5 ? g[s0 + 4] : 0.0f;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          float b = __fmul_rn(cq[q][0], g0);
-          b = __fmaf_rn(cq[q][1], g1, b);
-          b = __fmaf_rn(cq[q][2], g2, b);
-          b = __fmaf_rn(cq[q][3], g3, b);
-          bz[q] = __fmaf_rn(cq[q][4], g4, b);
-        }
-      } else {   // short spans: the general form (weights re-read, rare)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) bz[q] = dot4(az.w[z + q], g + sz[q]);
+      for (int q = 0; q < 4; ++q) {
+        float b = __fmul_rn(cq[q][0], g0);
+        b = __fmaf_rn(cq[q][1], g1, b);
+        b = __fmaf_rn(cq[q][2], g2, b);
+        b = __fmaf_rn(cq[q][3], g3, b);
+        bz[q] = __fmaf_rn(cq[q][4], g4, b);
       }
     };
-    if (!C.im) {
-      // the log field only (EvaluateBspline3D): stores, no loads
+    auto eval_gen = [&](const float *g, float (&bz)[4]) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bz[q] = dot4(az.w[z + q], g + sz[q]);
+    };
+    // the thread's rows r_first, r_first + rpp, ...: contractions gstep
+    // floats apart, voxels step float4s apart (offsets within the tile < 2^31)
+    const int gstep = rpp * ncz, step = rpp * (FZ >> 2);
+    const float *g_first = Gs + r_first * ncz;
+    const int v_first = r_first * (FZ >> 2) + (z >> 2);
+    float4 *out4 = (float4 *)(C.out + base);
+    auto rows = [&](auto &&ev) {
+      if constexpr (kLog) {
+        // the log field only (EvaluateBspline3D): stores, no loads
+        const float *g = g_first;
+        int v = v_first;
 #pragma unroll 4
-      for (int r = r_first; r < nr; r += rpp) {
-        float bz[4];
-        eval_row(r, bz);
-        __stcs((float4 *)(C.out + base + (long long)r * FZ + z), make_float4(bz[0], bz[1], bz[2], bz[3]));
-      }
-      return;
-    }
-    for (int rb = r_first; rb < nr; rb += kCorrectPre * rpp) {
-      // the next step's loads go out before this step's rows are evaluated
-      // (double buffering: 4 % faster on the 96-volume bench batch)
-      float4 xnx[kCorrectPre];
-#pragma unroll
-      for (int k = 0; k < kCorrectPre; ++k) {
-        const int r = rb + (kCorrectPre + k) * rpp;
-        xnx[k] = r < nr ? __ldcs((const float4 *)(C.im + base + (long long)r * FZ + z))
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-#pragma unroll
-      for (int k = 0; k < kCorrectPre; ++k) {
-        const int r = rb + k * rpp;
-        if (r >= nr) break;
-        float bz[4];
-        eval_row(r, bz);
-        const long long off = base + (long long)r * FZ + z;
-        // im / exp(b) as im * exp(-b): one special-function op per voxel
-        // (fast intrinsic, a few ulp); exp(b) only when it is an output
-        const float xa[4] = {xin[k].x, xin[k].y, xin[k].z, xin[k].w};
-        float o[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) o[q] = xa[q] > low ? xa[q] * __expf(-bz[q]) : 0.0f;
-        if (C.bias) {
-          float e[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) e[q] = __expf(bz[q]);
-          __stcs((float4 *)(C.bias + off), make_float4(e[0], e[1], e[2], e[3]));
+        for (int r = r_first; r < nr; r += rpp, g += gstep, v += step) {
+          float bz[4];
+          ev(g, bz);
+          __stcs(out4 + v, make_float4(bz[0], bz[1], bz[2], bz[3]));
         }
-        __stcs((float4 *)(C.out + off), make_float4(o[0], o[1], o[2], o[3]));
-      }
+      } else {
+        const float4 *in4 = (const float4 *)(C.im + base);
+        float4 *bias4 = C.bias ? (float4 *)(C.bias + base) : nullptr;
+        const float *g = g_first;
+        int v = v_first;
+        for (int rb = r_first; rb < nr; rb += kCorrectPre * rpp, g += kCorrectPre * gstep, v += kCorrectPre * step) {
+          // the next step's loads go out before this step's rows are evaluated
+          // (double buffering: 4 % faster on the 96-volume bench batch)
+          float4 xnx[kCorrectPre];
 #pragma unroll
-      for (int k = 0; k < kCorrectPre; ++k) xin[k] = xnx[k];
-    }
+          for (int k = 0; k < kCorrectPre; ++k) {
+            const int r = rb + (kCorrectPre + k) * rpp;
+            xnx[k] = r < nr ? __ldcs(in4 + v + (kCorrectPre + k) * step) : make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+#pragma unroll
+          for (int k = 0; k < kCorrectPre; ++k) {
+            if (rb + k * rpp >= nr) break;
+            float bz[4];
+            ev(g + k * gstep, bz);
+            // im / exp(b) as im * exp(-b): one special-function op per voxel
+            // (fast intrinsic, a few ulp); exp(b) only when it is an output
+            const float xa[4] = {xin[k].x, xin[k].y, xin[k].z, xin[k].w};
+            float o[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) o[q] = xa[q] > low ? xa[q] * __expf(-bz[q]) : 0.0f;
+            if (bias4) {
+              float e[4];
+#pragma unroll
+              for (int q = 0; q < 4; ++q) e[q] = __expf(bz[q]);
+              __stcs(bias4 + v + k * step, make_float4(e[0], e[1], e[2], e[3]));
+            }
+            __stcs(out4 + v + k * step, make_float4(o[0], o[1], o[2], o[3]));
+          }
+#pragma unroll
+          for (int k = 0; k < kCorrectPre; ++k) xin[k] = xnx[k];
+        }
+      }
+    };
+    if (two) rows(eval_two);
+    else rows(eval_gen);
   } else {
     for (int t = threadIdx.x; t < nr * FZ; t += blockDim.x) {
       const int r = t / FZ, zz = t - r * FZ;
       const long long off = base + (long long)r * FZ + zz;
       const float b = dot4(az.w[zz], Gs + r * ncz + az.s[zz]);
-      if (C.im) {
+      if constexpr (!kLog) {
         const float x = C.im[off];
         C.out[off] = x > low ? x * __expf(-b) : 0.0f;
         if (C.bias) C.bias[off] = __expf(b);
@@ -587,13 +607,14 @@ __device__ __forceinline__ void correct_tile(const CorrectVol *vols, const long 
 
 // Tile t0 + blockIdx.x of a batch (numbered as in CorrectVol::tile0, tiles of
 // `rt` rows) of the volumes vols[0 .. nvol); dynamic shared memory
-// correct_smem_bytes(rt, ncz).
-template <int NT>
-__global__ void __launch_bounds__(NT, NT <= 256 ? 3 : 1) k_correct(const CorrectVol *vols,
+// correct_smem_bytes(rt, ncz).  256 threads: 4 CTAs per SM for the log field
+// (64 registers), 3 for the correction, whose loads in flight need more.
+template <int NT, bool kLog>
+__global__ void __launch_bounds__(NT, NT <= 256 ? (kLog ? 4 : 3) : 1) k_correct(const CorrectVol *vols,
                                                                    const long long *tile_starts, int nvol,
                                                                    long long t0, float low, int rt) {
   extern __shared__ __align__(16) float correct_sm[];
-  correct_tile(vols, tile_starts, nvol, t0 + blockIdx.x, low, rt, correct_sm + 2 * kLxMax, correct_sm);
+  correct_tile<kLog>(vols, tile_starts, nvol, t0 + blockIdx.x, low, rt, correct_sm + 2 * kLxMax, correct_sm);
 }
 
 // ------------------------------------------------------------------ standalone fit

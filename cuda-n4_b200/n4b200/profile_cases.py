@@ -17,7 +17,8 @@ each (run from the repository root)::
 * ``fit``: ``FitBspline3D`` of a 256x256x160 field with a float mask on an
   11^3 lattice (the z contraction reads 8 B per voxel).
 * ``evaluate``: ``EvaluateBspline3D`` of an 11^3 lattice at 512x512x320 (4 B
-  per voxel written), after the component autotuner picked its tile.
+  per voxel written) on the default tile (128 rows, 256 threads; the one the
+  component autotuner picks for this size when it runs without a profiler).
 
 Every case prints one line and exits 0 on success.
 """
@@ -80,8 +81,6 @@ def evaluate():
     ctx = n4b200.Context(0)
     g = torch.Generator(device="cuda").manual_seed(7)
     lat = torch.randn((11, 11, 11), device="cuda", generator=g) * 0.1
-    field = torch.zeros((512, 512, 320), device="cuda")
-    n4b200.autotune_components(field, None, (11, 11, 11), ctx=ctx)
     out = n4b200.EvaluateBspline3D(lat, (11, 11, 11), (512, 512, 320), ctx=ctx)
     torch.cuda.synchronize()
     return f"evaluate {tuple(out.shape)}"
