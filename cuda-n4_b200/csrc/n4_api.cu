@@ -288,7 +288,7 @@ Plan make_plan(const n4_params_t *p, int K, const std::vector<Dims> &vols, bool 
     pl.o_fb = take(fft_bytes);
   }
   pl.o_H64 = take((size_t)pl.bins * 8);
-  pl.o_E2 = take((size_t)pl.bins * 8);   // E as float-float pairs
+  pl.o_R2 = take((size_t)pl.bins * 8);   // the residual's per-bin linear form
   pl.o_E = take((size_t)pl.bins * 8);
   pl.o_tw = take((size_t)pl.npad * 16);
   pl.o_ff = grid ? take((size_t)pl.npad * 8) : 0;   // cluster: in the Gd region

@@ -334,9 +334,10 @@ struct SharpenBufs {
 // E[0..bins) from the fractional histogram (bin b's weight hv(b)) (N4.py:32-101,
 // cudaN4.cu:733-817), all in FP64; all threads of the CTA call it.  Four FFTs;
 // each elementwise step is folded into the first pass of the FFT after it.
+// R2 (optional): the residual table of residual_lin, R2[b] for b < bins - 1.
 template <class HistF>
 __device__ void sharpen_map(const HistF &hv, int bins, int N, int off, double binMin, double slope,
-                            double wiener, double fwhm, const SharpenBufs &sb, double *E, float2 *E2 = nullptr) {
+                            double wiener, double fwhm, const SharpenBufs &sb, double *E, float2 *R2 = nullptr) {
   const double ln2 = 0.69314718055994530942;
   const double scaledFWHM = fwhm / slope;
   const double expFactor = 4.0 * ln2 / (scaledFWHM * scaledFWHM);
@@ -382,15 +383,16 @@ __device__ void sharpen_map(const HistF &hv, int bins, int N, int off, double bi
         return make_double2(v.x * f, -v.y * f);
       },
       P2, P, N, sb.tw);
-  for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+  auto e_at = [&](int b) {
     const double2 v = S[off + b];
     const double nu = v.x * invN, de = -v.y * invN;
-    const double e = (de != 0.0) ? nu / de : 0.0;
+    return (de != 0.0) ? nu / de : 0.0;
+  };
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+    const double e = e_at(b);
     E[b] = e;
-    if (E2) {
-      const float hi = (float)e;
-      E2[b] = make_float2(hi, (float)(e - (double)hi));
-    }
+    if (R2 && b + 1 < bins)
+      R2[b] = make_float2((float)(binMin + (double)b * slope - e), (float)(slope - (e_at(b + 1) - e)));
   }
   __syncthreads();
 }
@@ -524,15 +526,15 @@ __device__ __forceinline__ double sharpened_value(double c, const double *E, int
 }
 
 // Residual x - E(x) of the piecewise-linear remap for a value in bin
-// k < bins - 1 at fraction f, from E as float-float pairs (E2[b] = E[b] as
-// hi + lo): x - e0 by TwoSum, the slope term in FP32; within about an ulp of
-// the FP32 rounding of the FP64 residual.
-__device__ __forceinline__ float residual_ff(float x, int k, float f, const float2 *E2) {
-  const float2 e0 = E2[k], e1 = E2[k + 1];
-  const float de = __fadd_rn(__fsub_rn(e1.x, e0.x), __fsub_rn(e1.y, e0.y));
-  float terr;
-  const float t = two_sum(x, -e0.x, terr);
-  return __fadd_rn(t, __fsub_rn(__fsub_rn(terr, e0.y), __fmul_rn(de, f)));
+// k < bins - 1 at fraction f.  With x = binMin + (k + f) slope and
+// E(x) = E[k] + f (E[k+1] - E[k]) (N4.py:107-113) the residual is linear in f
+// within a bin: x - E(x) = R2[k].x + f R2[k].y, R2[k] = (binMin + k slope -
+// E[k], slope - (E[k+1] - E[k])) formed in FP64 by sharpen_map, so the
+// cancellation of the O(1) terms happens in FP64.  The fraction's own error
+// (~2^-24) moves the result by ~2^-24 |R2[k].y| <= 2^-24 slope.
+__device__ __forceinline__ float residual_lin(int k, float f, const float2 *R2) {
+  const float2 t = R2[k];
+  return __fmaf_rn(f, t.y, t.x);
 }
 
 // The FP64 residual of a value near the top bin, out of line: inlined, the
@@ -542,15 +544,15 @@ __device__ __noinline__ float residual_top(const BinMap &bm, float x, const doub
 }
 
 // Residual x - E(x) of a masked value (N4.py:107-113): the bin and fraction
-// from the float-float coordinate, x - E(c) in float-float; FP64 in the top
-// two bins.  (An FP32 coordinate, error ~2^-24 c, moved the lattice of a
+// from the float-float coordinate, then the bin's linear form; FP64 in the
+// top two bins.  (An FP32 coordinate, error ~2^-24 c, moved the lattice of a
 // 32x32x24 volume after 2 x 4 iterations by 1.4e-4 relative, measured with
 // the oracle: the bound is 1e-4.)
-__device__ __forceinline__ float residual_of(const BinMap &bm, float x, const float2 *E2, const double *E,
+__device__ __forceinline__ float residual_of(const BinMap &bm, float x, const float2 *R2, const double *E,
                                              int bins) {
   int k;
   float f;
-  if (bm.coord_ff(x, k, f)) return residual_ff(x, k, f, E2);
+  if (bm.coord_ff(x, k, f)) return residual_lin(k, f, R2);
   return residual_top(bm, x, E, bins);
 }
 

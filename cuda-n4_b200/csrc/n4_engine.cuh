@@ -61,7 +61,7 @@ struct Plan {
   int Xmax, Ymax, Zmax, slab_floats, rows_max, nvxl;
   int bins, npad, hoff;
   // shared
-  int o_ax, o_ay, o_az, o_L, o_D, o_den, o_tmp, o_aux, o_hist, o_H64, o_E2, o_E;
+  int o_ax, o_ay, o_az, o_L, o_D, o_den, o_tmp, o_aux, o_hist, o_H64, o_R2, o_E;
   int o_fa, o_fb, o_tw, o_ff, o_red, o_misc;
   int sm_bytes;
   // big
@@ -180,7 +180,7 @@ struct Engine {
   // smem views
   float *L, *D, *den, *tmp, *aux;
   double *E, *Ff;
-  float2 *E2;          // E as float-float pairs, for the residual
+  float2 *R2;          // the residual's per-bin linear form (residual_lin)
   unsigned *hist;
   unsigned long long *H64;
   double2 *fa, *fb, *tw;
@@ -194,7 +194,7 @@ struct Engine {
     L = (float *)(sm + pl.o_L); D = (float *)(sm + pl.o_D); den = (float *)(sm + pl.o_den);
     tmp = (float *)(sm + pl.o_tmp); aux = (float *)(sm + pl.o_aux);
     hist = (unsigned *)(sm + pl.o_hist); H64 = (unsigned long long *)(sm + pl.o_H64);
-    E2 = (float2 *)(sm + pl.o_E2); E = (double *)(sm + pl.o_E);
+    R2 = (float2 *)(sm + pl.o_R2); E = (double *)(sm + pl.o_E);
     fa = (double2 *)(sm + pl.o_fa); fb = (double2 *)(sm + pl.o_fb); tw = (double2 *)(sm + pl.o_tw);
     Ff = (double *)(sm + pl.o_ff); red = (double *)(sm + pl.o_red);
     Gd = (float *)(big + pl.b_Gd); T2 = (float *)(big + pl.b_T2);
@@ -451,7 +451,7 @@ struct Engine {
             for (int vz = lo; vz < hi; ++vz) {
               const float lu = iv[vz];
               if (isnan(lu)) continue;
-              const float r = degenerate ? 0.0f : residual_of(*bm, lu, E2, E, pr.bins);
+              const float r = degenerate ? 0.0f : residual_of(*bm, lu, R2, E, pr.bins);
               const float4 w = W4[vz];
               a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
               a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
@@ -468,7 +468,7 @@ struct Engine {
               if (isnan(v[u])) continue;
               const int vz = vb + u;
               const float lu = v[u];
-              const float r = degenerate ? 0.0f : residual_of(*bm, lu, E2, E, pr.bins);
+              const float r = degenerate ? 0.0f : residual_of(*bm, lu, R2, E, pr.bins);
               const float4 w = W4[vz];
               a0 = __fmaf_rn(w.x, r, a0); a1 = __fmaf_rn(w.y, r, a1);
               a2 = __fmaf_rn(w.z, r, a2); a3 = __fmaf_rn(w.w, r, a3);
@@ -735,7 +735,7 @@ struct Engine {
     const unsigned long long *h64 = H64;
     SharpenBufs sb{fa, fb, tw, Ff};
     sharpen_map([=](int b) { return (double)h64[b] * inv; }, bins, pl.npad, pl.hoff, bm.binMin, bm.slope,
-                pr.wiener, pr.fwhm, sb, E, E2);
+                pr.wiener, pr.fwhm, sb, E, R2);
     N4_MARK(PH_SHARP);
     return true;
   }
