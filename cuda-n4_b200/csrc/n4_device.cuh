@@ -447,6 +447,23 @@ struct BinMap {
   }
 };
 
+// exp(x) - 1 of a convergence term (N4.py:121-126): for |x| < 1/4 its Taylor
+// series through x^7 / 7! in Horner form, x + x^2 (1/2! + x (1/3! + ...)),
+// whose truncation is below x^7 / 8! < 2^-28 relative and whose last step
+// is one fused multiply-add (0.65 ulp at most against FP64 over 2^21 samples
+// of the interval); expm1f beyond (first iterations of a level).
+__device__ __forceinline__ float expm1_conv(float x) {
+  if (fabsf(x) < 0.25f) {
+    float p = __fmaf_rn(x, 1.0f / 5040.0f, 1.0f / 720.0f);
+    p = __fmaf_rn(p, x, 1.0f / 120.0f);
+    p = __fmaf_rn(p, x, 1.0f / 24.0f);
+    p = __fmaf_rn(p, x, 1.0f / 6.0f);
+    p = __fmaf_rn(p, x, 0.5f);
+    return __fmaf_rn(__fmul_rn(x, x), p, x);
+  }
+  return expm1f(x);
+}
+
 // Fractional histogram contribution of one value (N4.py:21-29) from its
 // FP64 bin coordinate, as fixed-point weights of 2^shift per voxel (the two
 // parts of a split add up to exactly one voxel).  Returns the bin or -1 when

@@ -599,7 +599,7 @@ struct Engine {
             if (isnan(lu)) continue;   // outside the mask
             if (need_cv) {
               const float ed = dot4(w, Gd + rl * ncz + sz);
-              const float y = expm1f(-ed);
+              const float y = expm1_conv(-ed);
               sy += (double)y;
               syy += (double)y * (double)y;
               if (apply) {
@@ -630,7 +630,7 @@ struct Engine {
             if (isnan(v[u])) continue;   // outside the mask
             float lu = v[u];
             if (need_cv) {
-              const float y = expm1f(-evd[u]);
+              const float y = expm1_conv(-evd[u]);
               sy += (double)y;
               syy += (double)y * (double)y;
               if (apply) {
@@ -651,7 +651,7 @@ struct Engine {
         if (need_cv) {
           const int rl = (int)divZ.div((unsigned)i), vz = i - rl * Z;
           const float ed = eval(Gd, rl, vz);
-          const float y = expm1f(-ed);
+          const float y = expm1_conv(-ed);
           sy += (double)y;
           syy += (double)y * (double)y;
           if (apply) {
