@@ -343,11 +343,17 @@ __device__ void sharpen_map(const HistF &hv, int bins, int N, int off, double bi
   const double expFactor = 4.0 * ln2 / (scaledFWHM * scaledFWHM);
   const double scaleFactor = 2.0 * sqrt(ln2 / 3.14159265358979323846) / scaledFWHM;
   const double invN = 1.0 / (double)N;
+  // the periodic Gaussian's N/2 + 1 distinct values, one per thread of the
+  // CTA (the first FFT pass has only N/4 threads busy), held in sb.Ff until
+  // the second FFT overwrites it with the transform
+  for (int d = threadIdx.x; d <= N / 2; d += blockDim.x)
+    sb.Ff[d] = scaleFactor * exp(-(double)d * (double)d * expFactor);
+  __syncthreads();
   // z = V + i F : the padded histogram and the periodic Gaussian in one FFT
   double2 *Z = fft_from(
       [&](int i) {
         const int d = i <= N / 2 ? i : N - i;
-        const double F = scaleFactor * exp(-(double)d * (double)d * expFactor);
+        const double F = sb.Ff[d];
         const double V = (i >= off && i < off + bins) ? hv(i - off) : 0.0;
         return make_double2(V, F);
       },
