@@ -434,15 +434,31 @@ struct Engine {
   __device__ void contract(bool num_mode, const BinMap *bm = nullptr, bool degenerate = false) {
     float *T1 = Gd;   // Gd is dead between pass A and the next update
     const int nt1 = nrow * ncz;
-    for (int t = threadIdx.x; t < nt1; t += blockDim.x) T1[t] = 0.0f;
+    // whole-GPU path, few spans per row (coarse levels): the (row, span) tasks
+    // leave most of the CTA's threads idle (443 rows of 160 voxels for 1024
+    // threads at 512x512x320), so each span is cut in two halves, summed by
+    // two threads into two tables (the second after the first in Gd, when it
+    // fits) that are added at the end.  (On the cluster path, rows of ~44
+    // voxels, the extra tasks and the final pass cost more than they save.)
+    const int gd_floats = (pl.b_T2 - pl.b_Gd) / 4;
+    const int halves = (Group::kGrid && az.nsp <= 4 && 2 * nt1 <= gd_floats) ? 2 : 1;
+    float *T1b = T1 + nt1;
+    for (int t = threadIdx.x; t < halves * nt1; t += blockDim.x) T1[t] = 0.0f;
     __syncthreads();
     const float4 *W4 = num_mode ? az.p4 : az.q4;
     for (int phase = 0; phase < 4; ++phase) {
       const int nsp = phase < az.nsp ? (az.nsp - phase + 3) / 4 : 0;   // spans phase, phase+4, ...
-      const int ntask = nrow * nsp;
+      const int per_row = nsp * halves;
+      const int ntask = nrow * per_row;
       for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
-        const int rl = t / nsp, sp = phase + 4 * (t - rl * nsp);
-        const int lo = az.lo[sp], hi = az.hi[sp];
+        const int rl = t / per_row, rem = t - rl * per_row;
+        const int sp = phase + 4 * (halves == 2 ? rem >> 1 : rem), h = halves == 2 ? rem & 1 : 0;
+        int lo = az.lo[sp], hi = az.hi[sp];
+        if (halves == 2) {
+          const int mid = (lo + hi) >> 1;
+          if (h) lo = mid;
+          else hi = mid;
+        }
         float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
         if (num_mode) {
           // residual R = logU - E(logU) of each masked voxel
@@ -495,9 +511,13 @@ struct Engine {
             }
           }
         }
-        float *t1 = T1 + rl * ncz + sp;
+        float *t1 = (h ? T1b : T1) + rl * ncz + sp;
         t1[0] += a0; t1[1] += a1; t1[2] += a2; t1[3] += a3;
       }
+      __syncthreads();
+    }
+    if (halves == 2) {
+      for (int t = threadIdx.x; t < nt1; t += blockDim.x) T1[t] = __fadd_rn(T1[t], T1b[t]);
       __syncthreads();
     }
     N4_MARK(PH_F_T1);
