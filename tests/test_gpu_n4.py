@@ -312,6 +312,34 @@ def test_vector_prologue_matches_scalar(cuda, shrink, u8):
     assert cuda.equal(res[0].im_normalized, res[1].im_normalized)
 
 
+def test_shrink2_batch_prologue_matches_scalar(cuda):
+    """A shrink-2 batch with more fitting voxels than prologue threads
+    (4 x 64x64x48 = 786k against 148 SMs x 16 CTAs x 256) makes threads take
+    further voxels, some of them in another volume, on their grid-stride loop;
+    the batch corrects bitwise alike when one volume sits 4 bytes off
+    alignment, which sends the whole batch through the scalar prologue."""
+    import n4b200
+    shape = (128, 128, 96)
+    phs = [make_phantom(shape, seed=300 + i) for i in range(4)]
+    n = phs[0].im.size
+    p = param(2, [4, 4], 0.0, ShrinkFactor=2)
+    res = []
+    for off in (0, 1):
+        vols = []
+        for i, ph in enumerate(phs):
+            o = off if i == 2 else 0
+            ib = cuda.zeros(n + 8, device="cuda")
+            ib[o:o + n] = cuda.tensor(ph.im.ravel(), device="cuda")
+            mb = cuda.zeros(n + 8, device="cuda")
+            mb[o:o + n] = cuda.tensor(ph.mask.ravel().astype(np.float32), device="cuda")
+            vols.append((ib[o:o + n].view(shape), mb[o:o + n].view(shape)))
+        res.append(n4b200.N4Batch(vols, p))
+    for a, b in zip(res[0], res[1]):
+        assert a.report["status"] == "N4_OK"
+        assert cuda.equal(a.lattice, b.lattice)
+        assert cuda.equal(a.im_normalized, b.im_normalized)
+
+
 def test_batch_graph_replays(cuda):
     """The graph-recorded batch equals N4Batch, and a launch after refilling
     an input in place corrects the new data."""
