@@ -879,7 +879,18 @@ void launch_prologue(const n4_params_t *p, const Prepared &P, const DescBuf &B, 
   const PrologueVol *pv = B.dp<PrologueVol>(P.o_pro) + lo;
   const long long *pst = B.dp<long long>(P.o_pst) + lo;
   int *flg = B.dp<int>(P.o_flg) + lo;
-  const int nb = std::max(blocks, 1);
+  // A grid of more than one wave is cut to whole waves of the variant's
+  // resident CTAs: every CTA runs the same number of grid-stride passes, so a
+  // last partial wave would run as long as a full one on a fraction of the SMs
+  // (148 x 16 CTAs of k_prologue<2>, 5 resident per SM, were 3.2 waves).
+  int nb = std::max(blocks, 1), dev = 0, nsm = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess &&
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+      (S == 4   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_prologue<4>, 256, 0)
+       : S == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_prologue<2>, 256, 0)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_prologue<0>, 256, 0)) == cudaSuccess &&
+      nsm > 0 && per_sm > 0 && nb > nsm * per_sm)
+    nb = nb / (nsm * per_sm) * (nsm * per_sm);
   if (S == 4) k_prologue<4><<<nb, 256, 0, st>>>(pv, pst, hi - lo, g0, count, p->low_value, flg);
   else if (S == 2) k_prologue<2><<<nb, 256, 0, st>>>(pv, pst, hi - lo, g0, count, p->low_value, flg);
   else k_prologue<0><<<nb, 256, 0, st>>>(pv, pst, hi - lo, g0, count, p->low_value, flg);
