@@ -68,9 +68,11 @@ __device__ __forceinline__ unsigned char vget(const uchar4 &v, int i) {
 // 2^31 fitting voxels and its rows of S voxels aligned to S floats (S bytes for
 // a byte mask): the block's S*S rows are read as one vector load per row and
 // array, all requested before they are summed, in the scalar path's order
-// (the same sums, bitwise).
+// (the same sums, bitwise).  The loads' latency bounds S = 0 and 2, so both
+// ask for 6 resident CTAs per SM (40 registers); S = 4 needs 62 for its
+// 16-row batches and keeps 4.
 template <int S>
-__global__ void __launch_bounds__(256, S == 0 ? 6 : 4) k_prologue(const PrologueVol *vols, const long long *starts,
+__global__ void __launch_bounds__(256, S == 4 ? 4 : 6) k_prologue(const PrologueVol *vols, const long long *starts,
                                                                   int nvol, long long g0, long long total, float low,
                                                                   int *flag_nonfinite) {
   const long long end = g0 + total;
